@@ -1,0 +1,412 @@
+// C ABI of the engine: contexts, equations of state and the RHS group.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "axb_flux_launch.cuh"
+#include "axb_internal.hxx"
+#include "axb_rhs_misc.cuh"
+
+using namespace axb;
+
+namespace {
+
+int check_box(const axb_box *b, int min_ng) {
+  if (!b)
+    return AXB_ERR_ARG;
+  for (int d = 0; d < 3; ++d)
+    if (b->n[d] < 1 || !(b->dx[d] > 0))
+      return AXB_ERR_ARG;
+  if (b->ng < min_ng)
+    return AXB_ERR_GHOSTS;
+  if (b->sy < b->n[0] + 2 * b->ng + 1 || b->sz < b->sy * (b->n[1] + 2 * b->ng + 1))
+    return AXB_ERR_ARG;
+  return AXB_OK;
+}
+
+ReconParams recon_params(const axb_params &p) {
+  ReconParams r;
+  r.ppm_shock_detection = p.ppm_shock_detection;
+  r.ppm_zone_flattening = p.ppm_zone_flattening;
+  r.poly_k = p.poly_k;
+  r.poly_gamma = p.poly_gamma;
+  r.ppm_eta1 = p.ppm_eta1;
+  r.ppm_eta2 = p.ppm_eta2;
+  r.ppm_eps = p.ppm_eps;
+  r.ppm_eps_shock = p.ppm_eps_shock;
+  r.ppm_small = p.ppm_small;
+  r.ppm_omega1 = p.ppm_omega1;
+  r.ppm_omega2 = p.ppm_omega2;
+  r.weno_eps = p.weno_eps;
+  r.mp5_alpha = p.mp5_alpha;
+  return r;
+}
+
+#define GFP(name) (f->gf[AXB_GF_##name])
+
+} // namespace
+
+AXB_API void axb_params_default(axb_params *p) {
+  std::memset(p, 0, sizeof *p);
+  // ReconX/param.ccl
+  p->reconstruction_method = AXB_RECON_GODUNOV;
+  p->loworder_method = AXB_RECON_GODUNOV;
+  p->reconstruct_with_temperature = 0;
+  p->ppm_shock_detection = 1;
+  p->ppm_zone_flattening = 0;
+  p->ppm_eta1 = 20.0;
+  p->ppm_eta2 = 0.05;
+  p->ppm_eps = 0.33;
+  p->ppm_eps_shock = 0.01;
+  p->ppm_small = 1e-7;
+  p->ppm_omega1 = 0.75;
+  p->ppm_omega2 = 10.0;
+  p->enhanced_ppm_C2 = 1.25;
+  p->weno_eps = 1e-26;
+  p->mp5_alpha = 4.0;
+  // EOSX/param.ccl
+  p->poly_k = 100.0;
+  p->poly_gamma = 2.0;
+  // AsterX/param.ccl
+  p->flux_type = AXB_FLUX_LXF;
+  p->recon_type = AXB_RECVAR_V;
+  p->vector_potential_gauge = AXB_GAUGE_GEN_LORENZ;
+  p->local_spatial_order = 2;
+  p->lorenz_damp_fac = 0.0;
+  // Con2PrimFactory/param.ccl
+  p->c2p_prime = AXB_C2P_NOBLE;
+  p->c2p_second = AXB_C2P_PALENZUELA;
+  p->max_iter = 30;
+  p->thermal_eos_atmo = 1;
+  p->c2p_tol = 1e-10;
+  p->rho_abs_min = 1e-13;
+  p->atmo_tol = 1e-3;
+  p->eps_atmo = 1e-10;
+  p->p_atmo = 1e-10;
+  p->t_atmo = 1e-2;
+  p->Ye_atmo = 0.5;
+  p->r_atmo = 1e100;
+  p->alp_thresh = 0.0;
+  p->rho_BH = 1e100;
+  p->eps_BH = 1e100;
+  p->vwlim_BH = 1e100;
+  p->cons_error_limit = -1;
+  p->vw_lim = 10.0;
+  p->B_lim = 100.0;
+}
+
+AXB_API const char *axb_gf_name(int id) {
+  static const char *names[] = {
+#define AXB_GF_NAME_(name) #name,
+      AXB_GF_LIST(AXB_GF_NAME_)
+#undef AXB_GF_NAME_
+  };
+  return (id >= 0 && id < AXB_NUM_GF) ? names[id] : nullptr;
+}
+
+AXB_API int axb_ctx_create(int device, axb_ctx **out) {
+  if (!out)
+    return AXB_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+    return AXB_ERR_NO_DEVICE;
+  cudaDeviceProp prop;
+  AXB_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10)
+    return AXB_ERR_NO_DEVICE;
+  AXB_CUDA_TRY(cudaSetDevice(device));
+  axb_ctx *c = new (std::nothrow) axb_ctx();
+  if (!c)
+    return AXB_ERR_ARG;
+  c->device = device;
+  if (cudaMalloc(&c->status, sizeof(DevStatus)) != cudaSuccess ||
+      cudaMallocHost(&c->status_host_pinned, sizeof(DevStatus)) != cudaSuccess) {
+    delete c;
+    return AXB_ERR_CUDA;
+  }
+  AXB_CUDA_TRY(cudaMemset(c->status, 0, sizeof(DevStatus)));
+  *out = c;
+  return AXB_OK;
+}
+
+AXB_API int axb_ctx_destroy(axb_ctx *c) {
+  if (!c)
+    return AXB_ERR_ARG;
+  cudaFree(c->status);
+  cudaFreeHost(c->status_host_pinned);
+  delete c;
+  return AXB_OK;
+}
+
+// Clear the device error word, CFL maximum and c2p counters (stream-ordered).
+AXB_API int axb_status_reset(axb_ctx *c, void *stream) {
+  if (!c)
+    return AXB_ERR_ARG;
+  AXB_CUDA_TRY(cudaMemsetAsync(c->status, 0, sizeof(DevStatus),
+                               (cudaStream_t)stream));
+  return AXB_OK;
+}
+
+// Synchronously read the device status: error word (AXB_EW_* bits), the
+// maximum characteristic speed seen by the flux passes since the last reset,
+// the number of C2P_FAIL cells, and (optionally, 64 entries) the histogram
+// of first-solver iteration counts.
+AXB_API int axb_status_read(axb_ctx *c, void *stream, uint32_t *error_word,
+                            double *max_speed, uint32_t *c2p_fail,
+                            uint64_t *iter_hist64) {
+  if (!c)
+    return AXB_ERR_ARG;
+  AXB_CUDA_TRY(cudaMemcpyAsync(c->status_host_pinned, c->status,
+                               sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                               (cudaStream_t)stream));
+  AXB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  const DevStatus &h = *c->status_host_pinned;
+  if (error_word)
+    *error_word = h.error_word;
+  if (max_speed) {
+    const long long bits = (long long)h.max_speed_bits;
+    double v;
+    std::memcpy(&v, &bits, sizeof v);
+    *max_speed = v;
+  }
+  if (c2p_fail)
+    *c2p_fail = h.c2p_fail_count;
+  if (iter_hist64)
+    for (int i = 0; i < 64; ++i)
+      iter_hist64[i] = h.c2p_iter_hist[i];
+  return AXB_OK;
+}
+
+// Ideal-gas evolution EOS (EOSX_Setup_EOS, EOSX/src/setup_eos.cxx:70-78) plus
+// the initial-data polytrope used for a cold atmosphere (:33-41).
+AXB_API int axb_eos_create_idealgas(double gamma, double particle_mass,
+                                    const double rho_range[2],
+                                    const double eps_range[2],
+                                    const double ye_range[2], double poly_gamma,
+                                    double poly_k, axb_eos **out) {
+  if (!out || !rho_range || !eps_range || !ye_range || !(gamma >= 1) ||
+      !(poly_gamma > 1))
+    return AXB_ERR_ARG;
+  axb_eos *e = new (std::nothrow) axb_eos();
+  if (!e)
+    return AXB_ERR_ARG;
+  e->kind = 0;
+  e->ideal = make_ideal(gamma, particle_mass, Range{eps_range[0], eps_range[1]},
+                        Range{rho_range[0], rho_range[1]},
+                        Range{ye_range[0], ye_range[1]});
+  e->poly = make_poly(poly_gamma, poly_k);
+  e->tab_host = nullptr;
+  e->tab_dev = nullptr;
+  *out = e;
+  return AXB_OK;
+}
+
+AXB_API int axb_eos_destroy(axb_eos *e) {
+  if (!e)
+    return AXB_ERR_ARG;
+  if (e->tab_dev)
+    cudaFree(e->tab_dev);
+  delete e->tab_host;
+  delete e;
+  return AXB_OK;
+}
+
+namespace {
+int fill_rhs_args(axb_ctx *c, const axb_box *box, const axb_fields *f,
+                  const axb_params *p, RhsArgs &a) {
+  int rc = check_box(box, 3);
+  if (rc)
+    return rc;
+  if (!f || !p)
+    return AXB_ERR_ARG;
+  if (p->recon_type != AXB_RECVAR_V || p->use_uct ||
+      p->reconstruct_with_temperature ||
+      p->reconstruction_method == AXB_RECON_EPPM ||
+      !(p->local_spatial_order == 2 || p->local_spatial_order == 4))
+    return AXB_ERR_UNSUPPORTED;
+  if (p->local_spatial_order == 4 && box->ng < 3)
+    return AXB_ERR_GHOSTS;
+  a.b = make_box(*box);
+  a.rho = GFP(rho);
+  a.vel[0] = GFP(velx);
+  a.vel[1] = GFP(vely);
+  a.vel[2] = GFP(velz);
+  a.eps = GFP(eps);
+  a.press = GFP(press);
+  a.Ye = GFP(Ye);
+  a.entropy = GFP(entropy);
+  a.Bvec[0] = GFP(Bvecx);
+  a.Bvec[1] = GFP(Bvecy);
+  a.Bvec[2] = GFP(Bvecz);
+  a.dBstag[0] = GFP(dBx_stag);
+  a.dBstag[1] = GFP(dBy_stag);
+  a.dBstag[2] = GFP(dBz_stag);
+  a.alp = GFP(alp);
+  a.beta[0] = GFP(betax);
+  a.beta[1] = GFP(betay);
+  a.beta[2] = GFP(betaz);
+  const int gid[6] = {AXB_GF_gxx, AXB_GF_gxy, AXB_GF_gxz, AXB_GF_gyy, AXB_GF_gyz, AXB_GF_gzz};
+  const int kid[6] = {AXB_GF_kxx, AXB_GF_kxy, AXB_GF_kxz, AXB_GF_kyy, AXB_GF_kyz, AXB_GF_kzz};
+  for (int q = 0; q < 6; ++q) {
+    a.g[q] = f->gf[gid[q]];
+    a.K[q] = f->gf[kid[q]];
+  }
+  a.Avec[0] = GFP(Avec_x);
+  a.Avec[1] = GFP(Avec_y);
+  a.Avec[2] = GFP(Avec_z);
+  a.Psi = GFP(Psi);
+  const int accid[7] = {AXB_GF_acc_dens, AXB_GF_acc_momx, AXB_GF_acc_momy,
+                        AXB_GF_acc_momz, AXB_GF_acc_tau,  AXB_GF_acc_DYe,
+                        AXB_GF_acc_DEnt};
+  const int rhsid[7] = {AXB_GF_densrhs, AXB_GF_momxrhs, AXB_GF_momyrhs,
+                        AXB_GF_momzrhs, AXB_GF_taurhs,  AXB_GF_DYe_rhs,
+                        AXB_GF_DEntrhs};
+  for (int q = 0; q < 7; ++q) {
+    a.acc[q] = f->gf[accid[q]];
+    a.rhs[q] = f->gf[rhsid[q]];
+  }
+  const int bfid[6] = {AXB_GF_fxBy, AXB_GF_fxBz, AXB_GF_fyBx,
+                       AXB_GF_fyBz, AXB_GF_fzBx, AXB_GF_fzBy};
+  for (int q = 0; q < 6; ++q)
+    a.bflux[q] = f->gf[bfid[q]];
+  const int auxid[7] = {AXB_GF_Fx, AXB_GF_Fy, AXB_GF_Fz, AXB_GF_Fbetax,
+                        AXB_GF_Fbetay, AXB_GF_Fbetaz, AXB_GF_G};
+  for (int q = 0; q < 7; ++q)
+    a.aux[q] = f->gf[auxid[q]];
+  a.Arhs[0] = GFP(Avec_x_rhs);
+  a.Arhs[1] = GFP(Avec_y_rhs);
+  a.Arhs[2] = GFP(Avec_z_rhs);
+  a.Psi_rhs = GFP(Psi_rhs);
+  a.rp = recon_params(*p);
+  a.recon_lo = p->loworder_method;
+  a.flux_type = p->flux_type;
+  a.gauge = p->vector_potential_gauge;
+  a.fd_order = p->local_spatial_order;
+  a.lorenz_damp_fac = p->lorenz_damp_fac;
+  a.write_bflux = 1;
+  a.status = c->status;
+  // every pointer the group reads or writes must be present
+  const void *req[] = {a.rho, a.vel[0], a.vel[1], a.vel[2], a.eps, a.press,
+                       a.Ye, a.entropy, a.Bvec[0], a.Bvec[1], a.Bvec[2],
+                       a.dBstag[0], a.dBstag[1], a.dBstag[2], a.alp, a.beta[0],
+                       a.beta[1], a.beta[2], a.Avec[0], a.Avec[1], a.Avec[2],
+                       a.Psi, a.Arhs[0], a.Arhs[1], a.Arhs[2], a.Psi_rhs};
+  for (const void *q : req)
+    if (!q)
+      return AXB_ERR_ARG;
+  for (int q = 0; q < 6; ++q)
+    if (!a.g[q] || !a.K[q] || !a.bflux[q])
+      return AXB_ERR_ARG;
+  for (int q = 0; q < 7; ++q)
+    if (!a.acc[q] || !a.rhs[q] || !a.aux[q])
+      return AXB_ERR_ARG;
+  return AXB_OK;
+}
+} // namespace
+
+namespace axb {
+int launch_flux_pass(int dir, int recon, const RhsArgs &a, const axb_eos &eos,
+                     int seglen, cudaStream_t s) {
+  switch (recon) {
+  case AXB_RECON_PPM: return launch_flux_ppm(dir, a, eos, seglen, s);
+  case AXB_RECON_WENOZ: return launch_flux_wenoz(dir, a, eos, seglen, s);
+  case AXB_RECON_MP5: return launch_flux_mp5(dir, a, eos, seglen, s);
+  default: return launch_flux_low(recon, dir, a, eos, seglen, s);
+  }
+}
+} // namespace axb
+
+// AsterX_RHSGroup (AsterX/schedule.ccl:169-228): AsterX_Fluxes
+// (fluxes.cxx:828-878), AsterX_SourceTerms (source.cxx:170-185) and
+// AsterX_RHS (rhs.cxx:18-253) on one box.  Writes densrhs..DEntrhs,
+// Avec_*_rhs and Psi_rhs on the interior; uses the scratch grid functions
+// acc_*, fxBy..fzBy and Fx..G.  Asynchronous on `stream`.
+AXB_API int axb_rhs_group(axb_ctx *c, const axb_box *box, const axb_fields *f,
+                          const axb_params *p, const axb_eos *eos, void *stream) {
+  if (!c || !eos)
+    return AXB_ERR_ARG;
+  RhsArgs a;
+  int rc = fill_rhs_args(c, box, f, p, a);
+  if (rc)
+    return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int seglen = 32;
+  if ((rc = launch_rhs_misc(p->local_spatial_order == 4 ? 1 : 0, a, s)))
+    return rc;
+  for (int dir = 0; dir < 3; ++dir)
+    if ((rc = launch_flux_pass(dir, p->reconstruction_method, a, *eos, seglen, s)))
+      return rc;
+  if ((rc = launch_rhs_misc(2, a, s)))
+    return rc;
+  return launch_rhs_misc(3, a, s);
+}
+
+namespace axb {
+// 0: sources FD2, 1: sources FD4, 2: aux, 3: CT + Psi
+int launch_rhs_misc(int which, const RhsArgs &a, cudaStream_t s) {
+  const BoxDev &b = a.b;
+  const int T = 128;
+  if (which <= 1) {
+    const dim3 grid((b.n[0] + T - 1) / T, b.n[1], b.n[2]);
+    if (which == 0)
+      k_sources<2><<<grid, T, 0, s>>>(a);
+    else
+      k_sources<4><<<grid, T, 0, s>>>(a);
+  } else if (which == 2) {
+    const dim3 grid((b.n[0] + 5 + T - 1) / T, b.n[1] + 5, b.n[2] + 5);
+    k_aux<<<grid, T, 0, s>>>(a);
+  } else {
+    const dim3 grid((b.n[0] + 1 + T - 1) / T, b.n[1] + 1, b.n[2] + 1);
+    k_ct_psi<<<grid, T, 0, s>>>(a);
+  }
+  return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+}
+} // namespace axb
+
+extern "C" int axb_con2prim_group(axb_ctx *, const axb_box *, const axb_fields *,
+                                  const axb_params *, const axb_eos *, void *);
+extern "C" int axb_rk_stage(axb_ctx *, const axb_box *, const axb_fields *,
+                            const axb_fields *, const axb_fields *,
+                            const axb_fields *, double, double, double, double,
+                            void *);
+extern "C" int axb_sync_periodic(axb_ctx *, const axb_box *, const axb_fields *,
+                                 const int *, int, void *);
+
+// One Runge-Kutta substep of one box: the RHS group, the stage update
+//   U_k <- alpha U_n + beta U_k + gamma dt RHS(U_k),
+// a periodic ghost fill of the evolved variables (when `periodic`), the
+// post-step group (curl A, dB, con2prim) and a periodic ghost fill of the
+// primitives.  `f` holds U_k (updated in place), the primitives and the
+// scratch; `fn` holds U_n (only its 11 evolved grid functions are read).
+// Graph-capturable: no allocation and no host synchronisation.
+AXB_API int axb_substep(axb_ctx *c, const axb_box *box, const axb_fields *f,
+                        const axb_fields *fn, const axb_params *p,
+                        const axb_eos *eos, double alpha, double beta,
+                        double gamma, double dt, int periodic, void *stream) {
+  int rc = axb_rhs_group(c, box, f, p, eos, stream);
+  if (rc)
+    return rc;
+  if ((rc = axb_rk_stage(c, box, f, fn, f, f, alpha, beta, gamma, dt, stream)))
+    return rc;
+  if (periodic) {
+    static const int evolved[] = {AXB_GF_dens,   AXB_GF_momx,   AXB_GF_momy,
+                                  AXB_GF_momz,   AXB_GF_tau,    AXB_GF_DYe,
+                                  AXB_GF_DEnt,   AXB_GF_Avec_x, AXB_GF_Avec_y,
+                                  AXB_GF_Avec_z, AXB_GF_Psi};
+    if ((rc = axb_sync_periodic(c, box, f, evolved, 11, stream)))
+      return rc;
+  }
+  if ((rc = axb_con2prim_group(c, box, f, p, eos, stream)))
+    return rc;
+  if (periodic) {
+    static const int prims[] = {AXB_GF_rho,   AXB_GF_velx,    AXB_GF_vely,
+                                AXB_GF_velz,  AXB_GF_eps,     AXB_GF_press,
+                                AXB_GF_temperature, AXB_GF_Ye, AXB_GF_entropy,
+                                AXB_GF_Bvecx, AXB_GF_Bvecy,   AXB_GF_Bvecz};
+    if ((rc = axb_sync_periodic(c, box, f, prims, 12, stream)))
+      return rc;
+  }
+  return AXB_OK;
+}

@@ -1,0 +1,507 @@
+// PostStep group (AsterX_Con2PrimGroup, AsterX/schedule.ccl:119-165):
+// curl A -> dB_stag, face-to-cell dB, and the con2prim driver with its
+// Noble -> Palenzuela -> atmosphere cascade (AsterX/src/con2prim.cxx:73-454).
+// Also the RK stage update and the periodic ghost fill of one box.
+#include <cmath>
+#include <cstring>
+
+#include "axb_c2p.cuh"
+#include "axb_internal.hxx"
+
+using namespace axb;
+
+namespace axb {
+
+struct C2PBoxArgs {
+  BoxDev b;
+  // inputs / outputs (all cell-centred unless noted)
+  const double *Avec[3];   // edges
+  double *dBstag[3];       // faces
+  const double *alp, *g[6];
+  double *dens, *mom[3], *tau, *DYe, *DEnt, *dB[3];
+  double *rho, *vel[3], *eps, *press, *temperature, *Ye, *entropy, *Bvec[3];
+  double *saved_rho, *saved_vel[3], *saved_eps, *saved_Ye;
+  double *zvec[3], *svec[3], *flag;
+  // settings
+  C2PParams cp;
+  int c2p_prime, c2p_second, excise, thermal_eos_atmo, use_press_atmo;
+  int atmo_uniform;
+  Atmo atmo_const; // when atmo_uniform
+  double rho_abs_min, r_atmo, n_rho_atmo, p_atmo, n_press_atmo, t_atmo,
+      n_temp_atmo, Ye_atmo, atmo_tol;
+  double gamma_noble, Zmin;
+  EosPoly poly;
+  int want_hist;
+  DevStatus *status;
+};
+
+// ComputeStaggeredB<dir> (AsterX/src/computeBfromA.cxx:20-56) on the faces
+// [ng, ng+n] along d and [ng-1, ng+n] across (one ghost layer, which the next
+// RHS needs and the reference obtains by SYNC).
+__global__ void __launch_bounds__(128) k_bstag(const C2PBoxArgs a) {
+  const BoxDev &b = a.b;
+  const int ng = b.ng;
+  const int i = ng - 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = ng - 1 + blockIdx.y;
+  const int k = ng - 1 + blockIdx.z;
+  if (i > ng + b.n[0])
+    return;
+  const long long I = b.at(i, j, k);
+  const long long ipjk = I + 1, ijpk = I + b.sy, ijkp = I + b.sz;
+  const double *Ax = a.Avec[0], *Ay = a.Avec[1], *Az = a.Avec[2];
+  const bool in_i = i >= ng && i <= ng + b.n[0];
+  const bool in_j = j >= ng && j <= ng + b.n[1];
+  const bool in_k = k >= ng && k <= ng + b.n[2];
+  // x-faces: vertex in x, cells in y, z
+  if (in_i && j <= ng + b.n[1] && k <= ng + b.n[2])
+    a.dBstag[0][I] = b.idx[1] * (Az[ijpk] - Az[I]) - b.idx[2] * (Ay[ijkp] - Ay[I]);
+  if (in_j && i <= ng + b.n[0] && k <= ng + b.n[2])
+    a.dBstag[1][I] = b.idx[2] * (Ax[ijkp] - Ax[I]) - b.idx[0] * (Az[ipjk] - Az[I]);
+  if (in_k && i <= ng + b.n[0] && j <= ng + b.n[1])
+    a.dBstag[2][I] = b.idx[0] * (Ay[ipjk] - Ay[I]) - b.idx[1] * (Ax[ijpk] - Ax[I]);
+}
+
+template <class EOS>
+AXB_D Atmo cell_atmosphere(const C2PBoxArgs &a, const EOS &eos, double x,
+                           double y, double z) {
+  // graded atmosphere (con2prim.cxx:81-133)
+  const double r = sqrt(x * x + y * y + z * z);
+  double rho_atm = (r > a.r_atmo) ? (a.rho_abs_min * pow((a.r_atmo / r), a.n_rho_atmo))
+                                  : a.rho_abs_min;
+  rho_atm = fmax(eos.rgrho.min, rho_atm);
+  double press_atm, eps_atm, temp_atm = 0.0;
+  if (a.thermal_eos_atmo) {
+    if (a.use_press_atmo) {
+      press_atm = (r > a.r_atmo) ? (a.p_atmo * pow(a.r_atmo / r, a.n_press_atmo)) : a.p_atmo;
+      press_atm = fmax(eos.press_from_valid_rho_temp_ye(rho_atm, eos.rgtemp.min, a.Ye_atmo),
+                       press_atm);
+      eps_atm = eos.eps_from_valid_rho_press_ye(rho_atm, press_atm, a.Ye_atmo);
+      temp_atm = eos.temp_from_valid_rho_eps_ye(rho_atm, eps_atm, a.Ye_atmo);
+    } else {
+      temp_atm = (r > a.r_atmo) ? (a.t_atmo * pow(a.r_atmo / r, a.n_temp_atmo)) : a.t_atmo;
+      temp_atm = fmax(eos.rgtemp.min, temp_atm);
+      press_atm = eos.press_from_valid_rho_temp_ye(rho_atm, temp_atm, a.Ye_atmo);
+      eps_atm = eos.eps_from_valid_rho_temp_ye(rho_atm, temp_atm, a.Ye_atmo);
+    }
+  } else {
+    const double gm1 = a.poly.gm1_from_valid_rho(rho_atm);
+    eps_atm = a.poly.sed_from_valid_gm1(gm1);
+    eps_atm = fmin(fmax(eos.rgeps.min, eps_atm), eos.rgeps.max);
+    press_atm = eos.press_from_valid_rho_eps_ye(rho_atm, eps_atm, a.Ye_atmo);
+  }
+  const double entropy_atm = eos.kappa_from_valid_rho_eps_ye(rho_atm, eps_atm, a.Ye_atmo);
+  return Atmo{rho_atm, eps_atm, a.Ye_atmo, press_atm, temp_atm, entropy_atm,
+              rho_atm * (1 + a.atmo_tol)};
+}
+
+template <class EOS>
+AXB_D void run_solver(int which, const EOS &eos, const C2PBoxArgs &a,
+                      const Atmo &atmo, Prim &pv, Prim &seeds, Cons &cv,
+                      const sym3 &glo, Report &rep) {
+  if (which == AXB_C2P_NOBLE)
+    noble_solve(eos, a.cp, atmo, a.gamma_noble, a.Zmin, pv, seeds, cv, glo, rep);
+  else if (which == AXB_C2P_PALENZUELA)
+    palenzuela_solve(eos, a.cp, atmo, pv, cv, glo, rep);
+}
+
+// One cell of AsterX_Con2Prim_typeEoS (con2prim.cxx:81-453), preceded by
+// AsterX_ComputedBFromdBstag (computeBfromA.cxx:67-85) for the same cell.
+template <class EOS>
+__global__ void __launch_bounds__(128) k_c2p_box(const C2PBoxArgs a, const EOS eos) {
+  __shared__ unsigned int s_hist[64];
+  const BoxDev &b = a.b;
+  if (a.want_hist) {
+    for (int q = threadIdx.x; q < 64; q += blockDim.x)
+      s_hist[q] = 0;
+    __syncthreads();
+  }
+  const int i = b.ng + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = b.ng + blockIdx.y;
+  const int k = b.ng + blockIdx.z;
+  int iters_first = -1;
+  bool failed = false;
+  if (i < b.ng + b.n[0]) {
+    const long long I = b.at(i, j, k);
+    double dB[3];
+    dB[0] = 0.5 * (a.dBstag[0][I] + a.dBstag[0][I + 1]);
+    dB[1] = 0.5 * (a.dBstag[1][I] + a.dBstag[1][I + b.sy]);
+    dB[2] = 0.5 * (a.dBstag[2][I] + a.dBstag[2][I + b.sz]);
+    Atmo atmo;
+    if (a.atmo_uniform) {
+      atmo = a.atmo_const;
+    } else {
+      const double x = b.xmin[0] + (i - b.ng + 0.5) * b.dx[0];
+      const double y = b.xmin[1] + (j - b.ng + 0.5) * b.dx[1];
+      const double z = b.xmin[2] + (k - b.ng + 0.5) * b.dx[2];
+      atmo = cell_atmosphere(a, eos, x, y, z);
+    }
+    // vertex-to-cell metric (aster_interp.hxx:23-36)
+    auto v2c = [&](const double *f) {
+      double s = 0.0;
+      s += f[I];
+      s += f[I + 1];
+      s += f[I + b.sy];
+      s += f[I + 1 + b.sy];
+      s += f[I + b.sz];
+      s += f[I + 1 + b.sz];
+      s += f[I + b.sy + b.sz];
+      s += f[I + 1 + b.sy + b.sz];
+      return s / 8.0;
+    };
+    const double alp_avg = v2c(a.alp);
+    const sym3 glo{v2c(a.g[0]), v2c(a.g[1]), v2c(a.g[2]),
+                   v2c(a.g[3]), v2c(a.g[4]), v2c(a.g[5])};
+    double mask_local = 1.0;
+    const double spatial_detg = det3(glo);
+    const double sqrt_detg = sqrt(spatial_detg);
+    double v_up[3] = {a.saved_vel[0][I], a.saved_vel[1][I], a.saved_vel[2][I]};
+    double v_low[3];
+    lower3(glo, v_up, v_low);
+    double zsq;
+    const double vsq = dot3(v_low, v_up);
+    if (vsq >= 1.0) {
+      const double wlim = sqrt(1.0 + a.cp.vw_lim * a.cp.vw_lim);
+      const double vlim = a.cp.vw_lim / wlim;
+      for (int q = 0; q < 3; ++q) {
+        v_up[q] *= vlim / sqrt(vsq);
+        v_low[q] *= vlim / sqrt(vsq);
+      }
+      zsq = a.cp.vw_lim * a.cp.vw_lim;
+    } else {
+      zsq = vsq / (1.0 - vsq);
+    }
+    double wlor = sqrt(1.0 + zsq);
+    Cons cv;
+    cv.dens = a.dens[I];
+    for (int q = 0; q < 3; ++q)
+      cv.mom[q] = a.mom[q][I];
+    cv.tau = a.tau[I];
+    cv.DYe = a.DYe[I];
+    cv.DEnt = a.DEnt[I];
+    for (int q = 0; q < 3; ++q)
+      cv.dBvec[q] = dB[q];
+    const double Bup[3] = {cv.dBvec[0] / sqrt_detg, cv.dBvec[1] / sqrt_detg,
+                           cv.dBvec[2] / sqrt_detg};
+    Prim pv;
+    pv.set_nan();
+    Prim seeds;
+    seeds.rho = a.saved_rho[I];
+    seeds.eps = a.saved_eps[I];
+    seeds.Ye = a.saved_Ye[I];
+    seeds.press = eos.press_from_valid_rho_eps_ye(seeds.rho, seeds.eps, seeds.Ye);
+    seeds.temperature = a.temperature[I];
+    seeds.entropy = 0.0; // only read by the excision path, filled there
+    for (int q = 0; q < 3; ++q) {
+      seeds.vel[q] = v_up[q];
+      seeds.Bvec[q] = Bup[q];
+      seeds.E[q] = 0.0;
+    }
+    seeds.w_lor = wlor;
+    bool flag_local = true;
+    int code = AXB_C2P_INIT;
+    bool call_c2p = true;
+    if (cv.dens <= sqrt_detg * atmo.rho_cut) {
+      for (int q = 0; q < 3; ++q)
+        pv.Bvec[q] = Bup[q];
+      atmo.set(pv, cv, glo);
+      atmo.set(seeds);
+      code = AXB_C2P_ATMO;
+      call_c2p = false;
+    }
+    if (alp_avg < a.cp.alp_thresh)
+      mask_local = 0.0;
+    if (a.excise && mask_local != 1.0) {
+      seeds.entropy = eos.kappa_from_valid_rho_eps_ye(seeds.rho, seeds.eps, seeds.Ye);
+      bh_interior<false>(eos, a.cp, atmo, seeds, cv, glo);
+      pv = seeds;
+      call_c2p = false;
+    }
+    cons_floors(cv, glo);
+    if (call_c2p) {
+      Report r1, r2;
+      code = AXB_C2P_PRIME;
+      run_solver(a.c2p_prime, eos, a, atmo, pv, seeds, cv, glo, r1);
+      iters_first = r1.iters;
+      if (r1.failed()) {
+        code = AXB_C2P_SECOND;
+        run_solver(a.c2p_second, eos, a, atmo, pv, seeds, cv, glo, r2);
+      }
+      if (r1.failed() && r2.failed()) {
+        flag_local = false;
+        code = AXB_C2P_FAIL;
+        failed = true;
+        if (mask_local != 1.0) {
+          bh_interior<false>(eos, a.cp, atmo, seeds, cv, glo);
+          pv = seeds;
+        } else {
+          for (int q = 0; q < 3; ++q) {
+            cv.dBvec[q] = sqrt_detg * Bup[q];
+            pv.Bvec[q] = Bup[q];
+          }
+          atmo.set(pv, cv, glo);
+        }
+      }
+      if ((mask_local != 1.0) && flag_local)
+        bh_interior<true>(eos, a.cp, atmo, pv, cv, glo);
+    }
+    a.flag[I] = code;
+    a.rho[I] = pv.rho;
+    a.eps[I] = pv.eps;
+    a.Ye[I] = pv.Ye;
+    a.press[I] = pv.press;
+    a.temperature[I] = pv.temperature;
+    a.entropy[I] = pv.entropy;
+    for (int q = 0; q < 3; ++q) {
+      a.vel[q][I] = pv.vel[q];
+      a.Bvec[q][I] = pv.Bvec[q];
+    }
+    wlor = pv.w_lor;
+    const double hW2 = (pv.rho + pv.rho * pv.eps + pv.press) * wlor * wlor;
+    for (int q = 0; q < 3; ++q) {
+      if (a.zvec[q])
+        a.zvec[q][I] = wlor * pv.vel[q];
+      if (a.svec[q])
+        a.svec[q][I] = hW2 * pv.vel[q];
+    }
+    a.dens[I] = cv.dens;
+    for (int q = 0; q < 3; ++q)
+      a.mom[q][I] = cv.mom[q];
+    a.tau[I] = cv.tau;
+    a.DYe[I] = cv.DYe;
+    a.DEnt[I] = cv.DEnt;
+    for (int q = 0; q < 3; ++q)
+      if (a.dB[q])
+        a.dB[q][I] = cv.dBvec[q];
+    a.saved_rho[I] = pv.rho;
+    for (int q = 0; q < 3; ++q)
+      a.saved_vel[q][I] = pv.vel[q];
+    a.saved_eps[I] = pv.eps;
+    a.saved_Ye[I] = pv.Ye;
+  }
+  const unsigned nfail = __popc(__ballot_sync(0xffffffffu, failed));
+  if (nfail && (threadIdx.x % 32) == 0) {
+    atomicAdd(&a.status->c2p_fail_count, nfail);
+    atomicOr(&a.status->error_word, AXB_EW_C2P_FAIL);
+  }
+  if (a.want_hist) {
+    if (iters_first >= 0)
+      atomicAdd(&s_hist[min(iters_first, 63)], 1u);
+    __syncthreads();
+    for (int q = threadIdx.x; q < 64; q += blockDim.x)
+      if (s_hist[q])
+        atomicAdd(&a.status->c2p_iter_hist[q], (unsigned long long)s_hist[q]);
+  }
+}
+
+} // namespace axb
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+namespace {
+
+int check_box_c2p(const axb_box *b) {
+  if (!b)
+    return AXB_ERR_ARG;
+  for (int d = 0; d < 3; ++d)
+    if (b->n[d] < 1 || !(b->dx[d] > 0))
+      return AXB_ERR_ARG;
+  if (b->ng < 1)
+    return AXB_ERR_GHOSTS;
+  if (b->sy < b->n[0] + 2 * b->ng + 1 || b->sz < b->sy * (b->n[1] + 2 * b->ng + 1))
+    return AXB_ERR_ARG;
+  return AXB_OK;
+}
+
+C2PParams make_c2p_params(const axb_params &p) {
+  C2PParams c;
+  c.maxIter = p.max_iter;
+  c.tol = p.c2p_tol;
+  // c2p_1DPalenzuela.hxx:388-390, evaluated with the host libm like the
+  // reference CPU build
+  c.minbits = int(std::abs(std::log(p.c2p_tol)) / std::log(2.0));
+  c.tolerance_0 = std::ldexp(1.0, -c.minbits);
+  c.alp_thresh = p.alp_thresh;
+  c.cons_error = p.cons_error_limit;
+  c.vw_lim = p.vw_lim;
+  c.w_lim = std::sqrt(1.0 + p.vw_lim * p.vw_lim);
+  c.v_lim = p.vw_lim / c.w_lim;
+  c.Bsq_lim = p.B_lim * p.B_lim;
+  c.rho_BH = p.rho_BH;
+  c.eps_BH = p.eps_BH;
+  c.vwlim_BH = p.vwlim_BH;
+  c.ye_lenient = p.Ye_lenient;
+  c.use_zprim = p.use_z;
+  c.use_temp = p.use_temperature;
+  c.use_press_atmo = p.use_press_atmo;
+  return c;
+}
+
+#define GFP(name) (f->gf[AXB_GF_##name])
+
+template <class EOS>
+Atmo host_atmosphere(const C2PBoxArgs &a, const EOS &eos) {
+  double rho_atm = std::fmax(eos.rgrho.min, a.rho_abs_min);
+  double press_atm, eps_atm, temp_atm = 0.0;
+  if (a.thermal_eos_atmo) {
+    if (a.use_press_atmo) {
+      press_atm = std::fmax(eos.press_from_valid_rho_temp_ye(rho_atm, eos.rgtemp.min, a.Ye_atmo),
+                            a.p_atmo);
+      eps_atm = eos.eps_from_valid_rho_press_ye(rho_atm, press_atm, a.Ye_atmo);
+      temp_atm = eos.temp_from_valid_rho_eps_ye(rho_atm, eps_atm, a.Ye_atmo);
+    } else {
+      temp_atm = std::fmax(eos.rgtemp.min, a.t_atmo);
+      press_atm = eos.press_from_valid_rho_temp_ye(rho_atm, temp_atm, a.Ye_atmo);
+      eps_atm = eos.eps_from_valid_rho_temp_ye(rho_atm, temp_atm, a.Ye_atmo);
+    }
+  } else {
+    const double gm1 = a.poly.gm1_from_valid_rho(rho_atm);
+    eps_atm = a.poly.sed_from_valid_gm1(gm1);
+    eps_atm = std::fmin(std::fmax(eos.rgeps.min, eps_atm), eos.rgeps.max);
+    press_atm = eos.press_from_valid_rho_eps_ye(rho_atm, eps_atm, a.Ye_atmo);
+  }
+  const double entropy_atm = eos.kappa_from_valid_rho_eps_ye(rho_atm, eps_atm, a.Ye_atmo);
+  return Atmo{rho_atm, eps_atm, a.Ye_atmo, press_atm, temp_atm, entropy_atm,
+              rho_atm * (1 + a.atmo_tol)};
+}
+
+int fill_c2p_args(axb_ctx *c, const axb_box *box, const axb_fields *f,
+                  const axb_params *p, const axb_eos *eos, C2PBoxArgs &a) {
+  int rc = check_box_c2p(box);
+  if (rc)
+    return rc;
+  if (!f || !p || !eos)
+    return AXB_ERR_ARG;
+  const bool ok_solver = [](int s) {
+    return s == AXB_C2P_NOBLE || s == AXB_C2P_PALENZUELA;
+  }(p->c2p_prime);
+  if (!ok_solver || p->use_entropy_fix || p->use_mask ||
+      !(p->c2p_second == AXB_C2P_NOBLE || p->c2p_second == AXB_C2P_PALENZUELA ||
+        p->c2p_second == AXB_C2P_NONE))
+    return AXB_ERR_UNSUPPORTED;
+  if (!(p->c2p_tol > 0) || p->max_iter < 1)
+    return AXB_ERR_ARG;
+  a.b = make_box(*box);
+  a.Avec[0] = GFP(Avec_x);
+  a.Avec[1] = GFP(Avec_y);
+  a.Avec[2] = GFP(Avec_z);
+  a.dBstag[0] = GFP(dBx_stag);
+  a.dBstag[1] = GFP(dBy_stag);
+  a.dBstag[2] = GFP(dBz_stag);
+  a.alp = GFP(alp);
+  const int gid[6] = {AXB_GF_gxx, AXB_GF_gxy, AXB_GF_gxz, AXB_GF_gyy, AXB_GF_gyz, AXB_GF_gzz};
+  for (int q = 0; q < 6; ++q)
+    a.g[q] = f->gf[gid[q]];
+  a.dens = GFP(dens);
+  a.mom[0] = GFP(momx);
+  a.mom[1] = GFP(momy);
+  a.mom[2] = GFP(momz);
+  a.tau = GFP(tau);
+  a.DYe = GFP(DYe);
+  a.DEnt = GFP(DEnt);
+  a.dB[0] = GFP(dBx);
+  a.dB[1] = GFP(dBy);
+  a.dB[2] = GFP(dBz);
+  a.rho = GFP(rho);
+  a.vel[0] = GFP(velx);
+  a.vel[1] = GFP(vely);
+  a.vel[2] = GFP(velz);
+  a.eps = GFP(eps);
+  a.press = GFP(press);
+  a.temperature = GFP(temperature);
+  a.Ye = GFP(Ye);
+  a.entropy = GFP(entropy);
+  a.Bvec[0] = GFP(Bvecx);
+  a.Bvec[1] = GFP(Bvecy);
+  a.Bvec[2] = GFP(Bvecz);
+  a.saved_rho = GFP(saved_rho);
+  a.saved_vel[0] = GFP(saved_velx);
+  a.saved_vel[1] = GFP(saved_vely);
+  a.saved_vel[2] = GFP(saved_velz);
+  a.saved_eps = GFP(saved_eps);
+  a.saved_Ye = GFP(saved_Ye);
+  a.zvec[0] = GFP(zvec_x);
+  a.zvec[1] = GFP(zvec_y);
+  a.zvec[2] = GFP(zvec_z);
+  a.svec[0] = GFP(svec_x);
+  a.svec[1] = GFP(svec_y);
+  a.svec[2] = GFP(svec_z);
+  a.flag = GFP(con2prim_flag);
+  const void *req[] = {a.Avec[0], a.Avec[1], a.Avec[2], a.dBstag[0], a.dBstag[1],
+                       a.dBstag[2], a.alp, a.dens, a.mom[0], a.mom[1], a.mom[2],
+                       a.tau, a.DYe, a.DEnt, a.rho, a.vel[0], a.vel[1], a.vel[2],
+                       a.eps, a.press, a.temperature, a.Ye, a.entropy, a.Bvec[0],
+                       a.Bvec[1], a.Bvec[2], a.saved_rho, a.saved_vel[0],
+                       a.saved_vel[1], a.saved_vel[2], a.saved_eps, a.saved_Ye,
+                       a.flag};
+  for (const void *q : req)
+    if (!q)
+      return AXB_ERR_ARG;
+  for (int q = 0; q < 6; ++q)
+    if (!a.g[q])
+      return AXB_ERR_ARG;
+  a.cp = make_c2p_params(*p);
+  a.c2p_prime = p->c2p_prime;
+  a.c2p_second = p->c2p_second;
+  a.excise = p->excise;
+  a.thermal_eos_atmo = p->thermal_eos_atmo;
+  a.use_press_atmo = p->use_press_atmo;
+  a.rho_abs_min = p->rho_abs_min;
+  a.r_atmo = p->r_atmo;
+  a.n_rho_atmo = p->n_rho_atmo;
+  a.p_atmo = p->p_atmo;
+  a.n_press_atmo = p->n_press_atmo;
+  a.t_atmo = p->t_atmo;
+  a.n_temp_atmo = p->n_temp_atmo;
+  a.Ye_atmo = p->Ye_atmo;
+  a.atmo_tol = p->atmo_tol;
+  a.poly = eos->poly;
+  a.want_hist = 1;
+  a.status = c->status;
+  // the atmosphere is uniform when no cell lies beyond r_atmo
+  double rmax2 = 0;
+  for (int d = 0; d < 3; ++d) {
+    const double lo = box->xmin[d], hi = box->xmin[d] + box->n[d] * box->dx[d];
+    const double m = std::fmax(std::fabs(lo), std::fabs(hi));
+    rmax2 += m * m;
+  }
+  a.atmo_uniform = std::sqrt(rmax2) <= p->r_atmo;
+  if (eos->kind == 0) {
+    a.gamma_noble = eos->ideal.gamma;
+    a.Zmin = eos->ideal.rgrho.min;
+    if (a.atmo_uniform)
+      a.atmo_const = host_atmosphere(a, eos->ideal);
+  } else {
+    return AXB_ERR_UNSUPPORTED;
+  }
+  return AXB_OK;
+}
+
+} // namespace
+
+// AsterX_Con2PrimGroup on one box (AsterX/schedule.ccl:119-165): replaces
+// AsterX_ComputedBstagFromA (computeBfromA.cxx:58-65),
+// AsterX_ComputedBFromdBstag (computeBfromA.cxx:67-85) and AsterX_Con2Prim
+// (con2prim.cxx:457-502).
+AXB_API int axb_con2prim_group(axb_ctx *c, const axb_box *box,
+                               const axb_fields *f, const axb_params *p,
+                               const axb_eos *eos, void *stream) {
+  if (!c)
+    return AXB_ERR_ARG;
+  C2PBoxArgs a;
+  int rc = fill_c2p_args(c, box, f, p, eos, a);
+  if (rc)
+    return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  const BoxDev &b = a.b;
+  const int T = 128;
+  {
+    const dim3 grid((b.n[0] + 2 + T - 1) / T, b.n[1] + 2, b.n[2] + 2);
+    k_bstag<<<grid, T, 0, s>>>(a);
+  }
+  {
+    const dim3 grid((b.n[0] + T - 1) / T, b.n[1], b.n[2]);
+    k_c2p_box<<<grid, T, 0, s>>>(a, eos->ideal);
+  }
+  return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+}

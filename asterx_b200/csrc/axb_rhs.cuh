@@ -1,0 +1,187 @@
+// Face physics and the RHS kernels of the engine (AsterX_RHSGroup:
+// AsterX_Fluxes + AsterX_SourceTerms + AsterX_RHS).
+//
+// Kernels (one launch each per box, all FP64):
+//   k_flux_pass<DIR>  reconstruct-once + face physics + Riemann flux along
+//                     one direction, marching a pencil segment per thread,
+//                     with the flux divergence carried in registers
+//                     (AsterX/src/fluxes.cxx:216-795, rhs.cxx:107-114,188-207)
+//   k_sources         geometric source terms (AsterX/src/source.cxx:20-168)
+//   k_aux             vertex auxiliaries F, Fbeta, G (fluxes.cxx:798-826)
+//   k_ct_psi          edge E from the face B fluxes (flux-CT), A and Psi RHS
+//                     (rhs.cxx:116-186,209-252)
+#pragma once
+
+#include "axb_common.cuh"
+#include "axb_eos.cuh"
+#include "axb_recon.cuh"
+
+namespace axb {
+
+enum { V_DENS = 0, V_MOMX, V_MOMY, V_MOMZ, V_TAU, V_DYE, V_DENT, NHYDRO };
+
+struct RhsArgs {
+  BoxDev b;
+  const double *rho, *vel[3], *eps, *press, *Ye, *entropy, *Bvec[3];
+  const double *dBstag[3];
+  const double *alp, *beta[3], *g[6], *K[6];
+  const double *Avec[3], *Psi;
+  double *acc[NHYDRO];
+  double *rhs[NHYDRO];
+  double *bflux[6]; // fxBy fxBz fyBx fyBz fzBx fzBy
+  double *aux[7];   // Fx Fy Fz Fbetax Fbetay Fbetaz G
+  double *Arhs[3], *Psi_rhs;
+  ReconParams rp;
+  int recon_lo, flux_type, gauge, fd_order, write_bflux;
+  double lorenz_damp_fac;
+  DevStatus *status;
+};
+
+// ---------------------------------------------------------------------------
+// face metric: v2f averages of the vertex metric (AsterUtils aster_interp.hxx
+// :68-80), determinant, sqrt, and the (dir,dir) element of the inverse
+// ---------------------------------------------------------------------------
+struct FaceMetric {
+  double alp, beta[3];
+  sym3 g;
+  double detg, sqrtg, uinv;
+};
+
+template <int DIR>
+AXB_D double avg_v2f(const double *__restrict__ f, long long I, long long s1,
+                     long long s2) {
+  double a = 0.0;
+  a += __ldg(f + I);
+  a += __ldg(f + I + s1);
+  a += __ldg(f + I + s2);
+  a += __ldg(f + I + s1 + s2);
+  return a / 4.0;
+}
+
+template <int DIR>
+AXB_D FaceMetric face_metric(const RhsArgs &a, long long I) {
+  constexpr int D1 = (DIR + 1) % 3, D2 = (DIR + 2) % 3;
+  const long long s1 = a.b.stride(D1), s2 = a.b.stride(D2);
+  FaceMetric m;
+  m.alp = avg_v2f<DIR>(a.alp, I, s1, s2);
+  for (int i = 0; i < 3; ++i)
+    m.beta[i] = avg_v2f<DIR>(a.beta[i], I, s1, s2);
+  m.g.xx = avg_v2f<DIR>(a.g[0], I, s1, s2);
+  m.g.xy = avg_v2f<DIR>(a.g[1], I, s1, s2);
+  m.g.xz = avg_v2f<DIR>(a.g[2], I, s1, s2);
+  m.g.yy = avg_v2f<DIR>(a.g[3], I, s1, s2);
+  m.g.yz = avg_v2f<DIR>(a.g[4], I, s1, s2);
+  m.g.zz = avg_v2f<DIR>(a.g[5], I, s1, s2);
+  m.detg = det3(m.g);
+  m.sqrtg = sqrt(m.detg);
+  // (dir,dir) element of calc_inv(g, detg)
+  const double idet = 1 / m.detg;
+  if (DIR == 0)
+    m.uinv = (m.g.yy * m.g.zz - m.g.yz * m.g.yz) * idet;
+  else if (DIR == 1)
+    m.uinv = (m.g.xx * m.g.zz - m.g.xz * m.g.xz) * idet;
+  else
+    m.uinv = (m.g.xx * m.g.yy - m.g.xy * m.g.xy) * idet;
+  return m;
+}
+
+// Reconstructed primitive state on one side of a face.  r[] order:
+//   0 rho, 1 entropy, 2 Ye, 3 press, 4 vx, 5 vy, 6 vz, 7 B_{dir+1}, 8 B_{dir+2}
+enum { R_RHO = 0, R_ENT, R_YE, R_PRESS, R_VX, R_VY, R_VZ, R_B1, R_B2, NREC };
+
+struct SideOut {
+  double U[10], F[10]; // conserved and flux: dens momx momy momz tau DYe DEnt Bx By Bz
+  double lam_p, lam_m; // the two distinct fast speeds of this side
+};
+
+// Per-side physics of CalcFlux (fluxes.cxx:357-654) for a v_vec state.
+template <int DIR, class EOS>
+AXB_D void side_physics(const FaceMetric &m, const double *r, double Bdir,
+                        const EOS &eos, SideOut &o) {
+  constexpr int D1 = (DIR + 1) % 3, D2 = (DIR + 2) % 3;
+  const double rho = r[R_RHO], ent = r[R_ENT], ye = r[R_YE], press = r[R_PRESS];
+  double eps = eos.eps_from_valid_rho_press_ye(rho, press, ye);
+  const double vel[3] = {r[R_VX], r[R_VY], r[R_VZ]};
+  double B[3];
+  B[DIR] = Bdir;
+  B[D1] = r[R_B1];
+  B[D2] = r[R_B2];
+  double vlow[3];
+  lower3(m.g, vel, vlow);
+  const double W = 1 / sqrt(1 - dot3(vlow, vel));
+  double vt[3];
+  for (int i = 0; i < 3; ++i)
+    vt[i] = m.alp * vel[i] - m.beta[i];
+  const double alp_b0 = W * dot3(B, vlow);
+  double Blow[3];
+  lower3(m.g, B, Blow);
+  const double B2 = dot3(B, Blow);
+  double blow[3];
+  for (int i = 0; i < 3; ++i)
+    blow[i] = Blow[i] / W + alp_b0 * vlow[i];
+  const double bsq = (B2 + sq(alp_b0)) / sq(W);
+  const double cs = eos.csnd_from_valid_rho_eps_ye(rho, eps, ye);
+  const double cs2 = cs * cs;
+  const double h = 1 + eps + press / rho;
+  const double dens = m.sqrtg * rho * W;
+  const double DEnt = m.sqrtg * rho * W * ent;
+  const double dhW = dens * h * W;
+  const double dhWp = dhW + m.sqrtg * (sq(alp_b0) + B2);
+  const double ppm = press + 0.5 * bsq;
+  const double vtd = vt[DIR];
+  const double alp_sqrtg = m.alp * m.sqrtg;
+  const double BoW = B[DIR] / W;
+  o.U[0] = dens;
+  o.F[0] = dens * vtd;
+  for (int j = 0; j < 3; ++j) {
+    const double mom = dhWp * vlow[j] - m.sqrtg * alp_b0 * blow[j];
+    o.U[1 + j] = mom;
+    o.F[1 + j] = mom * vtd + alp_sqrtg * (ppm * (j == DIR ? 1.0 : 0.0) - blow[j] * BoW);
+  }
+  const double tau = dhW - dens + m.sqrtg * (B2 - ppm);
+  o.U[4] = tau;
+  o.F[4] = tau * vtd + alp_sqrtg * (ppm * vel[DIR] - alp_b0 * BoW);
+  const double DYe = dens * ye;
+  o.U[5] = DYe;
+  o.F[5] = DYe * vtd;
+  o.U[6] = DEnt;
+  o.F[6] = DEnt * vtd;
+  double Bt[3];
+  for (int i = 0; i < 3; ++i)
+    Bt[i] = m.sqrtg * B[i];
+  const double E0 = Bt[1] * vt[2] - Bt[2] * vt[1];
+  const double E1 = Bt[2] * vt[0] - Bt[0] * vt[2];
+  const double E2 = Bt[0] * vt[1] - Bt[1] * vt[0];
+  o.U[7] = Bt[0];
+  o.U[8] = Bt[1];
+  o.U[9] = Bt[2];
+  // flux(Btilde) = unit_dir x E (fluxes.cxx:650-654)
+  if (DIR == 0) {
+    o.F[7] = 0.0;
+    o.F[8] = -E2;
+    o.F[9] = E1;
+  } else if (DIR == 1) {
+    o.F[7] = E2;
+    o.F[8] = 0.0;
+    o.F[9] = -E0;
+  } else {
+    o.F[7] = -E1;
+    o.F[8] = E0;
+    o.F[9] = 0.0;
+  }
+  // fast magnetosonic speeds (eigenvalues.hxx:19-79)
+  const double beta = m.beta[DIR];
+  const double a0 = (bsq + cs2 * h * rho) * (sq(beta) - sq(m.alp) * m.uinv) -
+                    (-1 + cs2) * h * rho * sq(beta - m.alp * vel[DIR]) * sq(W);
+  const double a1 = 2 * beta * (bsq + cs2 * h * rho) -
+                    2 * (-1 + cs2) * h * rho * (beta - m.alp * vel[DIR]) * sq(W);
+  const double a2 = bsq + h * rho * (cs2 + sq(W) - cs2 * sq(W));
+  double det = sq(a1) - 4 * a2 * a0;
+  if (det < 0)
+    det = 0;
+  const double sd = sqrt(det);
+  o.lam_p = ((-a1 + sd) / (2 * a2)) / m.alp;
+  o.lam_m = ((-a1 - sd) / (2 * a2)) / m.alp;
+}
+
+} // namespace axb

@@ -1,0 +1,257 @@
+// Cell, vertex and edge kernels of the RHS group (sources, auxiliaries,
+// flux-CT + gauge).  Included by exactly one translation unit.
+#pragma once
+
+#include "axb_rhs_kernels.cuh"
+
+namespace axb {
+
+// ---------------------------------------------------------------------------
+// k_sources: geometric source terms (AsterX/src/source.cxx:32-167); writes
+// the seven hydro RHS (dens, DEnt, DYe sources are zero).
+// ---------------------------------------------------------------------------
+AXB_D double avg_v2c(const double *__restrict__ f, long long I, long long sy,
+                     long long sz) {
+  double s = 0.0;
+  s += __ldg(f + I);
+  s += __ldg(f + I + 1);
+  s += __ldg(f + I + sy);
+  s += __ldg(f + I + 1 + sy);
+  s += __ldg(f + I + sz);
+  s += __ldg(f + I + 1 + sz);
+  s += __ldg(f + I + sy + sz);
+  s += __ldg(f + I + 1 + sy + sz);
+  return s / 8.0;
+}
+
+// calc_fd_v2c (AsterUtils/src/aster_fd.hxx:49-110): derivative along d of a
+// vertex function, averaged from the four edges of the cell.
+template <int FD>
+AXB_D double fd_v2c(const double *__restrict__ f, long long I, const BoxDev &b,
+                    int d) {
+  const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
+  const long long s = b.stride(d), s1 = b.stride(d1), s2 = b.stride(d2);
+  const double dx = b.dx[d];
+  const long long base[4] = {I, I + s1, I + s2, I + s1 + s2};
+  double e[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const long long J = base[q];
+    if (FD == 2) {
+      e[q] = (__ldg(f + J + s) - __ldg(f + J)) / dx;
+    } else {
+      e[q] = ((1.0 / 24.0) * __ldg(f + J - s) - (27.0 / 24.0) * __ldg(f + J) +
+              (27.0 / 24.0) * __ldg(f + J + s) - (1.0 / 24.0) * __ldg(f + J + 2 * s)) /
+             dx;
+    }
+  }
+  return 0.25 * (e[0] + e[1] + e[2] + e[3]);
+}
+
+template <int FD>
+__global__ void __launch_bounds__(128) k_sources(const RhsArgs a) {
+  const BoxDev &b = a.b;
+  const int i = b.ng + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = b.ng + blockIdx.y;
+  const int k = b.ng + blockIdx.z;
+  if (i >= b.ng + b.n[0])
+    return;
+  const long long I = b.at(i, j, k);
+  const long long sy = b.sy, sz = b.sz;
+  const double alp = avg_v2c(a.alp, I, sy, sz);
+  double beta[3];
+  for (int q = 0; q < 3; ++q)
+    beta[q] = avg_v2c(a.beta[q], I, sy, sz);
+  sym3 g, K;
+  g.xx = avg_v2c(a.g[0], I, sy, sz);
+  g.xy = avg_v2c(a.g[1], I, sy, sz);
+  g.xz = avg_v2c(a.g[2], I, sy, sz);
+  g.yy = avg_v2c(a.g[3], I, sy, sz);
+  g.yz = avg_v2c(a.g[4], I, sy, sz);
+  g.zz = avg_v2c(a.g[5], I, sy, sz);
+  K.xx = avg_v2c(a.K[0], I, sy, sz);
+  K.xy = avg_v2c(a.K[1], I, sy, sz);
+  K.xz = avg_v2c(a.K[2], I, sy, sz);
+  K.yy = avg_v2c(a.K[3], I, sy, sz);
+  K.yz = avg_v2c(a.K[4], I, sy, sz);
+  K.zz = avg_v2c(a.K[5], I, sy, sz);
+  const double detg = det3(g);
+  const double sqrt_detg = sqrt(detg);
+  const sym3 ug = inv3(g, detg);
+  double d_alp[3], d_beta[3][3];
+  sym3 d_g[3];
+  for (int d = 0; d < 3; ++d) {
+    d_alp[d] = fd_v2c<FD>(a.alp, I, b, d);
+    for (int q = 0; q < 3; ++q)
+      d_beta[d][q] = fd_v2c<FD>(a.beta[q], I, b, d);
+    d_g[d].xx = fd_v2c<FD>(a.g[0], I, b, d);
+    d_g[d].xy = fd_v2c<FD>(a.g[1], I, b, d);
+    d_g[d].xz = fd_v2c<FD>(a.g[2], I, b, d);
+    d_g[d].yy = fd_v2c<FD>(a.g[3], I, b, d);
+    d_g[d].yz = fd_v2c<FD>(a.g[4], I, b, d);
+    d_g[d].zz = fd_v2c<FD>(a.g[5], I, b, d);
+  }
+  const double v_up[3] = {a.vel[0][I], a.vel[1][I], a.vel[2][I]};
+  double v_low[3];
+  lower3(g, v_up, v_low);
+  const double w = 1.0 / sqrt(1.0 - dot3(v_low, v_up));
+  const double rho = a.rho[I], eps = a.eps[I], press = a.press[I];
+  const double rhW2 = (rho * (1.0 + eps) + press) * w * w;
+  double vs[3];
+  for (int q = 0; q < 3; ++q)
+    vs[q] = v_up[q] - beta[q] / alp;
+  const double B_up[3] = {a.Bvec[0][I], a.Bvec[1][I], a.Bvec[2][I]};
+  double B_low[3];
+  lower3(g, B_up, B_low);
+  const double bs0 = w * dot3(B_up, v_low) / alp;
+  double bs[3];
+  for (int q = 0; q < 3; ++q)
+    bs[q] = B_up[q] / w + alp * bs0 * vs[q];
+  const double bs2 = (dot3(B_up, B_low) + sq(alp * bs0)) / sq(w);
+  double gb[3], gbs[3], bs_low[3];
+  lower3(g, beta, gb);
+  lower3(g, bs, gbs);
+  for (int q = 0; q < 3; ++q)
+    bs_low[q] = gb[q] * bs0 + gbs[q];
+  const double A = rhW2 + bs2 * sq(w);
+  const double P = press + 0.5 * bs2;
+  const double t00 = (A - P) / sq(alp) - sq(bs0);
+  double t0[3], t0low[3];
+  for (int q = 0; q < 3; ++q) {
+    t0[q] = A * vs[q] / alp + P * beta[q] / sq(alp) - bs0 * bs[q];
+    t0low[q] = A * v_low[q] / alp - bs_low[q] * bs0;
+  }
+  double t[3][3];
+  for (int p = 0; p < 3; ++p)
+    for (int q = 0; q < 3; ++q)
+      t[p][q] = A * vs[p] * vs[q] + P * (ug(p, q) - beta[p] * beta[q] / sq(alp)) -
+                bs[p] * bs[q];
+  double shiftk[3];
+  lower3(K, beta, shiftk);
+  const double ssk = dot3(shiftk, beta);
+  double X[3];
+  for (int q = 0; q < 3; ++q)
+    X[q] = -d_alp[q] + 2.0 * shiftk[q];
+  double Kt = 0.0;
+  for (int p = 0; p < 3; ++p)
+    for (int q = 0; q < 3; ++q)
+      Kt += K(p, q) * t[p][q];
+  const double tau_source = t00 * (ssk - dot3(beta, d_alp)) + dot3(t0, X) + Kt;
+  double ms[3];
+  for (int d = 0; d < 3; ++d) {
+    double nrm = 0.0, c1 = 0.0, c3 = 0.0;
+    for (int p = 0; p < 3; ++p)
+      for (int q = 0; q < 3; ++q) {
+        nrm += d_g[d](p, q) * beta[p] * beta[q];
+        c1 += d_g[d](p, q) * t0[p] * beta[q];
+        c3 += t[p][q] * d_g[d](p, q);
+      }
+    const double c2 = dot3(t0low, d_beta[d]);
+    ms[d] = t00 * (0.5 * nrm - alp * d_alp[d]) + c1 + c2 + 0.5 * c3;
+  }
+  a.rhs[V_DENS][I] = 0.0;
+  a.rhs[V_DENT][I] = 0.0;
+  a.rhs[V_MOMX][I] = alp * sqrt_detg * ms[0];
+  a.rhs[V_MOMY][I] = alp * sqrt_detg * ms[1];
+  a.rhs[V_MOMZ][I] = alp * sqrt_detg * ms[2];
+  a.rhs[V_TAU][I] = alp * sqrt_detg * tau_source;
+  a.rhs[V_DYE][I] = 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// k_aux: vertex auxiliaries of the A/Psi RHS (fluxes.cxx:798-826) on the
+// vertices [ng-2, ng+n+2] (the Psi RHS reads F at +-1 and Fbeta at +-2).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_aux(const RhsArgs a) {
+  const BoxDev &b = a.b;
+  const int i = b.ng - 2 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = b.ng - 2 + blockIdx.y;
+  const int k = b.ng - 2 + blockIdx.z;
+  if (i > b.ng + b.n[0] + 2)
+    return;
+  const long long I = b.at(i, j, k);
+  double Av[3];
+  for (int d = 0; d < 3; ++d) {
+    double s = 0.0;
+    s += a.Avec[d][I];
+    s += a.Avec[d][I - b.stride(d)];
+    Av[d] = s / 2.0;
+  }
+  const sym3 g{a.g[0][I], a.g[1][I], a.g[2][I], a.g[3][I], a.g[4][I], a.g[5][I]};
+  const double be[3] = {a.beta[0][I], a.beta[1][I], a.beta[2][I]};
+  const double detg = det3(g);
+  const double sqrtg = sqrt(detg);
+  const sym3 ug = inv3(g, detg);
+  double Aup[3];
+  lower3(ug, Av, Aup);
+  const double alp = a.alp[I], psi = a.Psi[I];
+  a.aux[0][I] = alp * sqrtg * Aup[0];
+  a.aux[1][I] = alp * sqrtg * Aup[1];
+  a.aux[2][I] = alp * sqrtg * Aup[2];
+  a.aux[3][I] = be[0] * psi;
+  a.aux[4][I] = be[1] * psi;
+  a.aux[5][I] = be[2] * psi;
+  a.aux[6][I] = alp * psi / sqrtg - dot3(be, Av);
+}
+
+// ---------------------------------------------------------------------------
+// k_ct_psi: on every interior vertex (i,j,k): the x-, y-, z-edge starting
+// there (when it is interior) gets Avec_rhs = -E - dG (flux-CT E from the
+// stored face B fluxes, rhs.cxx:171-185), and the vertex gets Psi_rhs
+// (rhs.cxx:227-252).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_ct_psi(const RhsArgs a) {
+  const BoxDev &b = a.b;
+  const int ng = b.ng;
+  const int i = ng + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = ng + blockIdx.y;
+  const int k = ng + blockIdx.z;
+  if (i > ng + b.n[0])
+    return;
+  const long long I = b.at(i, j, k);
+  const int ijk[3] = {i, j, k};
+  const bool gl = a.gauge == AXB_GAUGE_GEN_LORENZ;
+  const double *G = a.aux[6];
+  // bflux: 0 fxBy 1 fxBz 2 fyBx 3 fyBz 4 fzBx 5 fzBy
+  for (int e = 0; e < 3; ++e) {
+    if (ijk[e] >= ng + b.n[e])
+      continue;
+    const int ej = (e + 1) % 3, ek = (e + 2) % 3;
+    // fBs(j)(k): flux along k of B_j; fBs(k)(j): flux along j of B_k
+    const double *fjk, *fkj;
+    if (e == 0) {
+      fjk = a.bflux[5]; // fzBy
+      fkj = a.bflux[3]; // fyBz
+    } else if (e == 1) {
+      fjk = a.bflux[1]; // fxBz
+      fkj = a.bflux[4]; // fzBx
+    } else {
+      fjk = a.bflux[2]; // fyBx
+      fkj = a.bflux[0]; // fxBy
+    }
+    const double E = 0.25 * ((fjk[I] + fjk[I - b.stride(ej)]) -
+                             (fkj[I] + fkj[I - b.stride(ek)]));
+    double r = -E;
+    if (gl)
+      r = -E - (G[I + b.stride(e)] - G[I]) / b.dx[e];
+    a.Arhs[e][I] = r;
+  }
+  if (gl) {
+    double dF = 0.0;
+    for (int d = 0; d < 3; ++d) {
+      const long long s = b.stride(d);
+      const double *F = a.aux[d], *Fb = a.aux[3 + d];
+      const double c2c = (0.5 / b.dx[d]) * (F[I + s] - F[I - s]);
+      const int sg = a.beta[d][I] < 0 ? -1 : 1;
+      const double one =
+          -sg * (Fb[I + 2 * sg * s] - 4.0 * Fb[I + sg * s] + 3.0 * Fb[I]) *
+          (0.5 / b.dx[d]);
+      dF += c2c - one;
+    }
+    a.Psi_rhs[I] = -dF - a.lorenz_damp_fac * a.alp[I] * a.Psi[I];
+  } else {
+    a.Psi_rhs[I] = 0.0;
+  }
+}
+
+} // namespace axb

@@ -1,0 +1,192 @@
+"""Python handle on the engine's C ABI (``include/asterx_b200.h``).
+
+This is the host-side driver used by the tests, ``bench.py`` and
+``__graft_entry__``: it loads the in-tree ``libasterx_b200.so``, keeps device
+buffers as torch CUDA tensors (torch is used only for memory and streams) and
+passes raw pointers to the C entry points.  There is no fallback: if the
+library or a B200 is missing, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .abi import GF, GF_NAMES, NUM_GF, Box, Fields, Layout, Params
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libasterx_b200.so")
+
+_vp = C.c_void_p
+_dp = C.POINTER(C.c_double)
+
+
+class AxbError(RuntimeError):
+    STATUS = {1: "AXB_ERR_ARG", 2: "AXB_ERR_GHOSTS", 3: "AXB_ERR_CUDA",
+              4: "AXB_ERR_UNSUPPORTED", 5: "AXB_ERR_TOO_LARGE",
+              6: "AXB_ERR_NO_DEVICE"}
+
+    def __init__(self, rc, what):
+        super().__init__(f"{what} failed: {self.STATUS.get(rc, rc)}")
+        self.rc = rc
+
+
+def load_library(path=LIB_PATH):
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} is missing: build it with `python -m asterx_b200.build`")
+    lib = C.CDLL(path)
+    lib.axb_params_default.argtypes = [C.POINTER(Params)]
+    lib.axb_gf_name.restype = C.c_char_p
+    lib.axb_gf_name.argtypes = [C.c_int]
+    lib.axb_ctx_create.argtypes = [C.c_int, C.POINTER(_vp)]
+    lib.axb_ctx_destroy.argtypes = [_vp]
+    lib.axb_status_reset.argtypes = [_vp, _vp]
+    lib.axb_status_read.argtypes = [_vp, _vp, C.POINTER(C.c_uint32),
+                                    C.POINTER(C.c_double), C.POINTER(C.c_uint32),
+                                    C.POINTER(C.c_uint64)]
+    lib.axb_eos_create_idealgas.argtypes = [C.c_double, C.c_double, _dp, _dp, _dp,
+                                            C.c_double, C.c_double, C.POINTER(_vp)]
+    lib.axb_eos_destroy.argtypes = [_vp]
+    lib.axb_rhs_group.argtypes = [_vp, C.POINTER(Box), C.POINTER(Fields),
+                                  C.POINTER(Params), _vp, _vp]
+    lib.axb_con2prim_group.argtypes = [_vp, C.POINTER(Box), C.POINTER(Fields),
+                                       C.POINTER(Params), _vp, _vp]
+    lib.axb_rk_stage.argtypes = [_vp, C.POINTER(Box)] + [C.POINTER(Fields)] * 4 + \
+        [C.c_double] * 4 + [_vp]
+    lib.axb_sync_periodic.argtypes = [_vp, C.POINTER(Box), C.POINTER(Fields),
+                                      C.POINTER(C.c_int), C.c_int, _vp]
+    lib.axb_substep.argtypes = [_vp, C.POINTER(Box), C.POINTER(Fields),
+                                C.POINTER(Fields), C.POINTER(Params), _vp,
+                                C.c_double, C.c_double, C.c_double, C.c_double,
+                                C.c_int, _vp]
+    for name in ("axb_con2prim_group", "axb_substep", "axb_rk_stage",
+                 "axb_sync_periodic", "axb_c2p_cells", "axb_eos_create_tabulated"):
+        if hasattr(lib, name):
+            getattr(lib, name).restype = C.c_int
+    return lib
+
+
+class Engine:
+    """One device context of the engine."""
+
+    def __init__(self, device=0, path=LIB_PATH):
+        import torch
+        if not torch.cuda.is_available():
+            raise RuntimeError("the engine needs a CUDA device (sm_100)")
+        self.torch = torch
+        self.device = torch.device("cuda", device)
+        torch.cuda.set_device(self.device)
+        self.lib = load_library(path)
+        self.ctx = _vp()
+        self._check(self.lib.axb_ctx_create(device, C.byref(self.ctx)), "axb_ctx_create")
+        self._eos = []
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise AxbError(rc, what)
+
+    def stream_ptr(self, stream=None):
+        s = stream if stream is not None else self.torch.cuda.current_stream(self.device)
+        return _vp(s.cuda_stream)
+
+    # -- equations of state ---------------------------------------------------
+    def eos_idealgas(self, gamma, umass=1.0, rho=(1e-40, 1.0), eps=(0.0, 2.0),
+                     ye=(0.0, 1.0), poly_gamma=2.0, poly_k=100.0):
+        h = _vp()
+        r = (C.c_double * 2)(*rho)
+        e = (C.c_double * 2)(*eps)
+        y = (C.c_double * 2)(*ye)
+        self._check(self.lib.axb_eos_create_idealgas(
+            gamma, umass, C.cast(r, _dp), C.cast(e, _dp), C.cast(y, _dp),
+            poly_gamma, poly_k, C.byref(h)), "axb_eos_create_idealgas")
+        self._eos.append(h)
+        return h
+
+    # -- memory ---------------------------------------------------------------
+    def upload(self, layout: Layout, fields: dict, names=None):
+        """Device copies (torch float64 tensors) of the given host arrays, plus
+        zero-filled buffers for every other grid function in ``names``."""
+        t = self.torch
+        out = {}
+        for n, a in fields.items():
+            out[n] = t.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(self.device)
+        for n in (names or GF_NAMES):
+            if n not in out:
+                out[n] = t.zeros(layout.size, dtype=t.float64, device=self.device)
+        return out
+
+    @staticmethod
+    def fields_struct(tensors: dict) -> Fields:
+        f = Fields()
+        for n, ten in tensors.items():
+            if n in GF:
+                f.gf[GF[n]] = ten.data_ptr()
+        return f
+
+    # -- routines ---------------------------------------------------------------
+    def rhs_group(self, layout: Layout, tensors: dict, params: Params, eos, stream=None):
+        box = layout.box()
+        f = self.fields_struct(tensors)
+        self._check(self.lib.axb_rhs_group(self.ctx, C.byref(box), C.byref(f),
+                                           C.byref(params), eos,
+                                           self.stream_ptr(stream)), "axb_rhs_group")
+
+    def con2prim_group(self, layout: Layout, tensors: dict, params: Params, eos,
+                       stream=None):
+        box = layout.box()
+        f = self.fields_struct(tensors)
+        self._check(self.lib.axb_con2prim_group(self.ctx, C.byref(box), C.byref(f),
+                                                C.byref(params), eos,
+                                                self.stream_ptr(stream)),
+                    "axb_con2prim_group")
+
+    def rk_stage(self, layout, out, un, uk, rhs, alpha, beta, gamma, dt, stream=None):
+        box = layout.box()
+        fs = [self.fields_struct(t) for t in (out, un, uk, rhs)]
+        self._check(self.lib.axb_rk_stage(self.ctx, C.byref(box), *[C.byref(x) for x in fs],
+                                          alpha, beta, gamma, dt,
+                                          self.stream_ptr(stream)), "axb_rk_stage")
+
+    def sync_periodic(self, layout, tensors, names, stream=None):
+        box = layout.box()
+        f = self.fields_struct(tensors)
+        ids = (C.c_int * len(names))(*[GF[n] for n in names])
+        self._check(self.lib.axb_sync_periodic(self.ctx, C.byref(box), C.byref(f), ids,
+                                               len(names), self.stream_ptr(stream)),
+                    "axb_sync_periodic")
+
+    def substep(self, layout, tensors, tensors_n, params, eos, alpha, beta, gamma, dt,
+                periodic=True, stream=None):
+        box = layout.box()
+        f = self.fields_struct(tensors)
+        fn = self.fields_struct(tensors_n)
+        self._check(self.lib.axb_substep(self.ctx, C.byref(box), C.byref(f), C.byref(fn),
+                                         C.byref(params), eos, alpha, beta, gamma, dt,
+                                         int(periodic), self.stream_ptr(stream)),
+                    "axb_substep")
+
+    def status_reset(self, stream=None):
+        self._check(self.lib.axb_status_reset(self.ctx, self.stream_ptr(stream)),
+                    "axb_status_reset")
+
+    def status(self, stream=None):
+        ew = C.c_uint32()
+        ms = C.c_double()
+        nf = C.c_uint32()
+        hist = (C.c_uint64 * 64)()
+        self._check(self.lib.axb_status_read(self.ctx, self.stream_ptr(stream),
+                                             C.byref(ew), C.byref(ms), C.byref(nf),
+                                             hist), "axb_status_read")
+        return dict(error_word=ew.value, max_speed=ms.value, c2p_fail=nf.value,
+                    iter_hist=np.array(hist[:], dtype=np.int64))
+
+    def close(self):
+        for h in self._eos:
+            self.lib.axb_eos_destroy(h)
+        self._eos = []
+        if self.ctx:
+            self.lib.axb_ctx_destroy(self.ctx)
+            self.ctx = _vp()

@@ -1,0 +1,304 @@
+"""Seeded synthetic inputs for the hot path (numpy, host side).
+
+There is no public dataset for this path: every workload is generated here
+from a seed, with the shapes and value ranges of the configurations it stands
+for.  Nothing here calls the engine; ``bench.py`` and the tests upload the
+arrays themselves.
+
+* ``balsara_box`` -- a uniform patch with the Balsara-1 planar discontinuity
+  (left rho=1, p=1, B=(0.5, 1, 0); right rho=0.125, p=0.1, B=(0.5, -1, 0)),
+  flat metric, seeded relative perturbations of rho and p; B is set through
+  the staggered vector potential A = (0, -Bx z, |x|) whose discrete curl is
+  exactly (Bx, sign, 0).
+* ``curved_box`` -- a periodic patch with a static curved metric
+  (gamma_ij = delta_ij + 0.05 * four seeded symmetric sine modes with
+  wavenumbers 1-4, lapse 1 - 0.05 sin, shift amplitude 0.01, extrinsic
+  curvature from a further sine mode), smooth seeded primitives plus three
+  planar jumps, Lorentz factors up to 10, rho log-uniform in [1e-8, 1],
+  magnetisation b^2/rho roughly log-uniform in [1e-3, 10]; B from the curl
+  of a seeded periodic vector potential.
+* ``c2p_cells`` -- independent cells for the primitive-recovery benchmark.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .abi import Layout
+
+
+def _modes(rng, coords, kmax=4, nmodes=4):
+    """Sum of seeded sine modes, periodic on the unit cube."""
+    x, y, z = coords
+    f = 0.0
+    for _ in range(nmodes):
+        k = rng.integers(1, kmax + 1, size=3) * rng.choice([-1, 1], size=3)
+        ph = rng.uniform(0, 2 * np.pi)
+        f = f + np.sin(2 * np.pi * (k[0] * x + k[1] * y + k[2] * z) + ph)
+    return f / nmodes
+
+
+def flat_metric(L: Layout, f: dict):
+    for n in ("gxy", "gxz", "gyz", "betax", "betay", "betaz", "kxx", "kxy",
+              "kxz", "kyy", "kyz", "kzz"):
+        f[n] = L.zeros()
+    for n in ("gxx", "gyy", "gzz", "alp"):
+        f[n] = np.ones(L.size)
+
+
+def curved_metric(L: Layout, f: dict, rng, amp=0.05, shift_amp=0.01,
+                  curv_amp=0.02):
+    cv = L.coords((0, 0, 0))
+    shape = L.view(L.zeros()).shape
+    diag = {"gxx": 1.0, "gyy": 1.0, "gzz": 1.0, "gxy": 0.0, "gxz": 0.0,
+            "gyz": 0.0}
+    for n, d in diag.items():
+        f[n] = np.broadcast_to(d + amp * _modes(rng, cv), shape).ravel().copy()
+    g = np.stack([f[n] for n in ("gxx", "gxy", "gxz", "gyy", "gyz", "gzz")])
+    m1 = g[0]
+    m2 = g[0] * g[3] - g[1] ** 2
+    det = (g[0] * (g[3] * g[5] - g[4] ** 2) - g[1] * (g[1] * g[5] - g[4] * g[2])
+           + g[2] * (g[1] * g[4] - g[3] * g[2]))
+    assert (m1 > 0).all() and (m2 > 0).all() and (det > 0).all(), \
+        "metric not positive definite"
+    f["alp"] = np.broadcast_to(1.0 - amp * _modes(rng, cv), shape).ravel().copy()
+    for n in ("betax", "betay", "betaz"):
+        f[n] = np.broadcast_to(shift_amp * _modes(rng, cv), shape).ravel().copy()
+    for n in ("kxx", "kxy", "kxz", "kyy", "kyz", "kzz"):
+        f[n] = np.broadcast_to(curv_amp * _modes(rng, cv), shape).ravel().copy()
+
+
+def _curl_stag(L: Layout, Ax, Ay, Az):
+    """Face curl of edge A exactly as AsterX/src/computeBfromA.cxx:32-55, on
+    every face whose neighbours exist."""
+    v = L.view
+    ax, ay, az = v(Ax), v(Ay), v(Az)
+    idx = [1.0 / d for d in L.dx]
+    bx, by, bz = (np.zeros_like(ax) for _ in range(3))
+    bx[:-1, :-1, :] = (idx[1] * (az[:-1, 1:, :] - az[:-1, :-1, :])
+                       - idx[2] * (ay[1:, :-1, :] - ay[:-1, :-1, :]))
+    by[:-1, :, :-1] = (idx[2] * (ax[1:, :, :-1] - ax[:-1, :, :-1])
+                       - idx[0] * (az[:-1, :, 1:] - az[:-1, :, :-1]))
+    bz[:, :-1, :-1] = (idx[0] * (ay[:, :-1, 1:] - ay[:, :-1, :-1])
+                       - idx[1] * (ax[:, 1:, :-1] - ax[:, :-1, :-1]))
+    return bx.ravel(), by.ravel(), bz.ravel()
+
+
+def _v2c(L: Layout, a):
+    """Vertex-to-cell average (the 8 corners, AsterUtils aster_interp.hxx:
+    23-36), defined on every cell whose corners exist."""
+    v = L.view(a)
+    out = np.zeros_like(v)
+    out[:-1, :-1, :-1] = (v[:-1, :-1, :-1] + v[:-1, :-1, 1:] + v[:-1, 1:, :-1]
+                          + v[:-1, 1:, 1:] + v[1:, :-1, :-1] + v[1:, :-1, 1:]
+                          + v[1:, 1:, :-1] + v[1:, 1:, 1:]) / 8.0
+    return out.ravel()
+
+
+def _sqrt_detg_cell(L: Layout, f):
+    g = [_v2c(L, f[n]) for n in ("gxx", "gxy", "gxz", "gyy", "gyz", "gzz")]
+    det = (g[0] * (g[3] * g[5] - g[4] ** 2) - g[1] * (g[1] * g[5] - g[4] * g[2])
+           + g[2] * (g[1] * g[4] - g[3] * g[2]))
+    return np.sqrt(np.where(det > 0, det, 1.0)), g
+
+
+def _finish_prims(L, f, gamma, ye=None):
+    """eps, temperature, entropy (kappa) and Ye from rho and press for an
+    ideal gas (EOSX/src/eos_3p_idealgas/eos_3p_idealgas.hxx:115-229)."""
+    rho, press = f["rho"], f["press"]
+    f["eps"] = press / (rho * (gamma - 1.0))
+    f["temperature"] = (gamma - 1.0) * f["eps"]
+    f["entropy"] = (gamma - 1.0) * f["eps"] * rho ** (1.0 - gamma)
+    f["Ye"] = np.full(L.size, 0.5) if ye is None else ye
+
+
+def _cell_B_from_stag(L, f):
+    v = L.view
+    dB = []
+    for n, ax in (("dBx_stag", 2), ("dBy_stag", 1), ("dBz_stag", 0)):
+        s = v(f[n])
+        c = np.zeros_like(s)
+        if ax == 2:
+            c[:, :, :-1] = 0.5 * (s[:, :, :-1] + s[:, :, 1:])
+        elif ax == 1:
+            c[:, :-1, :] = 0.5 * (s[:, :-1, :] + s[:, 1:, :])
+        else:
+            c[:-1, :, :] = 0.5 * (s[:-1, :, :] + s[1:, :, :])
+        dB.append(c.ravel())
+    sq, _ = _sqrt_detg_cell(L, f)
+    f["dBx"], f["dBy"], f["dBz"] = dB
+    f["Bvecx"], f["Bvecy"], f["Bvecz"] = (d / sq for d in dB)
+
+
+def balsara_box(n=64, ng=3, gamma=5.0 / 3.0, seed=1, pert=1e-3):
+    """Config-1 patch: Balsara-1 discontinuity at x = 0 on [-0.5, 0.5]^3."""
+    if isinstance(n, int):
+        n = (n, n, n)
+    L = Layout(n, ng, tuple(1.0 / v for v in n), (-0.5, -0.5, -0.5))
+    rng = np.random.default_rng(seed)
+    f = {}
+    flat_metric(L, f)
+    xc, _, _ = L.coords((1, 1, 1))
+    shape = L.view(L.zeros()).shape
+    left = np.broadcast_to(xc < 0, shape).ravel()
+    f["rho"] = np.where(left, 1.0, 0.125) * (1 + pert * rng.uniform(-1, 1, L.size))
+    f["press"] = np.where(left, 1.0, 0.1) * (1 + pert * rng.uniform(-1, 1, L.size))
+    for nm in ("velx", "vely", "velz"):
+        f[nm] = L.zeros()
+    _finish_prims(L, f, gamma)
+    # vector potential: A_x = 0, A_y = -Bx z (y-edges: z at vertices),
+    # A_z = |x| (z-edges: x at vertices) -> B = (0.5, +1 for x<0 / -1, 0)
+    xv, yv, zv = L.coords((0, 0, 0))
+    f["Avec_x"] = L.zeros()
+    f["Avec_y"] = np.broadcast_to(-0.5 * zv, shape).ravel().copy()
+    f["Avec_z"] = np.broadcast_to(np.abs(xv), shape).ravel().copy()
+    f["Psi"] = L.zeros()
+    f["dBx_stag"], f["dBy_stag"], f["dBz_stag"] = _curl_stag(
+        L, f["Avec_x"], f["Avec_y"], f["Avec_z"])
+    _cell_B_from_stag(L, f)
+    return L, f
+
+
+def curved_box(n=24, ng=3, gamma=4.0 / 3.0, seed=2, wmax=10.0, njumps=3,
+               with_ye=False, sigma=(1e-3, 10.0), jump=(2.0, 8.0),
+               rho_min=1e-8, theta=(1e-2, 1.0)):
+    """Config-2-like periodic patch on [0, 1]^3 with a curved static metric."""
+    if isinstance(n, int):
+        n = (n, n, n)
+    L = Layout(n, ng, tuple(1.0 / v for v in n), (0.0, 0.0, 0.0))
+    rng = np.random.default_rng(seed)
+    shape = L.view(L.zeros()).shape
+    f = {}
+    curved_metric(L, f, rng)
+    cc = L.coords((1, 1, 1))
+
+    def smooth(lo, hi, kmax=3, nmodes=3):
+        u = 0.5 * (1 + _modes(rng, cc, kmax=kmax, nmodes=nmodes))
+        return np.broadcast_to(lo + (hi - lo) * u, shape).ravel().copy()
+
+    # vector potential on edges, B from its curl
+    ev = {"Avec_x": (1, 0, 0), "Avec_y": (0, 1, 0), "Avec_z": (0, 0, 1)}
+    for nm, cent in ev.items():
+        c = L.coords(cent)
+        f[nm] = np.broadcast_to(0.05 * _modes(rng, c, kmax=3), shape).ravel().copy()
+    f["Psi"] = np.broadcast_to(1e-3 * _modes(rng, L.coords((0, 0, 0))),
+                               shape).ravel().copy()
+    f["dBx_stag"], f["dBy_stag"], f["dBz_stag"] = _curl_stag(
+        L, f["Avec_x"], f["Avec_y"], f["Avec_z"])
+    _cell_B_from_stag(L, f)
+    _, g = _sqrt_detg_cell(L, f)
+
+    # velocity: Lorentz factor in [1, wmax] along a smooth unit direction
+    W = smooth(1.0, wmax, kmax=1, nmodes=2)
+    th = smooth(0.3 * np.pi, 0.7 * np.pi, kmax=1, nmodes=2)
+    ph0 = rng.uniform(0, 2 * np.pi)
+    ph = smooth(ph0, ph0 + 0.5 * np.pi, kmax=1, nmodes=2)
+    d = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)])
+    gd = np.array([[g[0], g[1], g[2]], [g[1], g[3], g[4]], [g[2], g[4], g[5]]])
+    nrm = np.einsum("i...,ij...,j...->...", d, gd, d)
+    nrm = np.where(nrm > 1e-12, nrm, 1.0)
+    vmag = np.sqrt(1.0 - 1.0 / W ** 2)
+    vel = d * (vmag / np.sqrt(nrm))
+    f["velx"], f["vely"], f["velz"] = vel
+    # density from the magnetisation, then planar jumps
+    B = np.stack([f["Bvecx"], f["Bvecy"], f["Bvecz"]])
+    vlow = np.einsum("ij...,j...->i...", gd, vel)
+    Bsq = np.einsum("i...,ij...,j...->...", B, gd, B)
+    vB = np.einsum("i...,i...->...", vlow, B)
+    bsq = Bsq / W ** 2 + vB ** 2
+    sigma = 10 ** smooth(np.log10(sigma[0]), np.log10(sigma[1]))
+    rho = np.clip(bsq / sigma, rho_min, 1.0)
+    theta = 10 ** smooth(np.log10(theta[0]), np.log10(theta[1]))
+    xyz = [np.broadcast_to(c, shape).ravel() for c in cc]
+    for _ in range(njumps):
+        nv = rng.normal(size=3)
+        nv /= np.linalg.norm(nv)
+        x0 = rng.uniform(0.2, 0.8)
+        side = (nv[0] * (xyz[0] - x0) + nv[1] * (xyz[1] - 0.5)
+                + nv[2] * (xyz[2] - 0.5)) > 0
+        rho = np.where(side, rho * rng.uniform(*jump), rho)
+        theta = np.where(side, theta / rng.uniform(1.5, 4), theta)
+    f["rho"] = np.clip(rho, rho_min, 1.0)
+    f["press"] = f["rho"] * theta
+    ye = smooth(0.05, 0.5) if with_ye else None
+    _finish_prims(L, f, gamma, ye)
+    return L, f
+
+
+def saved_from_prims(f):
+    f["saved_rho"] = f["rho"].copy()
+    f["saved_velx"] = f["velx"].copy()
+    f["saved_vely"] = f["vely"].copy()
+    f["saved_velz"] = f["velz"].copy()
+    f["saved_eps"] = f["eps"].copy()
+    f["saved_Ye"] = f["Ye"].copy()
+
+
+def c2p_cells(ncells, seed=4, gamma=5.0 / 3.0, rho_range=(1e-12, 1e-2),
+              eps_range=(1e-6, 10.0), w_range=(1.0, 50.0),
+              sigma_range=(1e-4, 100.0), metric_amp=0.05):
+    """Independent-cell primitive sample for the recovery benchmark:
+    rho, eps log-uniform, W uniform, magnetisation b^2/rho log-uniform,
+    isotropic velocity and field directions, random metric perturbation.
+    Returns dict of 1-D arrays: rho, eps, press, vel (3,N), B (3,N), g (6,N)."""
+    rng = np.random.default_rng(seed)
+    N = int(ncells)
+    lu = lambda a, b: np.exp(rng.uniform(np.log(a), np.log(b), N))
+    rho = lu(*rho_range)
+    eps = lu(*eps_range)
+    W = rng.uniform(*w_range, N)
+    sigma = lu(*sigma_range)
+    g = np.zeros((6, N))
+    g[[0, 3, 5]] = 1.0
+    g += metric_amp * rng.uniform(-1, 1, (6, N))
+    gd = np.array([[g[0], g[1], g[2]], [g[1], g[3], g[4]], [g[2], g[4], g[5]]])
+
+    def unit(n):
+        v = rng.normal(size=(3, n))
+        return v / np.linalg.norm(v, axis=0)
+
+    dv = unit(N)
+    nrm = np.einsum("i...,ij...,j...->...", dv, gd, dv)
+    vel = dv * np.sqrt(1.0 - 1.0 / W ** 2) / np.sqrt(nrm)
+    db = unit(N)
+    # choose |B| so that b^2 = sigma * rho exactly
+    vlow = np.einsum("ij...,j...->i...", gd, vel)
+    Bsq1 = np.einsum("i...,ij...,j...->...", db, gd, db)
+    vB1 = np.einsum("i...,i...->...", vlow, db)
+    b2_per = Bsq1 / W ** 2 + vB1 ** 2
+    B = db * np.sqrt(sigma * rho / b2_per)
+    press = (gamma - 1.0) * rho * eps
+    return dict(rho=rho, eps=eps, press=press, vel=vel, B=B, g=g, W=W)
+
+
+def cons_from_prims(L: Layout, f: dict):
+    """Densitised conserved variables of every cell from its primitives and
+    the vertex-to-cell metric (the Valencia prim->cons map of
+    AsterX/src/prim2con.hxx:38-83), written into f."""
+    sq, g = _sqrt_detg_cell(L, f)
+    gd = np.array([[g[0], g[1], g[2]], [g[1], g[3], g[4]], [g[2], g[4], g[5]]])
+    v = np.stack([f["velx"], f["vely"], f["velz"]])
+    B = np.stack([f["Bvecx"], f["Bvecy"], f["Bvecz"]])
+    vl = np.einsum("ij...,j...->i...", gd, v)
+    Bl = np.einsum("ij...,j...->i...", gd, B)
+    v2 = np.clip(np.einsum("i...,i...->...", vl, v), 0, 1 - 1e-15)
+    W = 1.0 / np.sqrt(1.0 - v2)
+    bst = W * np.einsum("i...,i...->...", B, vl)
+    bl = Bl / W + bst * vl
+    bs2 = (np.einsum("i...,i...->...", B, Bl) + bst * bst) / (W * W)
+    rho, eps, press = f["rho"], f["eps"], f["press"]
+    hW2 = W * W * (rho * (1.0 + eps) + press + bs2)
+    f["dens"] = sq * rho * W
+    mom = sq * (hW2 * vl - bst * bl)
+    f["momx"], f["momy"], f["momz"] = mom
+    f["tau"] = sq * (hW2 - (press + 0.5 * bs2) - bst * bst) - f["dens"]
+    f["DYe"] = f["dens"] * f["Ye"]
+    f["DEnt"] = f["dens"] * f["entropy"]
+
+
+def perturbed_saved(f: dict, seed=7, amp=1e-2):
+    """Saved primitives (the recovery seeds) as the primitives times
+    (1 + amp * U(-1, 1)), as a time step leaves them."""
+    rng = np.random.default_rng(seed)
+    for n, s in (("rho", "saved_rho"), ("velx", "saved_velx"), ("vely", "saved_vely"),
+                 ("velz", "saved_velz"), ("eps", "saved_eps"), ("Ye", "saved_Ye")):
+        f[s] = f[n] * (1 + amp * rng.uniform(-1, 1, f[n].shape))

@@ -1,0 +1,241 @@
+/*
+ * asterx_b200.h -- C ABI of the B200 (sm_100a) GRMHD right-hand-side and
+ * primitive-recovery engine.
+ *
+ * The engine is a drop-in for the scheduled hot path of AsterX (Valencia
+ * GRMHD with a staggered vector potential): the ReconX reconstruction, the
+ * AsterX flux / source / RHS routines with flux-CT and generalised Lorenz
+ * gauge, the curl(A) -> B post-step and the Con2PrimFactory Noble and
+ * Palenzuela recoveries with the EOSX ideal-gas and tabulated3d equations of
+ * state.  Every entry point takes plain pointers and sizes, runs
+ * asynchronously on the caller's CUDA stream, allocates nothing on the hot
+ * path and returns an int status (0 = success, see axb_status).  All
+ * arithmetic is FP64; only the learned c2p guess runs in BF16/FP32.
+ *
+ * Data model (the CarpetX conventions the reference code assumes):
+ *  - A box has n[d] interior cells and ng ghost layers per axis.  Every grid
+ *    function of the box is one FP64 array addressed as
+ *        f[i + sy*j + sz*k],  0 <= i,j,k <= n[d] + 2*ng,
+ *    whatever its centring.  Cell i lies between vertices i and i+1; face i
+ *    along an axis is the lower face of cell i; an x-edge (i,j,k) is
+ *    cell-centred in x and vertex-centred in y and z (AsterX/interface.ccl:
+ *    39-83,102).  Interior cells are [ng, ng+n), interior vertices
+ *    [ng, ng+n].
+ *  - Grid functions are passed as an array of device pointers indexed by
+ *    axb_gf (the reference's variable names).  Pointers a call does not use
+ *    may be NULL.
+ */
+#ifndef ASTERX_B200_H
+#define ASTERX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+#define AXB_EXTERN extern "C"
+#else
+#define AXB_EXTERN extern
+#endif
+#define AXB_API AXB_EXTERN __attribute__((visibility("default")))
+
+/* ------------------------------------------------------------------------ */
+/* status codes                                                              */
+/* ------------------------------------------------------------------------ */
+typedef enum axb_status {
+  AXB_OK = 0,
+  AXB_ERR_ARG = 1,        /* invalid argument (null pointer, bad size/enum) */
+  AXB_ERR_GHOSTS = 2,     /* too few ghost layers for the stencil            */
+  AXB_ERR_CUDA = 3,       /* a CUDA runtime call failed                      */
+  AXB_ERR_UNSUPPORTED = 4,/* option combination not implemented             */
+  AXB_ERR_TOO_LARGE = 5,  /* size beyond a documented limit                 */
+  AXB_ERR_NO_DEVICE = 6   /* no usable sm_100 device                         */
+} axb_status;
+
+/* Device error-word bits (axb_error_word). */
+#define AXB_EW_NAN_FLUX 0x1u   /* non-finite face flux (reference asserts)   */
+#define AXB_EW_NAN_RHS 0x2u    /* non-finite hydro RHS (rhs.cxx:199-206)      */
+#define AXB_EW_C2P_FAIL 0x4u   /* at least one cell ended as C2P_FAIL        */
+#define AXB_EW_ROOT_CAP 0x8u   /* an EOS temperature root find hit its cap    */
+#define AXB_EW_QUEUE_TIMEOUT 0x10u /* persistent work queue gave up          */
+
+/* ------------------------------------------------------------------------ */
+/* grid functions                                                            */
+/* ------------------------------------------------------------------------ */
+#define AXB_GF_LIST(X)                                                         \
+  /* ADMBaseX, vertex-centred */                                               \
+  X(gxx) X(gxy) X(gxz) X(gyy) X(gyz) X(gzz) X(alp) X(betax) X(betay) X(betaz)  \
+  X(kxx) X(kxy) X(kxz) X(kyy) X(kyz) X(kzz)                                    \
+  /* HydroBaseX primitives, cell-centred */                                    \
+  X(rho) X(velx) X(vely) X(velz) X(eps) X(press) X(temperature) X(Ye)          \
+  X(entropy) X(Bvecx) X(Bvecy) X(Bvecz)                                        \
+  /* conserved variables and their RHS, cell-centred */                        \
+  X(dens) X(momx) X(momy) X(momz) X(tau) X(DYe) X(DEnt)                        \
+  X(densrhs) X(momxrhs) X(momyrhs) X(momzrhs) X(taurhs) X(DYe_rhs) X(DEntrhs)  \
+  /* vector potential (edges) and Psi (vertices) and their RHS */              \
+  X(Avec_x) X(Avec_y) X(Avec_z) X(Psi)                                         \
+  X(Avec_x_rhs) X(Avec_y_rhs) X(Avec_z_rhs) X(Psi_rhs)                         \
+  /* staggered and centred densitised magnetic field */                        \
+  X(dBx_stag) X(dBy_stag) X(dBz_stag) X(dBx) X(dBy) X(dBz)                     \
+  /* con2prim bookkeeping, cell-centred */                                     \
+  X(con2prim_flag) X(saved_rho) X(saved_velx) X(saved_vely) X(saved_velz)      \
+  X(saved_eps) X(saved_Ye)                                                     \
+  X(zvec_x) X(zvec_y) X(zvec_z) X(svec_x) X(svec_y) X(svec_z)                  \
+  /* scratch: vertex auxiliaries of the A/Psi RHS (fluxes.cxx:798-826) */      \
+  X(Fx) X(Fy) X(Fz) X(Fbetax) X(Fbetay) X(Fbetaz) X(G)                         \
+  /* scratch: face fluxes of the transverse B components (rhs.cxx:171-172) */  \
+  X(fxBy) X(fxBz) X(fyBx) X(fyBz) X(fzBx) X(fzBy)                              \
+  /* scratch: partial flux divergence of the 7 hydro variables */              \
+  X(acc_dens) X(acc_momx) X(acc_momy) X(acc_momz) X(acc_tau) X(acc_DYe)        \
+  X(acc_DEnt)
+
+typedef enum axb_gf {
+#define AXB_GF_ENUM_(name) AXB_GF_##name,
+  AXB_GF_LIST(AXB_GF_ENUM_)
+#undef AXB_GF_ENUM_
+  AXB_NUM_GF
+} axb_gf;
+
+typedef struct axb_box {
+  int32_t n[3];      /* interior cells per axis                           */
+  int32_t ng;        /* ghost layers per axis (>= 3)                       */
+  int64_t sy, sz;    /* element strides of j and k (stride of i is 1)      */
+  double dx[3];      /* grid spacing                                       */
+  double xmin[3];    /* coordinate of vertex (ng, ng, ng)                  */
+} axb_box;
+
+typedef struct axb_fields {
+  double *gf[AXB_NUM_GF];
+} axb_fields;
+
+/* ------------------------------------------------------------------------ */
+/* parameters: the param.ccl keywords of AsterX, ReconX and Con2PrimFactory */
+/* ------------------------------------------------------------------------ */
+typedef enum axb_recon {
+  AXB_RECON_GODUNOV = 0,
+  AXB_RECON_MINMOD = 1,
+  AXB_RECON_MONOCENTRAL = 2,
+  AXB_RECON_PPM = 3,
+  AXB_RECON_EPPM = 4,
+  AXB_RECON_WENOZ = 5,
+  AXB_RECON_MP5 = 6
+} axb_recon;
+typedef enum axb_flux { AXB_FLUX_LXF = 0, AXB_FLUX_HLLE = 1 } axb_flux;
+typedef enum axb_recvar { AXB_RECVAR_V = 0, AXB_RECVAR_Z = 1, AXB_RECVAR_S = 2 } axb_recvar;
+typedef enum axb_gauge { AXB_GAUGE_ALGEBRAIC = 0, AXB_GAUGE_GEN_LORENZ = 1 } axb_gauge;
+typedef enum axb_c2p {
+  AXB_C2P_NONE = 0,
+  AXB_C2P_NOBLE = 1,
+  AXB_C2P_PALENZUELA = 2,
+  AXB_C2P_ENTROPY = 3
+} axb_c2p;
+
+/* c2p cell flags, identical to AsterX/src/con2prim.cxx:27-35 */
+typedef enum axb_c2p_flag {
+  AXB_C2P_INIT = 0,
+  AXB_C2P_PRIME = 1,
+  AXB_C2P_SECOND = 2,
+  AXB_C2P_ENTROPY_OK = 3,
+  AXB_C2P_ATMO = 4,
+  AXB_C2P_AVG = 5,
+  AXB_C2P_FAIL = 6
+} axb_c2p_flag;
+
+typedef struct axb_params {
+  /* ReconX (ReconX/param.ccl) */
+  int32_t reconstruction_method;   /* axb_recon, default GODUNOV          */
+  int32_t loworder_method;         /* GODUNOV | MINMOD | MONOCENTRAL      */
+  int32_t reconstruct_with_temperature;
+  int32_t ppm_shock_detection, ppm_zone_flattening;
+  double ppm_eta1, ppm_eta2, ppm_eps, ppm_eps_shock, ppm_small, ppm_omega1,
+      ppm_omega2, enhanced_ppm_C2, weno_eps, mp5_alpha;
+  /* EOSX polytrope used by PPM shock detection (EOSX/param.ccl:22-30) */
+  double poly_k, poly_gamma;
+  /* AsterX (AsterX/param.ccl) */
+  int32_t flux_type;               /* axb_flux, default LXF               */
+  int32_t recon_type;              /* axb_recvar, default V               */
+  int32_t vector_potential_gauge;  /* axb_gauge, default GEN_LORENZ       */
+  int32_t local_spatial_order;     /* 2 or 4                              */
+  int32_t use_uct, use_entropy_fix, excise, use_mask;
+  double lorenz_damp_fac;
+  /* Con2PrimFactory (Con2PrimFactory/param.ccl) */
+  int32_t c2p_prime, c2p_second;   /* axb_c2p                             */
+  int32_t max_iter;
+  int32_t thermal_eos_atmo, use_press_atmo, use_z, use_temperature,
+      Ye_lenient;
+  double c2p_tol, rho_abs_min, atmo_tol, eps_atmo, p_atmo, t_atmo, Ye_atmo,
+      r_atmo, n_rho_atmo, n_press_atmo, n_temp_atmo, alp_thresh, rho_BH,
+      eps_BH, vwlim_BH, cons_error_limit, vw_lim, B_lim;
+} axb_params;
+
+/* Fill p with the reference defaults of every param.ccl above. */
+AXB_API void axb_params_default(axb_params *p);
+
+/* Name of grid function `id` (the reference's variable name), NULL if out of
+ * range. */
+AXB_API const char *axb_gf_name(int id);
+
+/* ------------------------------------------------------------------------ */
+/* context and device status                                                 */
+/* ------------------------------------------------------------------------ */
+typedef struct axb_ctx axb_ctx;
+
+/* Bind to CUDA device `device` (must be sm_100) and allocate the small
+ * device status block (error word, CFL maximum, c2p counters).  No
+ * counterpart in the reference, whose device errors are asserts. */
+AXB_API int axb_ctx_create(int device, axb_ctx **out);
+AXB_API int axb_ctx_destroy(axb_ctx *ctx);
+
+/* Zero the status block, stream-ordered. */
+AXB_API int axb_status_reset(axb_ctx *ctx, void *stream);
+
+/* Synchronise `stream` and read the status block: error word (AXB_EW_*),
+ * the maximum characteristic speed max|lambda| over all faces of the flux
+ * passes since the last reset (the CFL input; the reference keeps per-face
+ * amax/amin instead, AsterX/src/fluxes.cxx:779-785), the number of cells
+ * that ended as C2P_FAIL, and a 64-bin histogram of first-solver iteration
+ * counts.  Any output pointer may be NULL. */
+AXB_API int axb_status_read(axb_ctx *ctx, void *stream, uint32_t *error_word,
+                            double *max_speed, uint32_t *c2p_fail,
+                            uint64_t *iter_hist64);
+
+/* ------------------------------------------------------------------------ */
+/* equations of state                                                        */
+/* ------------------------------------------------------------------------ */
+typedef struct axb_eos axb_eos;
+
+/* Ideal gas p = (Gamma-1) rho eps with validity ranges, as EOSX_Setup_EOS
+ * builds eos_3p_idealgas (EOSX/src/setup_eos.cxx:70-78,
+ * EOSX/src/eos_3p_idealgas/eos_3p_idealgas.hxx:124-142), plus the
+ * initial-data polytrope (poly_gamma, poly_k) the cold atmosphere uses
+ * (EOSX/src/setup_eos.cxx:33-41).  Host-only; allocates nothing on the
+ * device. */
+AXB_API int axb_eos_create_idealgas(double gamma, double particle_mass,
+                                    const double rho_range[2],
+                                    const double eps_range[2],
+                                    const double ye_range[2], double poly_gamma,
+                                    double poly_k, axb_eos **out);
+AXB_API int axb_eos_destroy(axb_eos *eos);
+
+/* ------------------------------------------------------------------------ */
+/* scheduled routines                                                        */
+/* ------------------------------------------------------------------------ */
+
+/* AsterX_RHSGroup on one box (AsterX/schedule.ccl:169-228), replacing the
+ * scheduled routines AsterX_Fluxes (AsterX/src/fluxes.cxx:828-878),
+ * AsterX_SourceTerms (AsterX/src/source.cxx:170-185) and AsterX_RHS
+ * (AsterX/src/rhs.cxx:18-253).
+ * Reads: ADMBaseX metric, lapse, shift, curvature; HydroBaseX primitives;
+ *   dB*_stag; Avec_*; Psi -- on the interior and ng ghost layers.
+ * Writes: densrhs .. DEntrhs (interior cells), Avec_*_rhs (interior edges),
+ *   Psi_rhs (interior vertices).
+ * Scratch: acc_*, fxBy .. fzBy, Fx .. G.
+ * Face quantities the reference obtains by SYNC (face B fluxes one cell
+ * outside the interior, vertex auxiliaries two vertices outside) are computed
+ * from the ghost data instead, so no synchronisation is needed inside the
+ * group.  Requires ng >= 3 and recon_type v_vec, use_uct = no.  The CFL speed
+ * maximum accumulates into the context status. */
+AXB_API int axb_rhs_group(axb_ctx *ctx, const axb_box *box,
+                          const axb_fields *fields, const axb_params *params,
+                          const axb_eos *eos, void *stream);
+
+#endif /* ASTERX_B200_H */
