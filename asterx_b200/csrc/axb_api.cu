@@ -134,9 +134,61 @@ AXB_API int axb_ctx_create(int device, axb_ctx **out) {
 AXB_API int axb_ctx_destroy(axb_ctx *c) {
   if (!c)
     return AXB_ERR_ARG;
+  if (c->ev) {
+    for (int q = 0; q < 2 * AXB_EVENT_POOL; ++q)
+      cudaEventDestroy(c->ev[q]);
+    delete[] c->ev;
+    delete[] c->ev_region;
+  }
   cudaFree(c->status);
   cudaFreeHost(c->status_host_pinned);
   delete c;
+  return AXB_OK;
+}
+
+// Start recording a CUDA event pair around every kernel launch of the
+// entry points that follow (on their stream).  Creates the event pool on first
+// use; call it outside any stream capture.
+AXB_API int axb_timing_begin(axb_ctx *c) {
+  if (!c)
+    return AXB_ERR_ARG;
+  if (!c->ev) {
+    c->ev = new (std::nothrow) cudaEvent_t[2 * AXB_EVENT_POOL];
+    c->ev_region = new (std::nothrow) int[AXB_EVENT_POOL];
+    if (!c->ev || !c->ev_region)
+      return AXB_ERR_ARG;
+    for (int q = 0; q < 2 * AXB_EVENT_POOL; ++q)
+      AXB_CUDA_TRY(cudaEventCreate(&c->ev[q]));
+  }
+  c->ev_used = 0;
+  c->timing = 1;
+  return AXB_OK;
+}
+
+// Stop recording, wait for the recorded launches and return, per kernel
+// region (nregions entries: sources, flux x, flux y, flux z, aux, ct+psi,
+// rk stage, sync, bstag, c2p, c2p cells, mlp), the summed milliseconds and
+// the number of launches.
+AXB_API int axb_timing_end(axb_ctx *c, double *ms, int *count, int nregions) {
+  if (!c || !ms || !count)
+    return AXB_ERR_ARG;
+  c->timing = 0;
+  for (int r = 0; r < nregions; ++r) {
+    ms[r] = 0;
+    count[r] = 0;
+  }
+  if (c->ev_used > 0)
+    AXB_CUDA_TRY(cudaEventSynchronize(c->ev[2 * (c->ev_used - 1) + 1]));
+  for (int q = 0; q < c->ev_used; ++q) {
+    float t = 0;
+    AXB_CUDA_TRY(cudaEventElapsedTime(&t, c->ev[2 * q], c->ev[2 * q + 1]));
+    const int r = c->ev_region[q];
+    if (r < nregions) {
+      ms[r] += t;
+      count[r] += 1;
+    }
+  }
+  c->ev_used = 0;
   return AXB_OK;
 }
 
@@ -333,14 +385,27 @@ AXB_API int axb_rhs_group(axb_ctx *c, const axb_box *box, const axb_fields *f,
     return rc;
   cudaStream_t s = (cudaStream_t)stream;
   const int seglen = 32;
-  if ((rc = launch_rhs_misc(p->local_spatial_order == 4 ? 1 : 0, a, s)))
+  axb_mark(c, AXB_R_SOURCES, s, true);
+  rc = launch_rhs_misc(p->local_spatial_order == 4 ? 1 : 0, a, s);
+  axb_mark(c, AXB_R_SOURCES, s, false);
+  if (rc)
     return rc;
-  for (int dir = 0; dir < 3; ++dir)
-    if ((rc = launch_flux_pass(dir, p->reconstruction_method, a, *eos, seglen, s)))
+  for (int dir = 0; dir < 3; ++dir) {
+    axb_mark(c, AXB_R_FLUX_X + dir, s, true);
+    rc = launch_flux_pass(dir, p->reconstruction_method, a, *eos, seglen, s);
+    axb_mark(c, AXB_R_FLUX_X + dir, s, false);
+    if (rc)
       return rc;
-  if ((rc = launch_rhs_misc(2, a, s)))
+  }
+  axb_mark(c, AXB_R_AUX, s, true);
+  rc = launch_rhs_misc(2, a, s);
+  axb_mark(c, AXB_R_AUX, s, false);
+  if (rc)
     return rc;
-  return launch_rhs_misc(3, a, s);
+  axb_mark(c, AXB_R_CT, s, true);
+  rc = launch_rhs_misc(3, a, s);
+  axb_mark(c, AXB_R_CT, s, false);
+  return rc;
 }
 
 namespace axb {

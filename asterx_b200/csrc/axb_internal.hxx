@@ -6,12 +6,52 @@
 #include "axb_common.cuh"
 #include "axb_eos.cuh"
 
+// Kernel regions timed by the optional per-launch CUDA events.
+enum axb_region {
+  AXB_R_SOURCES = 0,
+  AXB_R_FLUX_X,
+  AXB_R_FLUX_Y,
+  AXB_R_FLUX_Z,
+  AXB_R_AUX,
+  AXB_R_CT,
+  AXB_R_STAGE,
+  AXB_R_SYNC,
+  AXB_R_BSTAG,
+  AXB_R_C2P,
+  AXB_R_C2P_CELLS,
+  AXB_R_MLP,
+  AXB_NREGIONS
+};
+constexpr int AXB_EVENT_POOL = 4096;
+
 struct axb_ctx {
   int device;
   axb::DevStatus *status; // device
   axb::DevStatus *status_host_pinned;
   char last_error[256];
+  // per-launch timing (off unless axb_timing_begin was called)
+  int timing = 0;
+  int ev_used = 0;
+  cudaEvent_t *ev = nullptr; // 2 * AXB_EVENT_POOL
+  int *ev_region = nullptr;
 };
+
+// Record the start / end event of one timed launch (no-ops unless timing).
+inline void axb_mark(axb_ctx *c, int region, cudaStream_t s, bool start) {
+  if (!c || !c->timing)
+    return;
+  if (start) {
+    if (c->ev_used >= AXB_EVENT_POOL)
+      return;
+    c->ev_region[c->ev_used] = region;
+    cudaEventRecord(c->ev[2 * c->ev_used], s);
+  } else {
+    if (c->ev_used >= AXB_EVENT_POOL)
+      return;
+    cudaEventRecord(c->ev[2 * c->ev_used + 1], s);
+    ++c->ev_used;
+  }
+}
 
 // Tabulated-EOS device data (see axb_tab.cuh); declared here so the host
 // handle can own it.

@@ -497,11 +497,15 @@ AXB_API int axb_con2prim_group(axb_ctx *c, const axb_box *box,
   const int T = 128;
   {
     const dim3 grid((b.n[0] + 2 + T - 1) / T, b.n[1] + 2, b.n[2] + 2);
+    axb_mark(c, AXB_R_BSTAG, s, true);
     k_bstag<<<grid, T, 0, s>>>(a);
+    axb_mark(c, AXB_R_BSTAG, s, false);
   }
   {
     const dim3 grid((b.n[0] + T - 1) / T, b.n[1], b.n[2]);
+    axb_mark(c, AXB_R_C2P, s, true);
     k_c2p_box<<<grid, T, 0, s>>>(a, eos->ideal);
+    axb_mark(c, AXB_R_C2P, s, false);
   }
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
 }

@@ -142,7 +142,9 @@ AXB_API int axb_rk_stage(axb_ctx *c, const axb_box *box, const axb_fields *out,
   a.gdt = gamma * dt;
   const int T = 128;
   const dim3 grid((box->n[0] + 1 + T - 1) / T, box->n[1] + 1, box->n[2] + 1);
+  axb_mark(c, AXB_R_STAGE, (cudaStream_t)stream, true);
   k_rk_stage<<<grid, T, 0, (cudaStream_t)stream>>>(a);
+  axb_mark(c, AXB_R_STAGE, (cudaStream_t)stream, false);
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
 }
 
@@ -169,6 +171,8 @@ AXB_API int axb_sync_periodic(axb_ctx *c, const axb_box *box,
     centring_of(ids[q], a.cent[q]);
   }
   const dim3 grid(box->n[1] + 2 * box->ng + 1, box->n[2] + 2 * box->ng + 1, nids);
+  axb_mark(c, AXB_R_SYNC, (cudaStream_t)stream, true);
   k_sync_periodic<<<grid, 128, 0, (cudaStream_t)stream>>>(a);
+  axb_mark(c, AXB_R_SYNC, (cudaStream_t)stream, false);
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
 }

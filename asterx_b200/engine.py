@@ -62,6 +62,8 @@ def load_library(path=LIB_PATH):
                                 C.POINTER(Fields), C.POINTER(Params), _vp,
                                 C.c_double, C.c_double, C.c_double, C.c_double,
                                 C.c_int, _vp]
+    lib.axb_timing_begin.argtypes = [_vp]
+    lib.axb_timing_end.argtypes = [_vp, C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_int]
     for name in ("axb_con2prim_group", "axb_substep", "axb_rk_stage",
                  "axb_sync_periodic", "axb_c2p_cells", "axb_eos_create_tabulated"):
         if hasattr(lib, name):
@@ -167,6 +169,15 @@ class Engine:
                                          C.byref(params), eos, alpha, beta, gamma, dt,
                                          int(periodic), self.stream_ptr(stream)),
                     "axb_substep")
+
+    def timing_begin(self):
+        self._check(self.lib.axb_timing_begin(self.ctx), "axb_timing_begin")
+
+    def timing_end(self, nregions=12):
+        ms = (C.c_double * nregions)()
+        cnt = (C.c_int * nregions)()
+        self._check(self.lib.axb_timing_end(self.ctx, ms, cnt, nregions), "axb_timing_end")
+        return list(ms), list(cnt)
 
     def status_reset(self, stream=None):
         self._check(self.lib.axb_status_reset(self.ctx, self.stream_ptr(stream)),

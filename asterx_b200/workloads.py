@@ -21,110 +21,169 @@ arrays themselves.
 """
 from __future__ import annotations
 
+import math
+
 import numpy as np
 
 from .abi import Layout
 
 
-def _modes(rng, coords, kmax=4, nmodes=4):
+class _XP:
+    """Minimal array namespace over numpy or torch (CPU or CUDA), so the same
+    generator builds small host boxes for the tests and 256^3 boxes directly
+    in device memory for the benchmark."""
+
+    def __init__(self, mod=np, device=None):
+        self.mod = mod
+        self.torch = mod is not np
+        self.device = device
+
+    def __getattr__(self, name):
+        return getattr(self.mod, name)
+
+    def asarray(self, a):
+        if self.torch:
+            return self.mod.as_tensor(np.asarray(a), dtype=self.mod.float64,
+                                      device=self.device)
+        return np.asarray(a, dtype=np.float64)
+
+    def zeros(self, n):
+        if self.torch:
+            return self.mod.zeros(n, dtype=self.mod.float64, device=self.device)
+        return np.zeros(n)
+
+    def full(self, n, v):
+        if self.torch:
+            return self.mod.full((n,), float(v), dtype=self.mod.float64,
+                                 device=self.device)
+        return np.full(n, float(v))
+
+    def copy(self, a):
+        return a.clone() if self.torch else a.copy()
+
+    def bcast(self, a, shape):
+        """broadcast to shape and flatten to a fresh contiguous array"""
+        if self.torch:
+            if not hasattr(a, "shape") or a.dim() == 0:
+                a = self.mod.as_tensor(a, dtype=self.mod.float64, device=self.device)
+            return self.mod.broadcast_to(a, shape).reshape(-1).clone()
+        return np.broadcast_to(a, shape).ravel().copy()
+
+    def coords(self, L, centring):
+        return [self.asarray(c) for c in L.coords(centring)]
+
+    def uniform(self, rng, lo, hi, n):
+        u = rng.uniform(lo, hi, n)
+        return self.asarray(u)
+
+
+_NP = _XP(np)
+
+
+def _modes(rng, coords, kmax=4, nmodes=4, xp=_NP):
     """Sum of seeded sine modes, periodic on the unit cube."""
     x, y, z = coords
     f = 0.0
     for _ in range(nmodes):
         k = rng.integers(1, kmax + 1, size=3) * rng.choice([-1, 1], size=3)
         ph = rng.uniform(0, 2 * np.pi)
-        f = f + np.sin(2 * np.pi * (k[0] * x + k[1] * y + k[2] * z) + ph)
+        f = f + xp.sin(2 * math.pi * (float(k[0]) * x + float(k[1]) * y
+                                      + float(k[2]) * z) + ph)
     return f / nmodes
 
 
-def flat_metric(L: Layout, f: dict):
+def _shape(L):
+    return (L.npts[2], L.npts[1], L.sy)
+
+
+def flat_metric(L: Layout, f: dict, xp=_NP):
     for n in ("gxy", "gxz", "gyz", "betax", "betay", "betaz", "kxx", "kxy",
               "kxz", "kyy", "kyz", "kzz"):
-        f[n] = L.zeros()
+        f[n] = xp.zeros(L.size)
     for n in ("gxx", "gyy", "gzz", "alp"):
-        f[n] = np.ones(L.size)
+        f[n] = xp.full(L.size, 1.0)
 
 
 def curved_metric(L: Layout, f: dict, rng, amp=0.05, shift_amp=0.01,
-                  curv_amp=0.02):
-    cv = L.coords((0, 0, 0))
-    shape = L.view(L.zeros()).shape
+                  curv_amp=0.02, xp=_NP):
+    cv = xp.coords(L, (0, 0, 0))
+    shape = _shape(L)
     diag = {"gxx": 1.0, "gyy": 1.0, "gzz": 1.0, "gxy": 0.0, "gxz": 0.0,
             "gyz": 0.0}
     for n, d in diag.items():
-        f[n] = np.broadcast_to(d + amp * _modes(rng, cv), shape).ravel().copy()
-    g = np.stack([f[n] for n in ("gxx", "gxy", "gxz", "gyy", "gyz", "gzz")])
+        f[n] = xp.bcast(d + amp * _modes(rng, cv, xp=xp), shape)
+    g = [f[n] for n in ("gxx", "gxy", "gxz", "gyy", "gyz", "gzz")]
     m1 = g[0]
     m2 = g[0] * g[3] - g[1] ** 2
     det = (g[0] * (g[3] * g[5] - g[4] ** 2) - g[1] * (g[1] * g[5] - g[4] * g[2])
            + g[2] * (g[1] * g[4] - g[3] * g[2]))
-    assert (m1 > 0).all() and (m2 > 0).all() and (det > 0).all(), \
+    assert bool((m1 > 0).all()) and bool((m2 > 0).all()) and bool((det > 0).all()), \
         "metric not positive definite"
-    f["alp"] = np.broadcast_to(1.0 - amp * _modes(rng, cv), shape).ravel().copy()
+    f["alp"] = xp.bcast(1.0 - amp * _modes(rng, cv, xp=xp), shape)
     for n in ("betax", "betay", "betaz"):
-        f[n] = np.broadcast_to(shift_amp * _modes(rng, cv), shape).ravel().copy()
+        f[n] = xp.bcast(shift_amp * _modes(rng, cv, xp=xp), shape)
     for n in ("kxx", "kxy", "kxz", "kyy", "kyz", "kzz"):
-        f[n] = np.broadcast_to(curv_amp * _modes(rng, cv), shape).ravel().copy()
+        f[n] = xp.bcast(curv_amp * _modes(rng, cv, xp=xp), shape)
 
 
-def _curl_stag(L: Layout, Ax, Ay, Az):
+def _curl_stag(L: Layout, Ax, Ay, Az, xp=_NP):
     """Face curl of edge A exactly as AsterX/src/computeBfromA.cxx:32-55, on
     every face whose neighbours exist."""
     v = L.view
     ax, ay, az = v(Ax), v(Ay), v(Az)
     idx = [1.0 / d for d in L.dx]
-    bx, by, bz = (np.zeros_like(ax) for _ in range(3))
+    bx, by, bz = (v(xp.zeros(L.size)) for _ in range(3))
     bx[:-1, :-1, :] = (idx[1] * (az[:-1, 1:, :] - az[:-1, :-1, :])
                        - idx[2] * (ay[1:, :-1, :] - ay[:-1, :-1, :]))
     by[:-1, :, :-1] = (idx[2] * (ax[1:, :, :-1] - ax[:-1, :, :-1])
                        - idx[0] * (az[:-1, :, 1:] - az[:-1, :, :-1]))
     bz[:, :-1, :-1] = (idx[0] * (ay[:, :-1, 1:] - ay[:, :-1, :-1])
                        - idx[1] * (ax[:, 1:, :-1] - ax[:, :-1, :-1]))
-    return bx.ravel(), by.ravel(), bz.ravel()
+    return bx.reshape(-1), by.reshape(-1), bz.reshape(-1)
 
 
-def _v2c(L: Layout, a):
+def _v2c(L: Layout, a, xp=_NP):
     """Vertex-to-cell average (the 8 corners, AsterUtils aster_interp.hxx:
     23-36), defined on every cell whose corners exist."""
     v = L.view(a)
-    out = np.zeros_like(v)
+    out = L.view(xp.zeros(L.size))
     out[:-1, :-1, :-1] = (v[:-1, :-1, :-1] + v[:-1, :-1, 1:] + v[:-1, 1:, :-1]
                           + v[:-1, 1:, 1:] + v[1:, :-1, :-1] + v[1:, :-1, 1:]
                           + v[1:, 1:, :-1] + v[1:, 1:, 1:]) / 8.0
-    return out.ravel()
+    return out.reshape(-1)
 
 
-def _sqrt_detg_cell(L: Layout, f):
-    g = [_v2c(L, f[n]) for n in ("gxx", "gxy", "gxz", "gyy", "gyz", "gzz")]
+def _sqrt_detg_cell(L: Layout, f, xp=_NP):
+    g = [_v2c(L, f[n], xp) for n in ("gxx", "gxy", "gxz", "gyy", "gyz", "gzz")]
     det = (g[0] * (g[3] * g[5] - g[4] ** 2) - g[1] * (g[1] * g[5] - g[4] * g[2])
            + g[2] * (g[1] * g[4] - g[3] * g[2]))
-    return np.sqrt(np.where(det > 0, det, 1.0)), g
+    return xp.sqrt(xp.where(det > 0, det, det * 0 + 1.0)), g
 
 
-def _finish_prims(L, f, gamma, ye=None):
+def _finish_prims(L, f, gamma, ye=None, xp=_NP):
     """eps, temperature, entropy (kappa) and Ye from rho and press for an
     ideal gas (EOSX/src/eos_3p_idealgas/eos_3p_idealgas.hxx:115-229)."""
     rho, press = f["rho"], f["press"]
     f["eps"] = press / (rho * (gamma - 1.0))
     f["temperature"] = (gamma - 1.0) * f["eps"]
     f["entropy"] = (gamma - 1.0) * f["eps"] * rho ** (1.0 - gamma)
-    f["Ye"] = np.full(L.size, 0.5) if ye is None else ye
+    f["Ye"] = xp.full(L.size, 0.5) if ye is None else ye
 
 
-def _cell_B_from_stag(L, f):
+def _cell_B_from_stag(L, f, xp=_NP):
     v = L.view
     dB = []
     for n, ax in (("dBx_stag", 2), ("dBy_stag", 1), ("dBz_stag", 0)):
         s = v(f[n])
-        c = np.zeros_like(s)
+        c = v(xp.zeros(L.size))
         if ax == 2:
             c[:, :, :-1] = 0.5 * (s[:, :, :-1] + s[:, :, 1:])
         elif ax == 1:
             c[:, :-1, :] = 0.5 * (s[:, :-1, :] + s[:, 1:, :])
         else:
             c[:-1, :, :] = 0.5 * (s[:-1, :, :] + s[1:, :, :])
-        dB.append(c.ravel())
-    sq, _ = _sqrt_detg_cell(L, f)
+        dB.append(c.reshape(-1))
+    sq, _ = _sqrt_detg_cell(L, f, xp)
     f["dBx"], f["dBy"], f["dBz"] = dB
     f["Bvecx"], f["Bvecy"], f["Bvecz"] = (d / sq for d in dB)
 
@@ -160,77 +219,84 @@ def balsara_box(n=64, ng=3, gamma=5.0 / 3.0, seed=1, pert=1e-3):
 
 def curved_box(n=24, ng=3, gamma=4.0 / 3.0, seed=2, wmax=10.0, njumps=3,
                with_ye=False, sigma=(1e-3, 10.0), jump=(2.0, 8.0),
-               rho_min=1e-8, theta=(1e-2, 1.0)):
-    """Config-2-like periodic patch on [0, 1]^3 with a curved static metric."""
+               rho_min=1e-8, theta=(1e-2, 1.0), xp=None):
+    """Config-2-like periodic patch on [0, 1]^3 with a curved static metric.
+    ``xp`` selects the array library: None/numpy for host arrays, or an
+    ``_XP(torch, device)`` to build the box in device memory."""
+    xp = xp or _NP
     if isinstance(n, int):
         n = (n, n, n)
     L = Layout(n, ng, tuple(1.0 / v for v in n), (0.0, 0.0, 0.0))
     rng = np.random.default_rng(seed)
-    shape = L.view(L.zeros()).shape
+    shape = _shape(L)
     f = {}
-    curved_metric(L, f, rng)
-    cc = L.coords((1, 1, 1))
+    curved_metric(L, f, rng, xp=xp)
+    cc = xp.coords(L, (1, 1, 1))
 
     def smooth(lo, hi, kmax=3, nmodes=3):
-        u = 0.5 * (1 + _modes(rng, cc, kmax=kmax, nmodes=nmodes))
-        return np.broadcast_to(lo + (hi - lo) * u, shape).ravel().copy()
+        u = 0.5 * (1 + _modes(rng, cc, kmax=kmax, nmodes=nmodes, xp=xp))
+        return xp.bcast(lo + (hi - lo) * u, shape)
 
     # vector potential on edges, B from its curl
     ev = {"Avec_x": (1, 0, 0), "Avec_y": (0, 1, 0), "Avec_z": (0, 0, 1)}
     for nm, cent in ev.items():
-        c = L.coords(cent)
-        f[nm] = np.broadcast_to(0.05 * _modes(rng, c, kmax=3), shape).ravel().copy()
-    f["Psi"] = np.broadcast_to(1e-3 * _modes(rng, L.coords((0, 0, 0))),
-                               shape).ravel().copy()
+        c = xp.coords(L, cent)
+        f[nm] = xp.bcast(0.05 * _modes(rng, c, kmax=3, xp=xp), shape)
+    f["Psi"] = xp.bcast(1e-3 * _modes(rng, xp.coords(L, (0, 0, 0)), xp=xp), shape)
     f["dBx_stag"], f["dBy_stag"], f["dBz_stag"] = _curl_stag(
-        L, f["Avec_x"], f["Avec_y"], f["Avec_z"])
-    _cell_B_from_stag(L, f)
-    _, g = _sqrt_detg_cell(L, f)
+        L, f["Avec_x"], f["Avec_y"], f["Avec_z"], xp)
+    _cell_B_from_stag(L, f, xp)
+    _, g = _sqrt_detg_cell(L, f, xp)
 
     # velocity: Lorentz factor in [1, wmax] along a smooth unit direction
     W = smooth(1.0, wmax, kmax=1, nmodes=2)
     th = smooth(0.3 * np.pi, 0.7 * np.pi, kmax=1, nmodes=2)
     ph0 = rng.uniform(0, 2 * np.pi)
     ph = smooth(ph0, ph0 + 0.5 * np.pi, kmax=1, nmodes=2)
-    d = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)])
-    gd = np.array([[g[0], g[1], g[2]], [g[1], g[3], g[4]], [g[2], g[4], g[5]]])
-    nrm = np.einsum("i...,ij...,j...->...", d, gd, d)
-    nrm = np.where(nrm > 1e-12, nrm, 1.0)
-    vmag = np.sqrt(1.0 - 1.0 / W ** 2)
-    vel = d * (vmag / np.sqrt(nrm))
+    d = [xp.sin(th) * xp.cos(ph), xp.sin(th) * xp.sin(ph), xp.cos(th)]
+    gd = [[g[0], g[1], g[2]], [g[1], g[3], g[4]], [g[2], g[4], g[5]]]
+
+    def lower(v):
+        return [gd[i][0] * v[0] + gd[i][1] * v[1] + gd[i][2] * v[2] for i in range(3)]
+
+    def dot(a, b):
+        return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]
+
+    nrm = dot(d, lower(d))
+    nrm = xp.where(nrm > 1e-12, nrm, nrm * 0 + 1.0)
+    vmag = xp.sqrt(1.0 - 1.0 / W ** 2)
+    vel = [di * (vmag / xp.sqrt(nrm)) for di in d]
     f["velx"], f["vely"], f["velz"] = vel
     # density from the magnetisation, then planar jumps
-    B = np.stack([f["Bvecx"], f["Bvecy"], f["Bvecz"]])
-    vlow = np.einsum("ij...,j...->i...", gd, vel)
-    Bsq = np.einsum("i...,ij...,j...->...", B, gd, B)
-    vB = np.einsum("i...,i...->...", vlow, B)
+    B = [f["Bvecx"], f["Bvecy"], f["Bvecz"]]
+    vlow = lower(vel)
+    Bsq = dot(B, lower(B))
+    vB = dot(vlow, B)
     bsq = Bsq / W ** 2 + vB ** 2
-    sigma = 10 ** smooth(np.log10(sigma[0]), np.log10(sigma[1]))
-    rho = np.clip(bsq / sigma, rho_min, 1.0)
-    theta = 10 ** smooth(np.log10(theta[0]), np.log10(theta[1]))
-    xyz = [np.broadcast_to(c, shape).ravel() for c in cc]
+    sigma_f = 10 ** smooth(np.log10(sigma[0]), np.log10(sigma[1]))
+    rho = xp.clip(bsq / sigma_f, rho_min, 1.0)
+    theta_f = 10 ** smooth(np.log10(theta[0]), np.log10(theta[1]))
+    xyz = [xp.bcast(c, shape) for c in cc]
     for _ in range(njumps):
         nv = rng.normal(size=3)
         nv /= np.linalg.norm(nv)
         x0 = rng.uniform(0.2, 0.8)
-        side = (nv[0] * (xyz[0] - x0) + nv[1] * (xyz[1] - 0.5)
-                + nv[2] * (xyz[2] - 0.5)) > 0
-        rho = np.where(side, rho * rng.uniform(*jump), rho)
-        theta = np.where(side, theta / rng.uniform(1.5, 4), theta)
-    f["rho"] = np.clip(rho, rho_min, 1.0)
-    f["press"] = f["rho"] * theta
+        side = (float(nv[0]) * (xyz[0] - x0) + float(nv[1]) * (xyz[1] - 0.5)
+                + float(nv[2]) * (xyz[2] - 0.5)) > 0
+        rho = xp.where(side, rho * float(rng.uniform(*jump)), rho)
+        theta_f = xp.where(side, theta_f / float(rng.uniform(1.5, 4)), theta_f)
+    f["rho"] = xp.clip(rho, rho_min, 1.0)
+    f["press"] = f["rho"] * theta_f
     ye = smooth(0.05, 0.5) if with_ye else None
-    _finish_prims(L, f, gamma, ye)
+    _finish_prims(L, f, gamma, ye, xp)
     return L, f
 
 
-def saved_from_prims(f):
-    f["saved_rho"] = f["rho"].copy()
-    f["saved_velx"] = f["velx"].copy()
-    f["saved_vely"] = f["vely"].copy()
-    f["saved_velz"] = f["velz"].copy()
-    f["saved_eps"] = f["eps"].copy()
-    f["saved_Ye"] = f["Ye"].copy()
+def saved_from_prims(f, xp=None):
+    xp = xp or _NP
+    for n, s in (("rho", "saved_rho"), ("velx", "saved_velx"), ("vely", "saved_vely"),
+                 ("velz", "saved_velz"), ("eps", "saved_eps"), ("Ye", "saved_Ye")):
+        f[s] = xp.copy(f[n])
 
 
 def c2p_cells(ncells, seed=4, gamma=5.0 / 3.0, rho_range=(1e-12, 1e-2),
@@ -270,26 +336,33 @@ def c2p_cells(ncells, seed=4, gamma=5.0 / 3.0, rho_range=(1e-12, 1e-2),
     return dict(rho=rho, eps=eps, press=press, vel=vel, B=B, g=g, W=W)
 
 
-def cons_from_prims(L: Layout, f: dict):
+def cons_from_prims(L: Layout, f: dict, xp=None):
     """Densitised conserved variables of every cell from its primitives and
     the vertex-to-cell metric (the Valencia prim->cons map of
     AsterX/src/prim2con.hxx:38-83), written into f."""
-    sq, g = _sqrt_detg_cell(L, f)
-    gd = np.array([[g[0], g[1], g[2]], [g[1], g[3], g[4]], [g[2], g[4], g[5]]])
-    v = np.stack([f["velx"], f["vely"], f["velz"]])
-    B = np.stack([f["Bvecx"], f["Bvecy"], f["Bvecz"]])
-    vl = np.einsum("ij...,j...->i...", gd, v)
-    Bl = np.einsum("ij...,j...->i...", gd, B)
-    v2 = np.clip(np.einsum("i...,i...->...", vl, v), 0, 1 - 1e-15)
-    W = 1.0 / np.sqrt(1.0 - v2)
-    bst = W * np.einsum("i...,i...->...", B, vl)
-    bl = Bl / W + bst * vl
-    bs2 = (np.einsum("i...,i...->...", B, Bl) + bst * bst) / (W * W)
+    xp = xp or _NP
+    sq, g = _sqrt_detg_cell(L, f, xp)
+    gd = [[g[0], g[1], g[2]], [g[1], g[3], g[4]], [g[2], g[4], g[5]]]
+
+    def lower(v):
+        return [gd[i][0] * v[0] + gd[i][1] * v[1] + gd[i][2] * v[2] for i in range(3)]
+
+    def dot(a, b):
+        return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]
+
+    v = [f["velx"], f["vely"], f["velz"]]
+    B = [f["Bvecx"], f["Bvecy"], f["Bvecz"]]
+    vl = lower(v)
+    Bl = lower(B)
+    v2 = xp.clip(dot(vl, v), 0.0, 1 - 1e-15)
+    W = 1.0 / xp.sqrt(1.0 - v2)
+    bst = W * dot(B, vl)
+    bl = [Bl[i] / W + bst * vl[i] for i in range(3)]
+    bs2 = (dot(B, Bl) + bst * bst) / (W * W)
     rho, eps, press = f["rho"], f["eps"], f["press"]
     hW2 = W * W * (rho * (1.0 + eps) + press + bs2)
     f["dens"] = sq * rho * W
-    mom = sq * (hW2 * vl - bst * bl)
-    f["momx"], f["momy"], f["momz"] = mom
+    f["momx"], f["momy"], f["momz"] = [sq * (hW2 * vl[i] - bst * bl[i]) for i in range(3)]
     f["tau"] = sq * (hW2 - (press + 0.5 * bs2) - bst * bst) - f["dens"]
     f["DYe"] = f["dens"] * f["Ye"]
     f["DEnt"] = f["dens"] * f["entropy"]

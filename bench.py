@@ -1,0 +1,402 @@
+#!/usr/bin/env python
+"""Benchmark: zone-updates/s per RK3 substep of the GRMHD hot path.
+
+Workload (one box per GPU): a periodic 256^3 patch with 3 ghost zones and a
+static curved metric (gamma_ij = delta_ij + 0.05 * seeded sine modes, lapse
+1 - 0.05 sin, shift amplitude 0.01), primitives from smooth seeded fields plus
+three planar jumps, Lorentz factor up to 10, ideal gas Gamma = 4/3, WENO-Z
+(or MP5) reconstruction, HLLE fluxes, flux-CT with generalised Lorenz gauge,
+Palenzuela recovery (Noble backup), SSP-RK3 stages.  The inputs are seeded
+synthetic fields of that shape; there is no dataset.  One "step" is one RK3
+substep: RHS group + stage update + periodic ghost fill + post-step group
+(curl A, dB, con2prim) + ghost fill of the primitives.
+
+Prints one JSON line (rank 0).  ``--impl reference`` times the reference's
+own CPU code for the same path (compiled from its sources through the
+stand-in headers in oracle/) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+if REPO not in sys.path:
+    sys.path.insert(0, REPO)
+
+METRIC = "Zone-updates/s per RK3 substep"
+UNIT = "zone-updates/s"
+SSPRK3 = [(0.0, 1.0, 1.0), (0.75, 0.25, 0.25), (1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0)]
+GAMMA = 4.0 / 3.0
+EOS_KW = dict(rho=(1e-40, 1e10), eps=(0.0, 1e10))
+REGIONS = ["sources", "flux_x", "flux_y", "flux_z", "aux", "ct_psi", "rk_stage",
+           "sync", "bstag", "c2p", "c2p_cells", "mlp"]
+# Algorithmic FP64 values moved per interior zone by each kernel (each field
+# read once, written once; ghost re-reads not counted).
+ALG_DOUBLES = {
+    "sources": 9 + 16 + 7,           # prims + vertex metric & curvature, 7 RHS
+    "flux_x": 9 + 1 + 10 + 7 + 2,    # recon fields, dB_stag, metric; acc, B fluxes
+    "flux_y": 9 + 1 + 10 + 14 + 2,   # + acc read-modify-write
+    "flux_z": 9 + 1 + 10 + 7 + 14 + 2,  # + acc read, RHS read-modify-write
+    "aux": 3 + 1 + 10 + 7,
+    "ct_psi": 6 + 7 + 4 + 4,
+    "rk_stage": 11 * 4,
+    "bstag": 3 + 3,
+    "c2p": 7 + 3 + 7 + 7 + 12 + 7 + 3 + 6 + 1,
+}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=12)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256, help="interior cells per axis")
+    ap.add_argument("--recon", default="wenoz", choices=["wenoz", "mp5", "ppm"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="target CPU time of the reference baseline sample")
+    return ap.parse_args()
+
+
+def peak_hbm():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_table():
+    """Per-launch DRAM bytes from the committed ncu summaries (profiles/)."""
+    p = os.path.join(REPO, "profiles", "traffic.json")
+    try:
+        with open(p) as fh:
+            return json.load(fh)
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            import tempfile
+            fd, self.path = tempfile.mkstemp(prefix="axb_clocks_", suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]),
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+# ---------------------------------------------------------------------------
+# reference CPU code (the checker build of the reference sources)
+# ---------------------------------------------------------------------------
+def reference_substep_rate(seconds, recon, seed=2, start_n=24):
+    """Time the reference's scheduled routines (AsterX_Fluxes,
+    AsterX_SourceTerms, AsterX_RHS, the stage update, AsterX_ComputedBstagFromA,
+    AsterX_ComputedBFromdBstag, AsterX_Con2Prim) on one box of the workload,
+    with the box edge chosen so that the sample takes about `seconds`.
+    Returns (zone-updates/s, sample description, threads)."""
+    import numpy as np
+    from asterx_b200 import abi
+    from asterx_b200 import workloads as W
+    from oracle.oracle import reference
+    ref = reference()
+    if ref is None:
+        raise RuntimeError("oracle/_ref/libaxref.so is not built")
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+
+    def one(n, nsub):
+        L, f = W.curved_box(n=n, ng=3, seed=seed, wmax=10.0)
+        W.cons_from_prims(L, f)
+        W.saved_from_prims(f)
+        for name in abi.GF_NAMES:
+            f.setdefault(name, L.zeros())
+        p = abi.default_params(reconstruction_method=recon, flux_type="hlle",
+                               c2p_prime="palenzuela", c2p_second="noble")
+        host = {k: v.copy() for k, v in f.items()}
+        ref.setup(L, p, host)
+        ref.eos_idealgas(GAMMA, **EOS_KW)
+        dt = 0.25 * L.dx[0]
+        evolved = abi.CONS + ["Avec_x", "Avec_y", "Avec_z", "Psi"]
+        rhs = abi.HYDRO_RHS + abi.AVEC_RHS
+        un = {k: host[k].copy() for k in evolved}
+        t0 = time.perf_counter()
+        for s in range(nsub):
+            a_, b_, g_ = SSPRK3[s % 3]
+            ref.run("fluxes")
+            ref.run("sources")
+            ref.run("rhs")
+            for u, r in zip(evolved, rhs):
+                host[u][:] = a_ * un[u] + b_ * host[u] + (g_ * dt) * host[r]
+            ref.run("bstag")
+            ref.run("dB")
+            ref.run("c2p")
+        return time.perf_counter() - t0, L
+
+    n = start_n
+    t, L = one(n, 1)
+    rate = n ** 3 / t
+    # box edge for ~seconds/3 per substep, then three substeps
+    n = int(max(16, min(160, round((rate * seconds / 3.0) ** (1 / 3)))))
+    t, L = one(n, 3)
+    rate = 3 * n ** 3 / t
+    return rate, f"{n}^3 box, 3 SSP-RK3 substeps, {t:.1f} s", threads, t
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    res_rate = []
+    sample = None
+    threads = None
+    for _ in range(args.warmup):
+        reference_substep_rate(2.0, args.recon)
+    for _ in range(args.steps):
+        rate, sample, threads, _t = reference_substep_rate(6.0, args.recon)
+        res_rate.append(rate)
+    value = statistics.median(res_rate)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.n}^3 curved-metric patch (bounded CPU sample), "
+                               f"{args.recon}+HLLE, Palenzuela c2p, flux-CT",
+                   "parallelism": "OpenMP host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# the engine
+# ---------------------------------------------------------------------------
+def ours(args):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    from asterx_b200 import abi
+    from asterx_b200 import workloads as W
+    from asterx_b200.engine import Engine
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=dev)
+    eng = Engine(local)
+    xp = W._XP(torch, dev)
+    L, f = W.curved_box(n=args.n, ng=3, seed=2 + rank, wmax=10.0, xp=xp)
+    W.cons_from_prims(L, f, xp=xp)
+    W.saved_from_prims(f, xp=xp)
+    skip = {"zvec_x", "zvec_y", "zvec_z", "svec_x", "svec_y", "svec_z", "dBx",
+            "dBy", "dBz"}
+    for name in abi.GF_NAMES:
+        if name not in f and name not in skip:
+            f[name] = torch.zeros(L.size, dtype=torch.float64, device=dev)
+    evolved = abi.CONS + ["Avec_x", "Avec_y", "Avec_z", "Psi"]
+    fn = {k: f[k].clone() for k in evolved}
+    params = abi.default_params(reconstruction_method=args.recon, flux_type="hlle",
+                                c2p_prime="palenzuela", c2p_second="noble")
+    eos = eng.eos_idealgas(GAMMA, **EOS_KW)
+    dt = 0.25 * L.dx[0]
+    zones = args.n ** 3
+    stream = torch.cuda.current_stream(dev)
+
+    def substep(s):
+        a_, b_, g_ = SSPRK3[s % 3]
+        if s % 3 == 0:
+            for k in evolved:
+                fn[k].copy_(f[k])
+        eng.substep(L, f, fn, params, eos, a_, b_, g_, dt, periodic=True)
+
+    for s in range(args.warmup):
+        substep(s)
+    torch.cuda.synchronize()
+    eng.status_reset()
+    sampler = ClockSampler(local)
+    sampler.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    eng.timing_begin()
+    e0.record(stream)
+    for s in range(args.steps):
+        substep(s)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    region_ms, region_n = eng.timing_end(len(REGIONS))
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    st = eng.status()
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * zones * args.steps / (ms / 1e3)
+    launches = int(sum(region_n))
+
+    # dominant kernel and its roofline
+    shares = {REGIONS[i]: region_ms[i] for i in range(len(REGIONS)) if region_n[i]}
+    dom = max(shares, key=shares.get)
+    idom = REGIONS.index(dom)
+    avg_launch_s = region_ms[idom] / region_n[idom] / 1e3
+    alg_bytes = ALG_DOUBLES[dom] * 8 * zones
+    achieved = alg_bytes / avg_launch_s / 1e9
+    peak, peak_kind = peak_hbm()
+    traffic = traffic_table().get(f"{dom}:{args.recon}:{args.n}")
+
+    # end to end through the C ABI from pinned host memory: every step copies
+    # the state the substep reads in and the state it writes back out
+    inputs = [k for k in f if k not in ("densrhs", "momxrhs", "momyrhs", "momzrhs",
+                                        "taurhs", "DYe_rhs", "DEntrhs", "Avec_x_rhs",
+                                        "Avec_y_rhs", "Avec_z_rhs", "Psi_rhs", "Fx",
+                                        "Fy", "Fz", "Fbetax", "Fbetay", "Fbetaz", "G",
+                                        "fxBy", "fxBz", "fyBx", "fyBz", "fzBx", "fzBy")
+              and not k.startswith("acc_")]
+    outputs = [k for k in ["rho", "velx", "vely", "velz", "eps", "press",
+                           "temperature", "Ye", "entropy", "Bvecx", "Bvecy", "Bvecz",
+                           "con2prim_flag"] + evolved + abi.SAVED if k in f]
+    host = {k: torch.empty(L.size, dtype=torch.float64, pin_memory=True) for k in
+            set(inputs) | set(outputs)}
+    for k in host:
+        host[k].copy_(f[k])
+    torch.cuda.synchronize()
+    h2d = 8 * L.size * len(inputs)
+    d2h = 8 * L.size * len(outputs)
+    ne = max(1, min(args.e2e_steps, args.steps))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for s in range(ne):
+        for k in inputs:
+            f[k].copy_(host[k], non_blocking=True)
+        substep(s)
+        for k in outputs:
+            host[k].copy_(f[k], non_blocking=True)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e2.elapsed_time(e3)
+    if world > 1:
+        t = torch.tensor([ms_e2e], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e_value = world * zones * ne / (ms_e2e / 1e3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            rate, sample, threads, _t = reference_substep_rate(args.cpu_seconds, args.recon)
+            cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": sample}
+        except Exception as exc:  # the checker library may be absent
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
+                   "sample": f"unavailable: {exc}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded fields of the configuration)",
+            "config": {"workload": f"{args.n}^3 periodic patch, 3 ghosts, curved static "
+                                   f"metric, {args.recon}+HLLE, flux-CT, Palenzuela c2p "
+                                   f"(Noble backup), ideal gas Gamma=4/3, SSP-RK3 substeps",
+                       "box": [args.n] * 3, "ghosts": 3, "recon": args.recon,
+                       "parallelism": f"one box per GPU x{world}",
+                       "l2": "inputs larger than L2 (146 MB per field)"},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved,
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "alg_bytes_per_launch": alg_bytes,
+                         "avg_launch_ms": avg_launch_s * 1e3},
+            "kernels_ms_per_step": {REGIONS[i]: region_ms[i] / args.steps
+                                    for i in range(len(REGIONS)) if region_n[i]},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": ne},
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "error_word": st["error_word"], "c2p_fail_cells": st["c2p_fail"],
+            "max_char_speed": st["max_speed"],
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -238,4 +238,61 @@ AXB_API int axb_rhs_group(axb_ctx *ctx, const axb_box *box,
                           const axb_fields *fields, const axb_params *params,
                           const axb_eos *eos, void *stream);
 
+/* AsterX_Con2PrimGroup on one box (AsterX/schedule.ccl:119-165), replacing
+ * AsterX_ComputedBstagFromA (AsterX/src/computeBfromA.cxx:58-65),
+ * AsterX_ComputedBFromdBstag (:67-85) and AsterX_Con2Prim
+ * (AsterX/src/con2prim.cxx:457-502) with the Con2PrimFactory functors
+ * c2p_2DNoble::solve (Con2PrimFactory/src/c2p_2DNoble.hxx:275-594) and
+ * c2p_1DPalenzuela::solve (Con2PrimFactory/src/c2p_1DPalenzuela.hxx:306-556).
+ * Reads: Avec_* (interior edges + one ghost layer), conserved variables,
+ *   saved_* and temperature (seeds), metric and lapse.
+ * Writes: dB*_stag on the interior faces and one transverse ghost layer,
+ *   dB*, the HydroBaseX primitives, conserved variables (after floors),
+ *   saved_*, con2prim_flag, and zvec_* / svec_* when given.
+ * c2p_prime and c2p_second must be Noble or Palenzuela (second may be None);
+ * use_entropy_fix and use_mask are not supported (AXB_ERR_UNSUPPORTED).
+ * C2P_FAIL cells are counted in the context status. */
+AXB_API int axb_con2prim_group(axb_ctx *ctx, const axb_box *box,
+                               const axb_fields *fields,
+                               const axb_params *params, const axb_eos *eos,
+                               void *stream);
+
+/* One Runge-Kutta stage of the 11 evolved variables (dens, mom*, tau, DYe,
+ * DEnt, Avec_*, Psi) on their interiors:
+ *   out = alpha * U_n + beta * U_k + gamma * dt * RHS.
+ * This is the stage combine that CarpetX's ODESolvers performs around the
+ * reference's scheduled routines (no counterpart in the reference sources);
+ * SSP-RK3 in Shu-Osher form uses (0,1,1), (3/4,1/4,1/4), (1/3,2/3,2/3).
+ * `out`, `un` and `uk` may be the same fields. */
+AXB_API int axb_rk_stage(axb_ctx *ctx, const axb_box *box, const axb_fields *out,
+                         const axb_fields *un, const axb_fields *uk,
+                         const axb_fields *rhs, double alpha, double beta,
+                         double gamma, double dt, void *stream);
+
+/* Periodic ghost fill of the grid functions `ids[0..nids)` of one box, each
+ * with its own centring: the single-box form of the driver's SYNC with
+ * periodic outer boundaries (AsterX/schedule.ccl:110-115,157-164). */
+AXB_API int axb_sync_periodic(axb_ctx *ctx, const axb_box *box,
+                              const axb_fields *fields, const int *ids, int nids,
+                              void *stream);
+
+/* One RK substep of one box: axb_rhs_group, axb_rk_stage (U_k updated in
+ * place in `fields`, U_n read from `fields_n`), periodic fill of the evolved
+ * variables (if `periodic`), axb_con2prim_group, periodic fill of the
+ * primitives (if `periodic`).  Stream-ordered, allocation-free. */
+AXB_API int axb_substep(axb_ctx *ctx, const axb_box *box,
+                        const axb_fields *fields, const axb_fields *fields_n,
+                        const axb_params *params, const axb_eos *eos,
+                        double alpha, double beta, double gamma, double dt,
+                        int periodic, void *stream);
+
+/* Optional per-launch timing: after axb_timing_begin every kernel launch of
+ * the entry points above is bracketed by CUDA events on its stream;
+ * axb_timing_end waits for them and returns, per kernel region (sources,
+ * flux x, flux y, flux z, aux, ct+psi, rk stage, sync, bstag, c2p, c2p
+ * cells, mlp -- `nregions` entries), the summed milliseconds and launch
+ * counts.  Not part of the reference; a measurement aid. */
+AXB_API int axb_timing_begin(axb_ctx *ctx);
+AXB_API int axb_timing_end(axb_ctx *ctx, double *ms, int *count, int nregions);
+
 #endif /* ASTERX_B200_H */
