@@ -188,7 +188,10 @@ __global__ void __launch_bounds__(128) k_c2p_box(const C2PBoxArgs a, const EOS e
     seeds.rho = a.saved_rho[I];
     seeds.eps = a.saved_eps[I];
     seeds.Ye = a.saved_Ye[I];
-    seeds.press = eos.press_from_valid_rho_eps_ye(seeds.rho, seeds.eps, seeds.Ye);
+    {
+      double e = seeds.eps; // the reference clamps a copy, not the seed
+      seeds.press = eos.press_from_valid_rho_eps_ye(seeds.rho, e, seeds.Ye);
+    }
     seeds.temperature = a.temperature[I];
     seeds.entropy = 0.0; // only read by the excision path, filled there
     for (int q = 0; q < 3; ++q) {

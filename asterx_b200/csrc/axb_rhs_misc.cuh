@@ -121,11 +121,14 @@ __global__ void __launch_bounds__(128) k_sources(const RhsArgs a) {
     t0[q] = A * vs[q] / alp + P * beta[q] / sq(alp) - bs0 * bs[q];
     t0low[q] = A * v_low[q] / alp - bs_low[q] * bs0;
   }
+  // T^{ij} is symmetric (an smat in the reference): upper triangle, mirrored
   double t[3][3];
+#pragma unroll
   for (int p = 0; p < 3; ++p)
-    for (int q = 0; q < 3; ++q)
-      t[p][q] = A * vs[p] * vs[q] + P * (ug(p, q) - beta[p] * beta[q] / sq(alp)) -
-                bs[p] * bs[q];
+#pragma unroll
+    for (int q = p; q < 3; ++q)
+      t[p][q] = t[q][p] = A * vs[p] * vs[q] +
+                          P * (ug(p, q) - beta[p] * beta[q] / sq(alp)) - bs[p] * bs[q];
   double shiftk[3];
   lower3(K, beta, shiftk);
   const double ssk = dot3(shiftk, beta);
