@@ -286,6 +286,25 @@ AXB_API int axb_substep(axb_ctx *ctx, const axb_box *box,
                         double alpha, double beta, double gamma, double dt,
                         int periodic, void *stream);
 
+/* axb_rhs_group for callers that cannot allocate device memory (a host
+ * framework that owns every device allocation, a tool that may not call
+ * cudaMalloc on a shared device, a driver whose footprint is fixed after
+ * set-up).  No counterpart in the reference.  Inputs and outputs are as for
+ * axb_rhs_group; the 20 scratch grid functions (acc_*, fxBy..fzBy, Fx..G) are
+ * ignored if given and taken instead from a 16 MiB array that this library
+ * holds in static device memory on every GPU it is loaded on, until exit.
+ * Limit: 20 * sz * (n[2] + 2*ng + 1) doubles (each rounded up to 32) must fit
+ * in 2^21 doubles -- e.g. a 32^3 box with 3 ghosts; larger boxes get
+ * AXB_ERR_TOO_LARGE.  Calls no cudaMalloc, cudaFree or allocating library
+ * routine and needs no axb_ctx (the error word and CFL maximum are kept in
+ * the static block, not reported).  The first call on a device looks up the
+ * arrays' device addresses with that device current; make it before any
+ * stream capture.  All calls share the arrays: calls that overlap on the GPU
+ * (other streams, other threads) race; order them on one stream. */
+AXB_API int axb_rhs_group_noalloc(const axb_box *box, const axb_fields *fields,
+                                  const axb_params *params, const axb_eos *eos,
+                                  void *stream);
+
 /* Optional per-launch timing: after axb_timing_begin every kernel launch of
  * the entry points above is bracketed by CUDA events on its stream;
  * axb_timing_end waits for them and returns, per kernel region (sources,
