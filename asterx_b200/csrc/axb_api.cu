@@ -1,7 +1,9 @@
 // C ABI of the engine: contexts, equations of state and the RHS group.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <new>
 
 #include "axb_flux_launch.cuh"
@@ -255,12 +257,104 @@ AXB_API int axb_eos_create_idealgas(double gamma, double particle_mass,
   return AXB_OK;
 }
 
+// Tabulated3d evolution EOS from a table already in memory, in the state
+// eos_3p_tabulated3d::init leaves it after reading and converting the file
+// (EOSX/src/eos_3p_tabulated3d/eos_3p_tabulated3d.hxx:53-192): natural-log
+// axes, 19 variables per node interleaved variable-fastest.  The ranges are
+// set up as at the end of init (:179-192), including the eps range of
+// compute_eps_range_full_table, which scans the EPS * (node count) block of
+// that interleaved array.
+AXB_API int axb_eos_create_tabulated3d(int nrho, int ntemp, int nye,
+                                       const double *logrho, const double *logtemp,
+                                       const double *ye, const double *table,
+                                       double energy_shift, double poly_gamma,
+                                       double poly_k, axb_eos **out) {
+  if (!out || !logrho || !logtemp || !ye || !table || nrho < 2 || ntemp < 2 ||
+      nye < 2 || !(poly_gamma > 1))
+    return AXB_ERR_ARG;
+  const int nax[3] = {nrho, ntemp, nye};
+  const double *ax[3] = {logrho, logtemp, ye};
+  for (int d = 0; d < 3; ++d)
+    if (!(ax[d][1] > ax[d][0]))
+      return AXB_ERR_ARG;
+  const size_t nodes = size_t(nrho) * ntemp * nye;
+  // the table starts on a 32-byte sector: axes padded to 4 doubles
+  const size_t naxes = (size_t(nrho) + ntemp + nye + 3) / 4 * 4;
+  const size_t total = naxes + nodes * TAB_NV;
+  double *h = static_cast<double *>(std::malloc(total * sizeof(double)));
+  if (!h)
+    return AXB_ERR_ARG;
+  double *dptr = nullptr;
+  if (cudaMalloc(&dptr, total * sizeof(double)) != cudaSuccess) {
+    std::free(h);
+    return AXB_ERR_CUDA;
+  }
+  size_t o = 0;
+  double *hx[3];
+  for (int d = 0; d < 3; ++d) {
+    hx[d] = h + o;
+    std::memcpy(hx[d], ax[d], nax[d] * sizeof(double));
+    o += nax[d];
+  }
+  double *hy = h + naxes;
+  const int keep[TAB_NV] = {0, 1, 2, 4}; // ln P, ln(eps + shift), s, cs^2
+  for (size_t q = 0; q < nodes; ++q)
+    for (int v = 0; v < TAB_NV; ++v)
+      hy[TAB_NV * q + v] = table[size_t(19) * q + keep[v]];
+  EosTab t{};
+  for (int d = 0; d < 3; ++d) {
+    t.n[d] = nax[d];
+    t.x[d] = hx[d];
+    t.idx[d] = 1. / (ax[d][1] - ax[d][0]);
+    t.x0[d] = ax[d][0];
+    t.xlast[d] = ax[d][nax[d] - 1];
+  }
+  t.y = hy;
+  t.shift = energy_shift;
+  t.rgrho = Range{std::exp(t.x0[0]), std::exp(t.xlast[0])};
+  t.rgtemp = Range{std::exp(t.x0[1]), std::exp(t.xlast[1])};
+  t.rgye = Range{t.x0[2], t.xlast[2]};
+  double emin = std::numeric_limits<double>::max();
+  double emax = std::numeric_limits<double>::lowest();
+  for (size_t q = 0; q < nodes; ++q) {
+    const double v = std::exp(table[1 * nodes + q]) - energy_shift;
+    emin = std::fmin(emin, v);
+    emax = std::fmax(emax, v);
+  }
+  t.rgeps = Range{std::fmax(emin, 1e-15), emax};
+  t.err = nullptr;
+  if (cudaMemcpy(dptr, h, total * sizeof(double), cudaMemcpyHostToDevice) !=
+      cudaSuccess) {
+    cudaFree(dptr);
+    std::free(h);
+    return AXB_ERR_CUDA;
+  }
+  axb_eos *e = new (std::nothrow) axb_eos();
+  if (!e) {
+    cudaFree(dptr);
+    std::free(h);
+    return AXB_ERR_ARG;
+  }
+  e->kind = 1;
+  e->ideal = EosIdeal{};
+  e->poly = make_poly(poly_gamma, poly_k);
+  e->tab_h = t;
+  e->tab_d = t;
+  for (int d = 0; d < 3; ++d)
+    e->tab_d.x[d] = dptr + (hx[d] - h);
+  e->tab_d.y = dptr + (hy - h);
+  e->tab_host = h;
+  e->tab_dev = dptr;
+  *out = e;
+  return AXB_OK;
+}
+
 AXB_API int axb_eos_destroy(axb_eos *e) {
   if (!e)
     return AXB_ERR_ARG;
   if (e->tab_dev)
     cudaFree(e->tab_dev);
-  delete e->tab_host;
+  std::free(e->tab_host);
   delete e;
   return AXB_OK;
 }
@@ -274,7 +368,6 @@ int fill_rhs_args(axb_ctx *c, const axb_box *box, const axb_fields *f,
   if (!f || !p)
     return AXB_ERR_ARG;
   if (p->recon_type != AXB_RECVAR_V || p->use_uct ||
-      p->reconstruct_with_temperature ||
       p->reconstruction_method == AXB_RECON_EPPM ||
       !(p->local_spatial_order == 2 || p->local_spatial_order == 4))
     return AXB_ERR_UNSUPPORTED;
@@ -287,6 +380,9 @@ int fill_rhs_args(axb_ctx *c, const axb_box *box, const axb_fields *f,
   a.vel[2] = GFP(velz);
   a.eps = GFP(eps);
   a.press = GFP(press);
+  a.temperature = GFP(temperature);
+  a.rec_temp = p->reconstruct_with_temperature != 0;
+  a.thermo = a.rec_temp ? a.temperature : a.press;
   a.Ye = GFP(Ye);
   a.entropy = GFP(entropy);
   a.Bvec[0] = GFP(Bvecx);
@@ -340,7 +436,7 @@ int fill_rhs_args(axb_ctx *c, const axb_box *box, const axb_fields *f,
   a.write_bflux = 1;
   a.status = c->status;
   // every pointer the group reads or writes must be present
-  const void *req[] = {a.rho, a.vel[0], a.vel[1], a.vel[2], a.eps, a.press,
+  const void *req[] = {a.rho, a.vel[0], a.vel[1], a.vel[2], a.eps, a.press, a.thermo,
                        a.Ye, a.entropy, a.Bvec[0], a.Bvec[1], a.Bvec[2],
                        a.dBstag[0], a.dBstag[1], a.dBstag[2], a.alp, a.beta[0],
                        a.beta[1], a.beta[2], a.Avec[0], a.Avec[1], a.Avec[2],
@@ -383,6 +479,11 @@ AXB_API int axb_rhs_group(axb_ctx *c, const axb_box *box, const axb_fields *f,
   int rc = fill_rhs_args(c, box, f, p, a);
   if (rc)
     return rc;
+  // the tabulated EOS has no eps(rho, press) (the reference asserts,
+  // eos_3p_tabulated3d.hxx:259-269): its fluxes need the reconstructed
+  // temperature
+  if (eos->kind == 1 && !a.rec_temp)
+    return AXB_ERR_UNSUPPORTED;
   cudaStream_t s = (cudaStream_t)stream;
   const int seglen = 32;
   axb_mark(c, AXB_R_SOURCES, s, true);

@@ -24,6 +24,8 @@ struct EosIdeal {
   double gamma, gm1, inv_gamma, temp_over_eps;
   Range rgrho, rgye, rgtemp, rgeps;
 
+  static constexpr bool kTabulated = false;
+
   AXB_HD double press_from_valid_rho_eps_ye(double rho, double &eps, double) const {
     return gm1 * rho * eps;
   }

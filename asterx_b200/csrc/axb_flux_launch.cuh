@@ -29,6 +29,8 @@ int launch_flux_pass_t(int dir, const RhsArgs &a, const axb_eos &eos,
                        int seglen, cudaStream_t s) {
   if (eos.kind == 0)
     return launch_flux_pass_eos<RECON>(dir, a, eos.ideal, seglen, s);
+  if (eos.kind == 1)
+    return launch_flux_pass_eos<RECON>(dir, a, tab_for_launch(eos, a.status), seglen, s);
   return AXB_ERR_UNSUPPORTED;
 }
 

@@ -5,6 +5,7 @@
 
 #include "axb_common.cuh"
 #include "axb_eos.cuh"
+#include "axb_tab.cuh"
 
 // Kernel regions timed by the optional per-launch CUDA events.
 enum axb_region {
@@ -53,19 +54,24 @@ inline void axb_mark(axb_ctx *c, int region, cudaStream_t s, bool start) {
   }
 }
 
-// Tabulated-EOS device data (see axb_tab.cuh); declared here so the host
-// handle can own it.
-namespace axb {
-struct EosTab;
-}
-
 struct axb_eos {
   int kind; // 0 ideal gas, 1 tabulated
   axb::EosIdeal ideal;
   axb::EosPoly poly;
-  axb::EosTab *tab_host; // host copy of the device descriptor (tabulated)
-  double *tab_dev;       // device table storage
+  // tabulated: the same descriptor over host memory (host-side atmosphere
+  // set-up) and over device memory (kernels); each owns one allocation
+  axb::EosTab tab_h, tab_d;
+  double *tab_host; // axes + compact table, host
+  double *tab_dev;  // axes + compact table, device
 };
+
+// The device descriptor of a tabulated EOS with its root-cap flag pointed at
+// the context's status word.
+inline axb::EosTab tab_for_launch(const axb_eos &e, axb::DevStatus *st) {
+  axb::EosTab t = e.tab_d;
+  t.err = st ? &st->error_word : nullptr;
+  return t;
+}
 
 namespace axb {
 // launchers (one per translation unit of kernels)

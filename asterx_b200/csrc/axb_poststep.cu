@@ -4,6 +4,7 @@
 // Also the RK stage update and the periodic ghost fill of one box.
 #include <cmath>
 #include <cstring>
+#include <limits>
 
 #include "axb_c2p.cuh"
 #include "axb_internal.hxx"
@@ -474,6 +475,18 @@ int fill_c2p_args(axb_ctx *c, const axb_box *box, const axb_fields *f,
     a.Zmin = eos->ideal.rgrho.min;
     if (a.atmo_uniform)
       a.atmo_const = host_atmosphere(a, eos->ideal);
+  } else if (eos->kind == 1) {
+    // no eps(rho, press) for the tabulated EOS (the reference asserts,
+    // eos_3p_tabulated3d.hxx:259-269): refuse the settings that need it
+    // on every cell
+    if (p->thermal_eos_atmo && p->use_press_atmo)
+      return AXB_ERR_UNSUPPORTED;
+    // the reader never sets the tabulated EOS's gamma, which the Noble
+    // scheme reads (c2p_2DNoble.hxx); NaN makes that scheme fail cleanly
+    a.gamma_noble = std::numeric_limits<double>::quiet_NaN();
+    a.Zmin = eos->tab_h.rgrho.min;
+    if (a.atmo_uniform)
+      a.atmo_const = host_atmosphere(a, eos->tab_h);
   } else {
     return AXB_ERR_UNSUPPORTED;
   }
@@ -507,7 +520,10 @@ AXB_API int axb_con2prim_group(axb_ctx *c, const axb_box *box,
   {
     const dim3 grid((b.n[0] + T - 1) / T, b.n[1], b.n[2]);
     axb_mark(c, AXB_R_C2P, s, true);
-    k_c2p_box<<<grid, T, 0, s>>>(a, eos->ideal);
+    if (eos->kind == 1)
+      k_c2p_box<<<grid, T, 0, s>>>(a, tab_for_launch(*eos, a.status));
+    else
+      k_c2p_box<<<grid, T, 0, s>>>(a, eos->ideal);
     axb_mark(c, AXB_R_C2P, s, false);
   }
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;

@@ -23,6 +23,10 @@ enum { V_DENS = 0, V_MOMX, V_MOMY, V_MOMZ, V_TAU, V_DYE, V_DENT, NHYDRO };
 struct RhsArgs {
   BoxDev b;
   const double *rho, *vel[3], *eps, *press, *Ye, *entropy, *Bvec[3];
+  // the thermodynamic variable reconstructed with rho, entropy and Ye:
+  // temperature when rec_temp, else pressure (fluxes.cxx:257-355)
+  const double *temperature, *thermo;
+  int rec_temp;
   const double *dBstag[3];
   const double *alp, *beta[3], *g[6], *K[6];
   const double *Avec[3], *Psi;
@@ -86,7 +90,8 @@ AXB_D FaceMetric face_metric(const RhsArgs &a, long long I) {
 }
 
 // Reconstructed primitive state on one side of a face.  r[] order:
-//   0 rho, 1 entropy, 2 Ye, 3 press, 4 vx, 5 vy, 6 vz, 7 B_{dir+1}, 8 B_{dir+2}
+//   0 rho, 1 entropy, 2 Ye, 3 press or temperature, 4 vx, 5 vy, 6 vz,
+//   7 B_{dir+1}, 8 B_{dir+2}
 enum { R_RHO = 0, R_ENT, R_YE, R_PRESS, R_VX, R_VY, R_VZ, R_B1, R_B2, NREC };
 
 struct SideOut {
@@ -95,12 +100,23 @@ struct SideOut {
 };
 
 // Per-side physics of CalcFlux (fluxes.cxx:357-654) for a v_vec state.
+// With rec_temp, r[R_PRESS] holds the reconstructed temperature and eps and
+// press come from (rho, T, Ye) (fluxes.cxx:297-304); otherwise eps comes
+// from (rho, press, Ye) (:346-353; the temperature computed there is unused
+// and only the tabulated EOS, which cannot take this route, would clamp eps).
 template <int DIR, class EOS>
 AXB_D void side_physics(const FaceMetric &m, const double *r, double Bdir,
-                        const EOS &eos, SideOut &o) {
+                        const EOS &eos, int rec_temp, SideOut &o) {
   constexpr int D1 = (DIR + 1) % 3, D2 = (DIR + 2) % 3;
-  const double rho = r[R_RHO], ent = r[R_ENT], ye = r[R_YE], press = r[R_PRESS];
-  double eps = eos.eps_from_valid_rho_press_ye(rho, press, ye);
+  const double rho = r[R_RHO], ent = r[R_ENT], ye = r[R_YE];
+  double eps, press;
+  if (rec_temp) {
+    eps = eos.eps_from_valid_rho_temp_ye(rho, r[R_PRESS], ye);
+    press = eos.press_from_valid_rho_temp_ye(rho, r[R_PRESS], ye);
+  } else {
+    press = r[R_PRESS];
+    eps = eos.eps_from_valid_rho_press_ye(rho, press, ye);
+  }
   const double vel[3] = {r[R_VX], r[R_VY], r[R_VZ]};
   double B[3];
   B[DIR] = Bdir;
@@ -120,8 +136,14 @@ AXB_D void side_physics(const FaceMetric &m, const double *r, double Bdir,
   for (int i = 0; i < 3; ++i)
     blow[i] = Blow[i] / W + alp_b0 * vlow[i];
   const double bsq = (B2 + sq(alp_b0)) / sq(W);
+  // cs^2 as the product of two sound-speed queries (fluxes.cxx:556-560); the
+  // first may clamp eps in place (tabulated), and only then can the second
+  // differ from the first
+  const double eps_in = eps;
   const double cs = eos.csnd_from_valid_rho_eps_ye(rho, eps, ye);
-  const double cs2 = cs * cs;
+  const double cs2 =
+      cs * ((EOS::kTabulated && !(eps == eps_in)) ? eos.csnd_from_valid_rho_eps_ye(rho, eps, ye)
+                                                  : cs);
   const double h = 1 + eps + press / rho;
   const double dens = m.sqrtg * rho * W;
   const double DEnt = m.sqrtg * rho * W * ent;

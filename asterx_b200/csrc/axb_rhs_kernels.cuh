@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(128)
     ijk[T1] = t1;
     ijk[DIR] = f0 - 1;
     long long I = b.at(ijk[0], ijk[1], ijk[2]);
-    const double *fld[NREC] = {a.rho,    a.entropy, a.Ye,       a.press,
+    const double *fld[NREC] = {a.rho,    a.entropy, a.Ye,       a.thermo,
                                a.vel[0], a.vel[1],  a.vel[2],   a.Bvec[D1],
                                a.Bvec[D2]};
     const double idxd = b.idx[DIR];
@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(128)
 #pragma unroll
       for (int v = 0; v < NREC; ++v) {
         double q[5];
-        if (v == R_PRESS) {
+        if (v == R_PRESS && !a.rec_temp) {
 #pragma unroll
           for (int m = 0; m < 5; ++m) q[m] = pr[m];
         } else if (v == R_VX + DIR) {
@@ -110,8 +110,8 @@ __global__ void __launch_bounds__(128)
         const FaceMetric m = face_metric<DIR>(a, I);
         const double Bdir = __ldg(a.dBstag[DIR] + I) / m.sqrtg;
         SideOut sL, sR;
-        side_physics<DIR>(m, L, Bdir, eos, sL);
-        side_physics<DIR>(m, R, Bdir, eos, sR);
+        side_physics<DIR>(m, L, Bdir, eos, a.rec_temp, sL);
+        side_physics<DIR>(m, R, Bdir, eos, a.rec_temp, sR);
         const double cmax = fmax(0.0, fmax(fmax(sL.lam_p, sL.lam_m),
                                            fmax(sR.lam_p, sR.lam_m)));
         const double cmin = fmin(0.0, fmin(fmin(sL.lam_p, sL.lam_m),

@@ -49,6 +49,9 @@ def load_library(path=LIB_PATH):
                                     C.POINTER(C.c_uint64)]
     lib.axb_eos_create_idealgas.argtypes = [C.c_double, C.c_double, _dp, _dp, _dp,
                                             C.c_double, C.c_double, C.POINTER(_vp)]
+    lib.axb_eos_create_tabulated3d.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp,
+                                               _dp, C.c_double, C.c_double, C.c_double,
+                                               C.POINTER(_vp)]
     lib.axb_eos_destroy.argtypes = [_vp]
     lib.axb_rhs_group.argtypes = [_vp, C.POINTER(Box), C.POINTER(Fields),
                                   C.POINTER(Params), _vp, _vp]
@@ -65,7 +68,7 @@ def load_library(path=LIB_PATH):
     lib.axb_timing_begin.argtypes = [_vp]
     lib.axb_timing_end.argtypes = [_vp, C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_int]
     for name in ("axb_con2prim_group", "axb_substep", "axb_rk_stage",
-                 "axb_sync_periodic", "axb_c2p_cells", "axb_eos_create_tabulated"):
+                 "axb_sync_periodic", "axb_c2p_cells", "axb_eos_create_tabulated3d"):
         if hasattr(lib, name):
             getattr(lib, name).restype = C.c_int
     return lib
@@ -104,6 +107,24 @@ class Engine:
         self._check(self.lib.axb_eos_create_idealgas(
             gamma, umass, C.cast(r, _dp), C.cast(e, _dp), C.cast(y, _dp),
             poly_gamma, poly_k, C.byref(h)), "axb_eos_create_idealgas")
+        self._eos.append(h)
+        return h
+
+    def eos_tabulated(self, logrho, logtemp, ye, table, energy_shift=0.0,
+                      poly_gamma=2.0, poly_k=100.0):
+        """Tabulated3d EOS from arrays in the layout of
+        ``workloads.synthetic_table`` (19 variables per node, variable
+        fastest)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64)
+                for a in (logrho, logtemp, ye, table)]
+        lr, lt, y, t = arrs
+        if t.size != 19 * lr.size * lt.size * y.size:
+            raise ValueError("table size does not match the axes")
+        h = _vp()
+        ptr = [a.ctypes.data_as(_dp) for a in arrs]
+        self._check(self.lib.axb_eos_create_tabulated3d(
+            len(lr), len(lt), len(y), *ptr, energy_shift, poly_gamma, poly_k,
+            C.byref(h)), "axb_eos_create_tabulated3d")
         self._eos.append(h)
         return h
 

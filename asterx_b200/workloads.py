@@ -219,7 +219,7 @@ def balsara_box(n=64, ng=3, gamma=5.0 / 3.0, seed=1, pert=1e-3):
 
 def curved_box(n=24, ng=3, gamma=4.0 / 3.0, seed=2, wmax=10.0, njumps=3,
                with_ye=False, sigma=(1e-3, 10.0), jump=(2.0, 8.0),
-               rho_min=1e-8, theta=(1e-2, 1.0), xp=None):
+               rho_min=1e-8, theta=(1e-2, 1.0), xp=None, a_amp=0.05, rho_max=1.0):
     """Config-2-like periodic patch on [0, 1]^3 with a curved static metric.
     ``xp`` selects the array library: None/numpy for host arrays, or an
     ``_XP(torch, device)`` to build the box in device memory."""
@@ -241,7 +241,7 @@ def curved_box(n=24, ng=3, gamma=4.0 / 3.0, seed=2, wmax=10.0, njumps=3,
     ev = {"Avec_x": (1, 0, 0), "Avec_y": (0, 1, 0), "Avec_z": (0, 0, 1)}
     for nm, cent in ev.items():
         c = xp.coords(L, cent)
-        f[nm] = xp.bcast(0.05 * _modes(rng, c, kmax=3, xp=xp), shape)
+        f[nm] = xp.bcast(a_amp * _modes(rng, c, kmax=3, xp=xp), shape)
     f["Psi"] = xp.bcast(1e-3 * _modes(rng, xp.coords(L, (0, 0, 0)), xp=xp), shape)
     f["dBx_stag"], f["dBy_stag"], f["dBz_stag"] = _curl_stag(
         L, f["Avec_x"], f["Avec_y"], f["Avec_z"], xp)
@@ -274,7 +274,7 @@ def curved_box(n=24, ng=3, gamma=4.0 / 3.0, seed=2, wmax=10.0, njumps=3,
     vB = dot(vlow, B)
     bsq = Bsq / W ** 2 + vB ** 2
     sigma_f = 10 ** smooth(np.log10(sigma[0]), np.log10(sigma[1]))
-    rho = xp.clip(bsq / sigma_f, rho_min, 1.0)
+    rho = xp.clip(bsq / sigma_f, rho_min, rho_max)
     theta_f = 10 ** smooth(np.log10(theta[0]), np.log10(theta[1]))
     xyz = [xp.bcast(c, shape) for c in cc]
     for _ in range(njumps):
@@ -285,10 +285,76 @@ def curved_box(n=24, ng=3, gamma=4.0 / 3.0, seed=2, wmax=10.0, njumps=3,
                 + float(nv[2]) * (xyz[2] - 0.5)) > 0
         rho = xp.where(side, rho * float(rng.uniform(*jump)), rho)
         theta_f = xp.where(side, theta_f / float(rng.uniform(1.5, 4)), theta_f)
-    f["rho"] = xp.clip(rho, rho_min, 1.0)
+    f["rho"] = xp.clip(rho, rho_min, rho_max)
     f["press"] = f["rho"] * theta_f
     ye = smooth(0.05, 0.5) if with_ye else None
     _finish_prims(L, f, gamma, ye, xp)
+    return L, f
+
+
+# ---------------------------------------------------------------------------
+# Synthetic tabulated equation of state
+# ---------------------------------------------------------------------------
+TAB_NV = 19  # variables per node of the EOSX table layout
+TAB_LOGPRESS, TAB_LOGENERGY, TAB_ENTROPY, TAB_CS2 = 0, 1, 2, 4
+
+
+def tab_thermo(rho, temp, ye, xp=_NP):
+    """Closed-form thermodynamics of the synthetic table:
+    P = rho T (1 + Ye) + T^4 / 3 + 100 rho^2 (ideal gas + radiation + cold
+    part), with the specific energy and entropy that satisfy the first law
+    for that pressure,
+        eps = 1.5 T (1 + Ye) + T^4 / rho + 100 rho,
+        s   = (1 + Ye) (1.5 ln T - ln rho) + 4 T^3 / (3 rho),
+    and the relativistic sound speed cs^2 = (dP/drho)_s / h, h = 1 + eps + P/rho.
+    Returns (press, eps, entropy, cs2)."""
+    y1 = 1.0 + ye
+    press = rho * temp * y1 + temp ** 4 / 3.0 + 100.0 * rho ** 2
+    eps = 1.5 * temp * y1 + temp ** 4 / rho + 100.0 * rho
+    ent = y1 * (1.5 * xp.log(temp) - xp.log(rho)) + 4.0 * temp ** 3 / (3.0 * rho)
+    p_rho = temp * y1 + 200.0 * rho
+    p_t = rho * y1 + 4.0 * temp ** 3 / 3.0
+    s_rho = -(y1 / rho + 4.0 * temp ** 3 / (3.0 * rho ** 2))
+    s_t = 1.5 * y1 / temp + 4.0 * temp ** 2 / rho
+    dp_rho_s = p_rho - p_t * s_rho / s_t
+    h = 1.0 + eps + press / rho
+    return press, eps, ent, dp_rho_s / h
+
+
+def synthetic_table(nrho=200, ntemp=100, nye=60, rho=(1e-14, 1e-2), temp=(0.01, 100.0),
+                    ye=(0.05, 0.6)):
+    """Uniform table on (ln rho, ln T, Ye) in the EOSX layout: 19 variables
+    per node, variable fastest, node = i_rho + nrho (i_T + ntemp i_Ye);
+    variable 0 ln P, 1 ln eps (energy shift 0, eps > 0 everywhere), 2 entropy,
+    4 cs^2, the others zero.  Returns (logrho, logtemp, ye, table)."""
+    lr = np.linspace(math.log(rho[0]), math.log(rho[1]), nrho)
+    lt = np.linspace(math.log(temp[0]), math.log(temp[1]), ntemp)
+    ys = np.linspace(ye[0], ye[1], nye)
+    Y, T, R = np.meshgrid(ys, np.exp(lt), np.exp(lr), indexing="ij")
+    press, eps, ent, cs2 = tab_thermo(R, T, Y)
+    table = np.zeros((nye, ntemp, nrho, TAB_NV))
+    table[..., TAB_LOGPRESS] = np.log(press)
+    table[..., TAB_LOGENERGY] = np.log(eps)
+    table[..., TAB_ENTROPY] = ent
+    table[..., TAB_CS2] = cs2
+    return lr, lt, ys, table.reshape(-1)
+
+
+def tabulated_box(n=24, ng=3, seed=5, wmax=10.0, sigma=(1e-3, 10.0), theta=(1e-2, 1.0),
+                  temp_scale=0.5, xp=None, **kw):
+    """Config-5 patch: the curved-metric box with Ye smooth in [0.05, 0.5],
+    densities brought inside the table (vector potential scaled by 10^-1.5, so
+    b^2 and rho drop by 10^-3; rho in [1e-10, 5e-3]) and the thermodynamics
+    of the synthetic table: T = temp_scale * (p/rho of the ideal-gas box),
+    clipped to [0.011, 90], then P, eps and entropy in closed form."""
+    xp = xp or _NP
+    L, f = curved_box(n=n, ng=ng, seed=seed, wmax=wmax, with_ye=True, sigma=sigma,
+                      theta=theta, xp=xp, a_amp=0.05 * 10 ** -1.5, rho_min=1e-10,
+                      rho_max=5e-3, **kw)
+    rho, ye = f["rho"], f["Ye"]
+    temp = xp.clip(temp_scale * f["press"] / rho, 0.011, 90.0)
+    press, eps, ent, _ = tab_thermo(rho, temp, ye, xp)
+    f["temperature"], f["press"], f["eps"], f["entropy"] = temp, press, eps, ent
     return L, f
 
 

@@ -214,6 +214,24 @@ AXB_API int axb_eos_create_idealgas(double gamma, double particle_mass,
                                     const double eps_range[2],
                                     const double ye_range[2], double poly_gamma,
                                     double poly_k, axb_eos **out);
+
+/* Tabulated3d EOS (eos_3p_tabulated3d) from a table already read and
+ * converted, in the state eos_3p_tabulated3d::init leaves it
+ * (EOSX/src/eos_3p_tabulated3d/eos_3p_tabulated3d.hxx:53-192; the HDF5 read
+ * itself stays with the caller): uniform axes logrho[nrho] and logtemp[ntemp]
+ * (natural logs), ye[nye], and `table` holding 19 variables per node,
+ * variable fastest, node = i_rho + nrho * (i_temp + ntemp * i_ye); variables
+ * 0 (ln press), 1 (ln(eps + energy_shift)), 2 (entropy) and 4 (cs^2) are
+ * used.  Ranges as at the end of init (:179-192).  Copies the four used
+ * variables to the current device (one cudaMalloc; 32 B per node).  The
+ * fluxes need reconstruct_with_temperature = 1 with this EOS, as in the
+ * reference.  Temperature inversions are capped at 10000 Brent steps
+ * (AXB_EW_ROOT_CAP). */
+AXB_API int axb_eos_create_tabulated3d(int nrho, int ntemp, int nye,
+                                       const double *logrho, const double *logtemp,
+                                       const double *ye, const double *table,
+                                       double energy_shift, double poly_gamma,
+                                       double poly_k, axb_eos **out);
 AXB_API int axb_eos_destroy(axb_eos *eos);
 
 /* ------------------------------------------------------------------------ */

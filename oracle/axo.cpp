@@ -506,6 +506,8 @@ void calc_flux(const EOS &eos, int dir) {
   const char *bnames[3][2] = {{"fxBy", "fxBz"}, {"fyBx", "fyBz"}, {"fzBx", "fzBy"}};
   const double *rho = need("rho"), *ent = need("entropy"), *ye = need("Ye"),
                *press = need("press");
+  const bool with_temp = g_p.reconstruct_with_temperature != 0;
+  const double *temp = with_temp ? need("temperature") : nullptr;
   const double *vel[3] = {need("velx"), need("vely"), need("velz")};
   const double *Bv[3] = {need("Bvecx"), need("Bvecy"), need("Bvecz")};
   const double *dBs[3] = {need("dBx_stag"), need("dBy_stag"), need("dBz_stag")};
@@ -539,13 +541,16 @@ void calc_flux(const EOS &eos, int dir) {
       recon_face(method, v, pr, vd, is_rho, o);
     };
     const int hi = g_p.reconstruction_method, lo = g_p.loworder_method;
-    double r_rho[2], r_ent[2], r_ye[2], r_p[2];
+    // the thermodynamic variable reconstructed beside rho, entropy and Ye:
+    // the temperature or the pressure (fluxes.cxx:257-355)
+    const double *thermo = with_temp ? temp : press;
+    double r_rho[2], r_ent[2], r_ye[2], r_p[2], r_t[2];
     rec(rho, hi, true, r_rho);
     rec(ent, hi, false, r_ent);
     rec(ye, hi, false, r_ye);
-    rec(press, hi, false, r_p);
-    const bool lo0 = r_rho[0] <= 0.0 || r_ent[0] <= 0.0 || r_ye[0] <= 0.0 || r_p[0] <= 0.0;
-    const bool lo1 = r_rho[1] <= 0.0 || r_ent[1] <= 0.0 || r_ye[1] <= 0.0 || r_p[1] <= 0.0;
+    rec(thermo, hi, false, r_t);
+    const bool lo0 = r_rho[0] <= 0.0 || r_ent[0] <= 0.0 || r_ye[0] <= 0.0 || r_t[0] <= 0.0;
+    const bool lo1 = r_rho[1] <= 0.0 || r_ent[1] <= 0.0 || r_ye[1] <= 0.0 || r_t[1] <= 0.0;
     auto lowfix = [&](const double *f, bool is_rho, double o[2]) {
       double t[2];
       if (lo0) {
@@ -560,11 +565,17 @@ void calc_flux(const EOS &eos, int dir) {
     lowfix(rho, true, r_rho);
     lowfix(ent, false, r_ent);
     lowfix(ye, false, r_ye);
-    lowfix(press, false, r_p);
+    lowfix(thermo, false, r_t);
     double eps[2];
     for (int f = 0; f < 2; ++f) {
-      eps[f] = eos.eps_rp(r_rho[f], r_p[f], r_ye[f]);
-      (void)eos.temp_re(r_rho[f], eps[f], r_ye[f]); // may clamp eps (tabulated)
+      if (with_temp) {
+        eps[f] = eos.eps_rt(r_rho[f], r_t[f], r_ye[f]);
+        r_p[f] = eos.press_rt(r_rho[f], r_t[f], r_ye[f]);
+      } else {
+        r_p[f] = r_t[f];
+        eps[f] = eos.eps_rp(r_rho[f], r_p[f], r_ye[f]);
+        (void)eos.temp_re(r_rho[f], eps[f], r_ye[f]); // may clamp eps (tabulated)
+      }
     }
     double B[3][2];
     B[dir][0] = B[dir][1] = dBs[dir][I] / sqrtg;
@@ -1855,8 +1866,8 @@ void ora_eos_tab_ranges(double *o) {
 
 int ora_fluxes(void) {
   return guarded([] {
-    if (g_p.recon_type != AXB_RECVAR_V || g_p.reconstruct_with_temperature)
-      throw Fail("only v_vec reconstruction of the pressure is restated");
+    if (g_p.recon_type != AXB_RECVAR_V)
+      throw Fail("only v_vec reconstruction is restated");
     with_eos([](const auto &eos) {
       for (int d = 0; d < 3; ++d)
         calc_flux(eos, d);

@@ -139,3 +139,86 @@ def test_minmod_identities(axo):
         out = axo.reconstruct(abi.RECON["minmod"], v)
         mm = 0.0 if np.signbit(s1) != np.signbit(s2) else (s1 if abs(s1) < abs(s2) else s2)
         assert out[0] == v[2] + mm / 2
+
+
+# ---------------------------------------------------------------------------
+# tabulated3d EOS (synthetic table of the 192^3 tabulated configuration)
+# ---------------------------------------------------------------------------
+TAB = None
+
+
+def tab():
+    global TAB
+    if TAB is None:
+        TAB = W.synthetic_table()
+    return TAB
+
+
+def run_tab(lib, L, f, p, what):
+    host = {n: a.copy() for n, a in f.items()}
+    lib.setup(L, p, host)
+    lib.eos_tabulated(*tab())
+    getattr(lib, what)()
+    return lib.fields
+
+
+def test_tab_queries_bitwise(ref, axo):
+    for lib in (ref, axo):
+        lib.setup(W.Layout((4, 4, 4), 3, (1, 1, 1), (0, 0, 0)), abi.default_params(), {})
+        lib.eos_tabulated(*tab())
+    assert np.array_equal(ref.tab_ranges(), axo.tab_ranges())
+    rng = np.random.default_rng(11)
+    for _ in range(300):
+        rho = 10 ** rng.uniform(-15, -1)
+        ye = rng.uniform(0.0, 0.7)
+        eps = 10 ** rng.uniform(-3, 3)
+        temp = 10 ** rng.uniform(-2.5, 2.5)
+        for which in range(4):
+            a, b = ref.tab_query(which, rho, eps, ye), axo.tab_query(which, rho, eps, ye)
+            assert np.array_equal(np.asarray(a), np.asarray(b)), (which, rho, eps, ye)
+        for which in (4, 5, 6):
+            a, b = ref.tab_query(which, rho, temp, ye), axo.tab_query(which, rho, temp, ye)
+            assert np.array_equal(np.asarray(a), np.asarray(b)), (which, rho, temp, ye)
+
+
+def test_tab_thermo_matches_table():
+    """The table interpolates the closed-form thermodynamics it was built from."""
+    lr, lt, ye, t = tab()
+    t = t.reshape(len(ye), len(lt), len(lr), W.TAB_NV)
+    k, j, i = 17, 43, 101
+    pr, eps, ent, cs2 = W.tab_thermo(np.exp(lr[i]), np.exp(lt[j]), ye[k])
+    assert t[k, j, i, W.TAB_LOGPRESS] == np.log(pr)
+    assert t[k, j, i, W.TAB_LOGENERGY] == np.log(eps)
+    assert 0 < cs2 < 1
+
+
+@pytest.mark.parametrize("recon", ["mp5", "ppm"])
+def test_rhs_group_tabulated_bitwise(ref, axo, recon):
+    L, f = W.tabulated_box(n=8, ng=5, seed=5, wmax=2.0, sigma=(1e-3, 0.3),
+                           theta=(0.1, 1.0))
+    f = full_fields(L, f)
+    p = abi.default_params(reconstruction_method=recon, flux_type="hlle",
+                           reconstruct_with_temperature=1)
+    a = run_tab(ref, L, f, p, "rhs_group")
+    b = run_tab(axo, L, f, p, "rhs_group")
+    for n in RHS_OUT:
+        x, y = interior(L, n, a[n]), interior(L, n, b[n])
+        assert np.isfinite(x).all() and np.array_equal(x, y), n
+
+
+@pytest.mark.parametrize("prime,second", [("noble", "palenzuela"),
+                                          ("palenzuela", "noble")])
+def test_con2prim_group_tabulated_bitwise(ref, axo, prime, second):
+    L, f = W.tabulated_box(n=8, ng=5, seed=6, wmax=3.0)
+    W.cons_from_prims(L, f)
+    W.perturbed_saved(f, seed=4)
+    f = full_fields(L, f)
+    p = abi.default_params(c2p_prime=prime, c2p_second=second, c2p_tol=1e-12,
+                           max_iter=60, reconstruct_with_temperature=1)
+    a = run_tab(ref, L, f, p, "con2prim_group")
+    b = run_tab(axo, L, f, p, "con2prim_group")
+    for n in C2P_OUT:
+        x, y = interior(L, n, a[n]), interior(L, n, b[n])
+        assert np.array_equal(x, y, equal_nan=True), n
+    flags = interior(L, "con2prim_flag", a["con2prim_flag"])
+    print("flags", np.unique(flags, return_counts=True))
