@@ -107,8 +107,12 @@ AXB_D void run_solver(int which, const EOS &eos, const C2PBoxArgs &a,
 
 // One cell of AsterX_Con2Prim_typeEoS (con2prim.cxx:81-453), preceded by
 // AsterX_ComputedBFromdBstag (computeBfromA.cxx:67-85) for the same cell.
+#ifndef AXB_C2P_MINB
+#define AXB_C2P_MINB 4 // resident CTAs per SM the register budget must allow
+#endif
 template <class EOS>
-__global__ void __launch_bounds__(128) k_c2p_box(const C2PBoxArgs a, const EOS eos) {
+__global__ void __launch_bounds__(128, AXB_C2P_MINB)
+    k_c2p_box(const C2PBoxArgs a, const EOS eos) {
   __shared__ unsigned int s_hist[64];
   const BoxDev &b = a.b;
   if (a.want_hist) {

@@ -128,6 +128,10 @@ AXB_HD CellLoUp recon_ppm(const double q[5], const double pr[5],
 }
 
 AXB_HD CellLoUp recon_wenoz(const double q[5], double weno_eps) {
+  // Same weights and candidate stencils as the reference; the divisions by
+  // the weight sums and by 6 are folded into one reciprocal per side, which
+  // changes results only at the last-ulp level (5 FP64 divisions per cell
+  // instead of 15).
   const double a = q[0], b = q[1], c = q[2], d = q[3], e = q[4];
   const double beta0 = (13.0 / 12.0) * sq(a - 2.0 * b + c) +
                        (1.0 / 4.0) * sq(a - 4.0 * b + 3.0 * c);
@@ -143,22 +147,23 @@ AXB_HD CellLoUp recon_wenoz(const double q[5], double weno_eps) {
   // minus side (lower value): weights w0, w1, w2; plus side: w2, w1, w0
   const double am0 = w0 * aux0, am1 = w1 * aux1, am2 = w2 * aux2;
   const double ap0 = w2 * aux0, ap1 = w1 * aux1, ap2 = w0 * aux2;
-  const double dm = am0 + am1 + am2;
-  const double dp = ap0 + ap1 + ap2;
-  const double om0 = am0 / dm, om1 = am1 / dm, om2 = am2 / dm;
-  const double op0 = ap0 / dp, op1 = ap1 / dp, op2 = ap2 / dp;
-  const double var_m = (om2 / 6.0) * (2.0 * e - 7.0 * d + 11.0 * c) +
-                       (om1 / 6.0) * (-1.0 * d + 5.0 * c + 2.0 * b) +
-                       (om0 / 6.0) * (2.0 * c + 5.0 * b - 1.0 * a);
-  const double var_p = (op0 / 6.0) * (2.0 * a - 7.0 * b + 11.0 * c) +
-                       (op1 / 6.0) * (-1.0 * b + 5.0 * c + 2.0 * d) +
-                       (op2 / 6.0) * (2.0 * c + 5.0 * d - 1.0 * e);
+  const double idm6 = 1.0 / (6.0 * (am0 + am1 + am2));
+  const double idp6 = 1.0 / (6.0 * (ap0 + ap1 + ap2));
+  const double var_m = (am2 * (2.0 * e - 7.0 * d + 11.0 * c) +
+                        am1 * (-1.0 * d + 5.0 * c + 2.0 * b) +
+                        am0 * (2.0 * c + 5.0 * b - 1.0 * a)) *
+                       idm6;
+  const double var_p = (ap0 * (2.0 * a - 7.0 * b + 11.0 * c) +
+                        ap1 * (-1.0 * b + 5.0 * c + 2.0 * d) +
+                        ap2 * (2.0 * c + 5.0 * d - 1.0 * e)) *
+                       idp6;
   return {var_m, var_p};
 }
 
 // MP5 interface value of the middle cell towards u_p1's side.
 AXB_HD double mp5_one(double gf_Imm, double gf_Im, double gf_I, double gf_Ip,
                       double gf_Ipp, double alpha) {
+  // (kept as the reference's division: ul feeds the early-accept test)
   const double ul = (2 * gf_Imm - 13 * gf_Im + 47 * gf_I + 27 * gf_Ip - 3 * gf_Ipp) / 60.0;
   const double deltam = gf_I - gf_Im;
   const double deltap = gf_Ip - gf_I;

@@ -124,7 +124,10 @@ AXB_D void side_physics(const FaceMetric &m, const double *r, double Bdir,
   B[D2] = r[R_B2];
   double vlow[3];
   lower3(m.g, vel, vlow);
-  const double W = 1 / sqrt(1 - dot3(vlow, vel));
+  // 1/W is used in four places: take it as the square root itself and
+  // multiply (last-ulp differences from the reference's divisions by W)
+  const double iW = sqrt(1 - dot3(vlow, vel));
+  const double W = 1 / iW;
   double vt[3];
   for (int i = 0; i < 3; ++i)
     vt[i] = m.alp * vel[i] - m.beta[i];
@@ -134,8 +137,8 @@ AXB_D void side_physics(const FaceMetric &m, const double *r, double Bdir,
   const double B2 = dot3(B, Blow);
   double blow[3];
   for (int i = 0; i < 3; ++i)
-    blow[i] = Blow[i] / W + alp_b0 * vlow[i];
-  const double bsq = (B2 + sq(alp_b0)) / sq(W);
+    blow[i] = Blow[i] * iW + alp_b0 * vlow[i];
+  const double bsq = (B2 + sq(alp_b0)) * sq(iW);
   // cs^2 as the product of two sound-speed queries (fluxes.cxx:556-560); the
   // first may clamp eps in place (tabulated), and only then can the second
   // differ from the first
@@ -152,7 +155,7 @@ AXB_D void side_physics(const FaceMetric &m, const double *r, double Bdir,
   const double ppm = press + 0.5 * bsq;
   const double vtd = vt[DIR];
   const double alp_sqrtg = m.alp * m.sqrtg;
-  const double BoW = B[DIR] / W;
+  const double BoW = B[DIR] * iW;
   o.U[0] = dens;
   o.F[0] = dens * vtd;
   for (int j = 0; j < 3; ++j) {
@@ -202,8 +205,9 @@ AXB_D void side_physics(const FaceMetric &m, const double *r, double Bdir,
   if (det < 0)
     det = 0;
   const double sd = sqrt(det);
-  o.lam_p = ((-a1 + sd) / (2 * a2)) / m.alp;
-  o.lam_m = ((-a1 - sd) / (2 * a2)) / m.alp;
+  const double i2a2alp = 1 / (2 * a2 * m.alp);
+  o.lam_p = (-a1 + sd) * i2a2alp;
+  o.lam_m = (-a1 - sd) * i2a2alp;
 }
 
 } // namespace axb

@@ -21,21 +21,146 @@ AXB_D double warp_max(double v) {
 }
 
 // ---------------------------------------------------------------------------
-// k_flux_pass: one thread marches one pencil segment along DIR.  Per step it
-// reconstructs one cell (both interface values, ReconX per-cell formulas),
-// forms the face between the previous cell and this one, computes the ten
-// Riemann fluxes, stores the two transverse B fluxes (for flux-CT), and
+// Shared pieces of the flux passes.
+// ---------------------------------------------------------------------------
+
+// Reconstruct the NREC variables of the cell at I (stride sd along DIR).
+template <int DIR, int RECON>
+AXB_D void recon_cell_all(const RhsArgs &a, const double *const (&fld)[NREC],
+                          long long I, long long sd, double (&lo)[NREC],
+                          double (&up)[NREC]) {
+  double pr[5], vd[5];
+  load_pencil<5>(a.press, I, sd, pr);
+  load_pencil<5>(a.vel[DIR], I, sd, vd);
+#pragma unroll
+  for (int v = 0; v < NREC; ++v) {
+    double q[5];
+    if (v == R_PRESS && !a.rec_temp) {
+#pragma unroll
+      for (int m = 0; m < 5; ++m) q[m] = pr[m];
+    } else if (v == R_VX + DIR) {
+#pragma unroll
+      for (int m = 0; m < 5; ++m) q[m] = vd[m];
+    } else {
+      load_pencil<5>(fld[v], I, sd, q);
+    }
+    const CellLoUp r = recon_cell<RECON>(q, pr, vd, v == R_RHO, a.rp);
+    lo[v] = r.lo;
+    up[v] = r.up;
+  }
+}
+
+// The face between the cells at I - sd and I, given the left state L (upper
+// values of the left cell) and the right state R (lower values of the right
+// cell): low-order redo of a side with a non-positive rho, entropy, Ye or
+// thermodynamic variable (fluxes.cxx:263-343), face metric, both states'
+// conserved variables, fluxes and fast speeds, and the Riemann flux
+// (HLLE or LxF, fluxes.cxx:162-200).  Stores the two transverse B fluxes
+// when asked.
+template <int DIR, class EOS>
+AXB_D void face_fluxes(const RhsArgs &a, const EOS &eos,
+                       const double *const (&fld)[NREC], long long I, long long sd,
+                       double (&L)[NREC], double (&R)[NREC], double (&F)[10],
+                       double &smax, bool &bad) {
+  constexpr int D1 = (DIR + 1) % 3, D2 = (DIR + 2) % 3;
+  const bool lo0 = (L[R_RHO] <= 0.0) || (L[R_ENT] <= 0.0) ||
+                   (L[R_YE] <= 0.0) || (L[R_PRESS] <= 0.0);
+  const bool lo1 = (R[R_RHO] <= 0.0) || (R[R_ENT] <= 0.0) ||
+                   (R[R_YE] <= 0.0) || (R[R_PRESS] <= 0.0);
+  if (lo0 || lo1) {
+    for (int v = 0; v < NREC; ++v) {
+      double q[5];
+      if (lo0) {
+        load_pencil<5>(fld[v], I - sd, sd, q);
+        L[v] = recon_cell_lo(a.recon_lo, q).up;
+      }
+      if (lo1) {
+        load_pencil<5>(fld[v], I, sd, q);
+        R[v] = recon_cell_lo(a.recon_lo, q).lo;
+      }
+    }
+  }
+  const FaceMetric m = face_metric<DIR>(a, I);
+  const double Bdir = __ldg(a.dBstag[DIR] + I) / m.sqrtg;
+  SideOut sL, sR;
+  side_physics<DIR>(m, L, Bdir, eos, a.rec_temp, sL);
+  side_physics<DIR>(m, R, Bdir, eos, a.rec_temp, sR);
+  const double cmax = fmax(0.0, fmax(fmax(sL.lam_p, sL.lam_m), fmax(sR.lam_p, sR.lam_m)));
+  const double cmin = fmin(0.0, fmin(fmin(sL.lam_p, sL.lam_m), fmin(sR.lam_p, sR.lam_m)));
+  smax = fmax(smax, fmax(cmax, -cmin));
+  if (a.flux_type == AXB_FLUX_HLLE) {
+    const double icpm = 1 / (cmax - cmin);
+#pragma unroll
+    for (int v = 0; v < 10; ++v)
+      F[v] = (cmax * sL.F[v] - cmin * sR.F[v] + cmax * cmin * (sR.U[v] - sL.U[v])) * icpm;
+  } else {
+    const double ch = fmax(cmax, -cmin);
+#pragma unroll
+    for (int v = 0; v < 10; ++v)
+      F[v] = 0.5 * ((sL.F[v] + sR.F[v]) - ch * (sR.U[v] - sL.U[v]));
+  }
+#pragma unroll
+  for (int v = 0; v < 10; ++v)
+    bad |= isnan(F[v]);
+  if (a.write_bflux) {
+    // bflux slots per direction hold the two transverse components in
+    // ascending order: x (y, z), y (x, z), z (x, y)
+    constexpr int BLO = D1 < D2 ? D1 : D2, BHI = D1 < D2 ? D2 : D1;
+    a.bflux[2 * DIR + 0][I] = F[7 + BLO];
+    a.bflux[2 * DIR + 1][I] = F[7 + BHI];
+  }
+}
+
+// Fold F(face c+1) - F(face c) into the partial divergence of cell c (at I),
+// in the reference's summation order (rhs.cxx:188-207): x writes, y adds,
+// z adds and forms the RHS.
+template <int DIR>
+AXB_D void fold_divergence(const RhsArgs &a, long long I, double idxd,
+                           const double (&Fhi)[NHYDRO], const double (&Flo)[NHYDRO]) {
+#pragma unroll
+  for (int v = 0; v < NHYDRO; ++v) {
+    const double dF = Fhi[v] - Flo[v];
+    if (DIR == 0)
+      a.acc[v][I] = idxd * dF;
+    else if (DIR == 1)
+      a.acc[v][I] = a.acc[v][I] + idxd * dF;
+    else
+      a.rhs[v][I] = a.rhs[v][I] + (-(a.acc[v][I] + idxd * dF));
+  }
+}
+
+AXB_D void flux_status(const RhsArgs &a, double smax, bool bad) {
+  // characteristic-speed maximum: warp shuffle, one atomic per warp
+  smax = warp_max(smax);
+  if ((threadIdx.x + threadIdx.y * blockDim.x) % 32 == 0)
+    atomic_max_nonneg(&a.status->max_speed_bits, smax);
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x + threadIdx.y * blockDim.x) % 32 == 0)
+    atomicOr(&a.status->error_word, AXB_EW_NAN_FLUX);
+}
+
+#ifndef AXB_FLUX_MINB
+#define AXB_FLUX_MINB 4 // resident CTAs per SM the register budget must allow
+#endif
+#ifndef AXB_FLUX_X_MINB
+#define AXB_FLUX_X_MINB 4
+#endif
+
+// ---------------------------------------------------------------------------
+// k_flux_pass (y and z): one thread marches one pencil segment along DIR.
+// Per step it reconstructs one cell (both interface values, ReconX per-cell
+// formulas), forms the face between the previous cell and this one, and
 // folds F(face) - F(face-1) into the partial divergence of the previous cell.
-// Threads of a warp are adjacent along the fast transverse axis, so every
-// load of a y- or z-pass is a coalesced 256-byte row.
+// Threads of a warp are adjacent along x, so every load is a coalesced
+// 256-byte row.
 // Transverse range: cells [ng-1, ng+n] (one ghost layer each side, needed
 // by the edge electric field); faces along DIR: [ng, ng+n].
 // ---------------------------------------------------------------------------
 template <int DIR, int RECON, class EOS>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, AXB_FLUX_MINB)
     k_flux_pass(const RhsArgs a, const EOS eos, const int seglen) {
+  static_assert(DIR != 0, "the x pass is k_flux_x");
   constexpr int D1 = (DIR + 1) % 3, D2 = (DIR + 2) % 3;
-  constexpr int T0 = (DIR == 0) ? 1 : 0;
+  constexpr int T0 = 0;
   constexpr int T1 = (DIR == 2) ? 1 : 2;
   const BoxDev &b = a.b;
   const int ng = b.ng;
@@ -55,104 +180,30 @@ __global__ void __launch_bounds__(128)
     ijk[T1] = t1;
     ijk[DIR] = f0 - 1;
     long long I = b.at(ijk[0], ijk[1], ijk[2]);
-    const double *fld[NREC] = {a.rho,    a.entropy, a.Ye,       a.thermo,
-                               a.vel[0], a.vel[1],  a.vel[2],   a.Bvec[D1],
-                               a.Bvec[D2]};
+    const double *const fld[NREC] = {a.rho,    a.entropy, a.Ye,       a.thermo,
+                                     a.vel[0], a.vel[1],  a.vel[2],   a.Bvec[D1],
+                                     a.Bvec[D2]};
     const double idxd = b.idx[DIR];
     double upL[NREC];
     double Fprev[NHYDRO];
     for (int c = f0 - 1; c <= flast; ++c, I += sd) {
       double lo[NREC], up[NREC];
-      double pr[5], vd[5];
-      load_pencil<5>(a.press, I, sd, pr);
-      load_pencil<5>(a.vel[DIR], I, sd, vd);
-#pragma unroll
-      for (int v = 0; v < NREC; ++v) {
-        double q[5];
-        if (v == R_PRESS && !a.rec_temp) {
-#pragma unroll
-          for (int m = 0; m < 5; ++m) q[m] = pr[m];
-        } else if (v == R_VX + DIR) {
-#pragma unroll
-          for (int m = 0; m < 5; ++m) q[m] = vd[m];
-        } else {
-          load_pencil<5>(fld[v], I, sd, q);
-        }
-        const CellLoUp r = recon_cell<RECON>(q, pr, vd, v == R_RHO, a.rp);
-        lo[v] = r.lo;
-        up[v] = r.up;
-      }
+      recon_cell_all<DIR, RECON>(a, fld, I, sd, lo, up);
       if (c >= f0) {
         // face c: left state = upper values of cell c-1, right = lower of c
-        double L[NREC], R[NREC];
+        double L[NREC], R[NREC], F[10];
 #pragma unroll
         for (int v = 0; v < NREC; ++v) {
           L[v] = upL[v];
           R[v] = lo[v];
         }
-        const bool lo0 = (L[R_RHO] <= 0.0) || (L[R_ENT] <= 0.0) ||
-                         (L[R_YE] <= 0.0) || (L[R_PRESS] <= 0.0);
-        const bool lo1 = (R[R_RHO] <= 0.0) || (R[R_ENT] <= 0.0) ||
-                         (R[R_YE] <= 0.0) || (R[R_PRESS] <= 0.0);
-        if (lo0 || lo1) { // low-order redo (fluxes.cxx:313-343)
-          for (int v = 0; v < NREC; ++v) {
-            double q[5];
-            if (lo0) {
-              load_pencil<5>(fld[v], I - sd, sd, q);
-              L[v] = recon_cell_lo(a.recon_lo, q).up;
-            }
-            if (lo1) {
-              load_pencil<5>(fld[v], I, sd, q);
-              R[v] = recon_cell_lo(a.recon_lo, q).lo;
-            }
-          }
-        }
-        const FaceMetric m = face_metric<DIR>(a, I);
-        const double Bdir = __ldg(a.dBstag[DIR] + I) / m.sqrtg;
-        SideOut sL, sR;
-        side_physics<DIR>(m, L, Bdir, eos, a.rec_temp, sL);
-        side_physics<DIR>(m, R, Bdir, eos, a.rec_temp, sR);
-        const double cmax = fmax(0.0, fmax(fmax(sL.lam_p, sL.lam_m),
-                                           fmax(sR.lam_p, sR.lam_m)));
-        const double cmin = fmin(0.0, fmin(fmin(sL.lam_p, sL.lam_m),
-                                           fmin(sR.lam_p, sR.lam_m)));
-        smax = fmax(smax, fmax(cmax, -cmin));
-        double F[10];
-        if (a.flux_type == AXB_FLUX_HLLE) {
-          const double cpm = cmax - cmin;
-#pragma unroll
-          for (int v = 0; v < 10; ++v)
-            F[v] = (cmax * sL.F[v] - cmin * sR.F[v] +
-                    cmax * cmin * (sR.U[v] - sL.U[v])) /
-                   cpm;
-        } else {
-          const double ch = fmax(cmax, -cmin);
-#pragma unroll
-          for (int v = 0; v < 10; ++v)
-            F[v] = 0.5 * ((sL.F[v] + sR.F[v]) - ch * (sR.U[v] - sL.U[v]));
-        }
-#pragma unroll
-        for (int v = 0; v < 10; ++v)
-          bad |= isnan(F[v]);
-        if (a.write_bflux) {
-          // bflux slots per direction hold the two transverse components in
-          // ascending order: x (y, z), y (x, z), z (x, y)
-          constexpr int BLO = D1 < D2 ? D1 : D2, BHI = D1 < D2 ? D2 : D1;
-          a.bflux[2 * DIR + 0][I] = F[7 + BLO];
-          a.bflux[2 * DIR + 1][I] = F[7 + BHI];
-        }
+        face_fluxes<DIR>(a, eos, fld, I, sd, L, R, F, smax, bad);
         if (c > f0 && trans_int) {
-          const long long Ic = I - sd;
+          double Fc[NHYDRO];
 #pragma unroll
-          for (int v = 0; v < NHYDRO; ++v) {
-            const double dF = F[v] - Fprev[v];
-            if (DIR == 0)
-              a.acc[v][Ic] = idxd * dF;
-            else if (DIR == 1)
-              a.acc[v][Ic] = a.acc[v][Ic] + idxd * dF;
-            else
-              a.rhs[v][Ic] = a.rhs[v][Ic] + (-(a.acc[v][Ic] + idxd * dF));
-          }
+          for (int v = 0; v < NHYDRO; ++v)
+            Fc[v] = F[v];
+          fold_divergence<DIR>(a, I - sd, idxd, Fc, Fprev);
         }
 #pragma unroll
         for (int v = 0; v < NHYDRO; ++v)
@@ -163,13 +214,78 @@ __global__ void __launch_bounds__(128)
         upL[v] = up[v];
     }
   }
-  // characteristic-speed maximum: warp shuffle, one atomic per warp
-  smax = warp_max(smax);
-  if ((threadIdx.x + threadIdx.y * blockDim.x) % 32 == 0)
-    atomic_max_nonneg(&a.status->max_speed_bits, smax);
-  if (__any_sync(0xffffffffu, bad) &&
-      (threadIdx.x + threadIdx.y * blockDim.x) % 32 == 0)
-    atomicOr(&a.status->error_word, AXB_EW_NAN_FLUX);
+  flux_status(a, smax, bad);
+}
+
+// ---------------------------------------------------------------------------
+// k_flux_x: the x pass with the lanes of a warp along x, so that every
+// stencil load is a coalesced row segment (a thread marching along x would
+// touch 32 rows per load and lose its sectors before coming back to them).
+// Each warp owns one (y, z) row and walks it in chunks of 32 cells that
+// overlap by two: lane l reconstructs cell c0 + l once, takes the left state
+// of its face (c0 + l) from lane l - 1 by shuffle, computes the face, and
+// takes the flux of face c0 + l + 1 from lane l + 1 to form the divergence
+// of its cell.  Lanes 1..31 compute faces, lanes 1..30 divergences; a chunk
+// advances 30 cells.
+// ---------------------------------------------------------------------------
+template <int RECON, class EOS>
+__global__ void __launch_bounds__(128, AXB_FLUX_X_MINB)
+    k_flux_x(const RhsArgs a, const EOS eos) {
+  const BoxDev &b = a.b;
+  const int ng = b.ng;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int ny = b.n[1] + 2; // rows j, k in [ng-1, ng+n]
+  const int nz = b.n[2] + 2;
+  double smax = 0.0;
+  bool bad = false;
+  if (warp < ny * nz) { // warp-uniform
+    const int j = ng - 1 + warp % ny;
+    const int k = ng - 1 + warp / ny;
+    const bool trans_int = (j >= ng) && (j < ng + b.n[1]) && (k >= ng) && (k < ng + b.n[2]);
+    const double *const fld[NREC] = {a.rho,    a.entropy, a.Ye,     a.thermo, a.vel[0],
+                                     a.vel[1], a.vel[2],  a.Bvec[1], a.Bvec[2]};
+    const double idxd = b.idx[0];
+    const long long row = b.at(0, j, k);
+    const int clast = ng + b.n[0]; // last cell needed (right state of the last face)
+    for (int c0 = ng - 1; c0 < ng + b.n[0] - 1; c0 += 30) {
+      const int c = c0 + lane;
+      const bool has_cell = c <= clast;
+      const long long I = row + c;
+      double lo[NREC], up[NREC];
+      if (has_cell) {
+        recon_cell_all<0, RECON>(a, fld, I, 1, lo, up);
+      } else {
+#pragma unroll
+        for (int v = 0; v < NREC; ++v)
+          lo[v] = up[v] = 0.0;
+      }
+      double L[NREC], R[NREC], F[10];
+#pragma unroll
+      for (int v = 0; v < NREC; ++v) {
+        L[v] = __shfl_up_sync(0xffffffffu, up[v], 1);
+        R[v] = lo[v];
+      }
+      const bool has_face = lane >= 1 && has_cell; // face c in [ng, ng+n]
+      if (has_face) {
+        face_fluxes<0>(a, eos, fld, I, 1, L, R, F, smax, bad);
+      } else {
+#pragma unroll
+        for (int v = 0; v < 10; ++v)
+          F[v] = 0.0;
+      }
+      double Fhi[NHYDRO], Flo[NHYDRO];
+#pragma unroll
+      for (int v = 0; v < NHYDRO; ++v) {
+        Flo[v] = F[v];
+        Fhi[v] = __shfl_down_sync(0xffffffffu, F[v], 1);
+      }
+      // cell c's divergence needs faces c and c+1
+      if (trans_int && lane >= 1 && lane <= 30 && c < ng + b.n[0])
+        fold_divergence<0>(a, I, idxd, Fhi, Flo);
+    }
+  }
+  flux_status(a, smax, bad);
 }
 
 } // namespace axb

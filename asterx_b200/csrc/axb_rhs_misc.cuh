@@ -9,7 +9,66 @@ namespace axb {
 // ---------------------------------------------------------------------------
 // k_sources: geometric source terms (AsterX/src/source.cxx:32-167); writes
 // the seven hydro RHS (dens, DEnt, DYe sources are zero).
+//
+// Each vertex field is read once per cell as its 8 cube corners, from which
+// the cell average (calc_avg_v2c, AsterUtils/src/aster_interp.hxx) and, at
+// second order, the three edge-averaged derivatives (calc_fd_v2c,
+// AsterUtils/src/aster_fd.hxx:49-64) are formed in registers.  The
+// derivatives multiply by 1/dx once instead of dividing each edge difference
+// by dx (last-ulp differences).
 // ---------------------------------------------------------------------------
+struct V2C {
+  double avg, d[3];
+};
+
+// corner (bx, by, bz) of the cell at I is c[bx + 2 by + 4 bz]
+template <int FD>
+AXB_D V2C v2c_field(const double *__restrict__ f, long long I, const BoxDev &b) {
+  const long long sy = b.sy, sz = b.sz;
+  double c[8];
+  c[0] = __ldg(f + I);
+  c[1] = __ldg(f + I + 1);
+  c[2] = __ldg(f + I + sy);
+  c[3] = __ldg(f + I + 1 + sy);
+  c[4] = __ldg(f + I + sz);
+  c[5] = __ldg(f + I + 1 + sz);
+  c[6] = __ldg(f + I + sy + sz);
+  c[7] = __ldg(f + I + 1 + sy + sz);
+#ifdef AXB_SOURCES_SEQ
+  // keep the compiler from hoisting every field's corner loads up front
+  asm volatile("" ::: "memory");
+#endif
+  V2C r;
+  double s = 0.0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q)
+    s += c[q];
+  r.avg = s / 8.0;
+  if (FD == 2) {
+    // edges along d from the base corners I, I+s1, I+s2, I+s1+s2
+    r.d[0] = ((c[1] - c[0]) + (c[3] - c[2]) + (c[5] - c[4]) + (c[7] - c[6])) * (0.25 * b.idx[0]);
+    r.d[1] = ((c[2] - c[0]) + (c[6] - c[4]) + (c[3] - c[1]) + (c[7] - c[5])) * (0.25 * b.idx[1]);
+    r.d[2] = ((c[4] - c[0]) + (c[5] - c[1]) + (c[6] - c[2]) + (c[7] - c[3])) * (0.25 * b.idx[2]);
+  } else {
+    // calc_fd_v2c<4> (aster_fd.hxx:77-110): 4-point differences along each edge
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
+      const long long st = b.stride(d), s1 = b.stride(d1), s2 = b.stride(d2);
+      const long long base[4] = {I, I + s1, I + s2, I + s1 + s2};
+      double e = 0.0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const long long J = base[q];
+        e += (1.0 / 24.0) * __ldg(f + J - st) - (27.0 / 24.0) * __ldg(f + J) +
+             (27.0 / 24.0) * __ldg(f + J + st) - (1.0 / 24.0) * __ldg(f + J + 2 * st);
+      }
+      r.d[d] = e * (0.25 * b.idx[d]);
+    }
+  }
+  return r;
+}
+
 AXB_D double avg_v2c(const double *__restrict__ f, long long I, long long sy,
                      long long sz) {
   double s = 0.0;
@@ -24,32 +83,13 @@ AXB_D double avg_v2c(const double *__restrict__ f, long long I, long long sy,
   return s / 8.0;
 }
 
-// calc_fd_v2c (AsterUtils/src/aster_fd.hxx:49-110): derivative along d of a
-// vertex function, averaged from the four edges of the cell.
-template <int FD>
-AXB_D double fd_v2c(const double *__restrict__ f, long long I, const BoxDev &b,
-                    int d) {
-  const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
-  const long long s = b.stride(d), s1 = b.stride(d1), s2 = b.stride(d2);
-  const double dx = b.dx[d];
-  const long long base[4] = {I, I + s1, I + s2, I + s1 + s2};
-  double e[4];
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const long long J = base[q];
-    if (FD == 2) {
-      e[q] = (__ldg(f + J + s) - __ldg(f + J)) / dx;
-    } else {
-      e[q] = ((1.0 / 24.0) * __ldg(f + J - s) - (27.0 / 24.0) * __ldg(f + J) +
-              (27.0 / 24.0) * __ldg(f + J + s) - (1.0 / 24.0) * __ldg(f + J + 2 * s)) /
-             dx;
-    }
-  }
-  return 0.25 * (e[0] + e[1] + e[2] + e[3]);
-}
+AXB_HD double sym_get(const sym3 &m, int p, int q) { return m(p, q); }
 
+#ifndef AXB_SOURCES_MINB
+#define AXB_SOURCES_MINB 1
+#endif
 template <int FD>
-__global__ void __launch_bounds__(128) k_sources(const RhsArgs a) {
+__global__ void __launch_bounds__(128, AXB_SOURCES_MINB) k_sources(const RhsArgs a) {
   const BoxDev &b = a.b;
   const int i = b.ng + blockIdx.x * blockDim.x + threadIdx.x;
   const int j = b.ng + blockIdx.y;
@@ -58,17 +98,38 @@ __global__ void __launch_bounds__(128) k_sources(const RhsArgs a) {
     return;
   const long long I = b.at(i, j, k);
   const long long sy = b.sy, sz = b.sz;
-  const double alp = avg_v2c(a.alp, I, sy, sz);
-  double beta[3];
-  for (int q = 0; q < 3; ++q)
-    beta[q] = avg_v2c(a.beta[q], I, sy, sz);
+  double d_alp[3], d_beta[3][3];
+  sym3 d_g[3];
+  double alp, beta[3];
   sym3 g, K;
-  g.xx = avg_v2c(a.g[0], I, sy, sz);
-  g.xy = avg_v2c(a.g[1], I, sy, sz);
-  g.xz = avg_v2c(a.g[2], I, sy, sz);
-  g.yy = avg_v2c(a.g[3], I, sy, sz);
-  g.yz = avg_v2c(a.g[4], I, sy, sz);
-  g.zz = avg_v2c(a.g[5], I, sy, sz);
+  {
+    const V2C r = v2c_field<FD>(a.alp, I, b);
+    alp = r.avg;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      d_alp[d] = r.d[d];
+  }
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const V2C r = v2c_field<FD>(a.beta[q], I, b);
+    beta[q] = r.avg;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      d_beta[d][q] = r.d[d];
+  }
+  double gv[6], dgv[6][3];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    const V2C r = v2c_field<FD>(a.g[q], I, b);
+    gv[q] = r.avg;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      dgv[q][d] = r.d[d];
+  }
+  g = sym3{gv[0], gv[1], gv[2], gv[3], gv[4], gv[5]};
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    d_g[d] = sym3{dgv[0][d], dgv[1][d], dgv[2][d], dgv[3][d], dgv[4][d], dgv[5][d]};
   K.xx = avg_v2c(a.K[0], I, sy, sz);
   K.xy = avg_v2c(a.K[1], I, sy, sz);
   K.xz = avg_v2c(a.K[2], I, sy, sz);
@@ -78,48 +139,41 @@ __global__ void __launch_bounds__(128) k_sources(const RhsArgs a) {
   const double detg = det3(g);
   const double sqrt_detg = sqrt(detg);
   const sym3 ug = inv3(g, detg);
-  double d_alp[3], d_beta[3][3];
-  sym3 d_g[3];
-  for (int d = 0; d < 3; ++d) {
-    d_alp[d] = fd_v2c<FD>(a.alp, I, b, d);
-    for (int q = 0; q < 3; ++q)
-      d_beta[d][q] = fd_v2c<FD>(a.beta[q], I, b, d);
-    d_g[d].xx = fd_v2c<FD>(a.g[0], I, b, d);
-    d_g[d].xy = fd_v2c<FD>(a.g[1], I, b, d);
-    d_g[d].xz = fd_v2c<FD>(a.g[2], I, b, d);
-    d_g[d].yy = fd_v2c<FD>(a.g[3], I, b, d);
-    d_g[d].yz = fd_v2c<FD>(a.g[4], I, b, d);
-    d_g[d].zz = fd_v2c<FD>(a.g[5], I, b, d);
-  }
   const double v_up[3] = {a.vel[0][I], a.vel[1][I], a.vel[2][I]};
   double v_low[3];
   lower3(g, v_up, v_low);
   const double w = 1.0 / sqrt(1.0 - dot3(v_low, v_up));
   const double rho = a.rho[I], eps = a.eps[I], press = a.press[I];
   const double rhW2 = (rho * (1.0 + eps) + press) * w * w;
+  const double ialp = 1.0 / alp;
   double vs[3];
+#pragma unroll
   for (int q = 0; q < 3; ++q)
-    vs[q] = v_up[q] - beta[q] / alp;
+    vs[q] = v_up[q] - beta[q] * ialp;
   const double B_up[3] = {a.Bvec[0][I], a.Bvec[1][I], a.Bvec[2][I]};
   double B_low[3];
   lower3(g, B_up, B_low);
-  const double bs0 = w * dot3(B_up, v_low) / alp;
+  const double bs0 = w * dot3(B_up, v_low) * ialp;
   double bs[3];
+#pragma unroll
   for (int q = 0; q < 3; ++q)
     bs[q] = B_up[q] / w + alp * bs0 * vs[q];
   const double bs2 = (dot3(B_up, B_low) + sq(alp * bs0)) / sq(w);
   double gb[3], gbs[3], bs_low[3];
   lower3(g, beta, gb);
   lower3(g, bs, gbs);
+#pragma unroll
   for (int q = 0; q < 3; ++q)
     bs_low[q] = gb[q] * bs0 + gbs[q];
   const double A = rhW2 + bs2 * sq(w);
   const double P = press + 0.5 * bs2;
-  const double t00 = (A - P) / sq(alp) - sq(bs0);
+  const double ialp2 = 1.0 / sq(alp);
+  const double t00 = (A - P) * ialp2 - sq(bs0);
   double t0[3], t0low[3];
+#pragma unroll
   for (int q = 0; q < 3; ++q) {
-    t0[q] = A * vs[q] / alp + P * beta[q] / sq(alp) - bs0 * bs[q];
-    t0low[q] = A * v_low[q] / alp - bs_low[q] * bs0;
+    t0[q] = A * vs[q] * ialp + P * beta[q] * ialp2 - bs0 * bs[q];
+    t0low[q] = A * v_low[q] * ialp - bs_low[q] * bs0;
   }
   // T^{ij} is symmetric (an smat in the reference): upper triangle, mirrored
   double t[3][3];
@@ -128,36 +182,44 @@ __global__ void __launch_bounds__(128) k_sources(const RhsArgs a) {
 #pragma unroll
     for (int q = p; q < 3; ++q)
       t[p][q] = t[q][p] = A * vs[p] * vs[q] +
-                          P * (ug(p, q) - beta[p] * beta[q] / sq(alp)) - bs[p] * bs[q];
+                          P * (ug(p, q) - beta[p] * beta[q] * ialp2) - bs[p] * bs[q];
   double shiftk[3];
   lower3(K, beta, shiftk);
   const double ssk = dot3(shiftk, beta);
   double X[3];
+#pragma unroll
   for (int q = 0; q < 3; ++q)
     X[q] = -d_alp[q] + 2.0 * shiftk[q];
   double Kt = 0.0;
+#pragma unroll
   for (int p = 0; p < 3; ++p)
+#pragma unroll
     for (int q = 0; q < 3; ++q)
       Kt += K(p, q) * t[p][q];
   const double tau_source = t00 * (ssk - dot3(beta, d_alp)) + dot3(t0, X) + Kt;
   double ms[3];
+#pragma unroll
   for (int d = 0; d < 3; ++d) {
     double nrm = 0.0, c1 = 0.0, c3 = 0.0;
+#pragma unroll
     for (int p = 0; p < 3; ++p)
+#pragma unroll
       for (int q = 0; q < 3; ++q) {
-        nrm += d_g[d](p, q) * beta[p] * beta[q];
-        c1 += d_g[d](p, q) * t0[p] * beta[q];
-        c3 += t[p][q] * d_g[d](p, q);
+        const double dg = d_g[d](p, q);
+        nrm += dg * beta[p] * beta[q];
+        c1 += dg * t0[p] * beta[q];
+        c3 += t[p][q] * dg;
       }
     const double c2 = dot3(t0low, d_beta[d]);
     ms[d] = t00 * (0.5 * nrm - alp * d_alp[d]) + c1 + c2 + 0.5 * c3;
   }
+  const double as = alp * sqrt_detg;
   a.rhs[V_DENS][I] = 0.0;
   a.rhs[V_DENT][I] = 0.0;
-  a.rhs[V_MOMX][I] = alp * sqrt_detg * ms[0];
-  a.rhs[V_MOMY][I] = alp * sqrt_detg * ms[1];
-  a.rhs[V_MOMZ][I] = alp * sqrt_detg * ms[2];
-  a.rhs[V_TAU][I] = alp * sqrt_detg * tau_source;
+  a.rhs[V_MOMX][I] = as * ms[0];
+  a.rhs[V_MOMY][I] = as * ms[1];
+  a.rhs[V_MOMZ][I] = as * ms[2];
+  a.rhs[V_TAU][I] = as * tau_source;
   a.rhs[V_DYE][I] = 0.0;
 }
 
