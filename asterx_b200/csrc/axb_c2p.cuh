@@ -615,23 +615,29 @@ AXB_HD void brent_bracket(const F &f, double a, double b, int minbits,
   hi = fmax(a, b);
 }
 
-// Palenzuela invariants (c2p_1DPalenzuela.hxx:150-153,267-270)
+// Palenzuela invariants (c2p_1DPalenzuela.hxx:150-153,267-270), plus the
+// loop-invariant Ye of the root function
 struct PalQRST {
-  double q, r, s, t;
+  double q, r, s, t, ye;
 };
 
+// Root function of the Palenzuela scheme (c2p_1DPalenzuela.hxx:264-303).
+// W^-2 is clamped as in the reference; W = (W^-2)^(-1/2) is taken as
+// 1/sqrt instead of pow, and the divisions by W become products with its
+// square root (last-ulp differences; the bracket search converges to the
+// same tolerance).
 template <class EOS>
 AXB_HD double pal_froot(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
                         const PalQRST &k, double x, const Cons &cv) {
-  double Wminus2 = 1.0 - (x * x * k.r + (2.0 * x + k.s) * k.t * k.t) /
-                             (x * x * (x + k.s) * (x + k.s));
+  const double xs = x + k.s;
+  double Wminus2 = 1.0 - (x * x * k.r + (2.0 * x + k.s) * k.t * k.t) / (x * x * xs * xs);
   Wminus2 = fmin(fmax(Wminus2, 1e-10), 1);
-  const double W_loc = pow(Wminus2, -0.5);
-  const double rho_loc = cv.dens / W_loc;
-  const double Ye_loc = cv.DYe / cv.dens;
-  double eps_loc = W_loc - 1.0 + (1.0 - W_loc * W_loc) * x / W_loc +
-                   W_loc * (k.q - k.s + k.t * k.t / (2 * x * x) +
-                            k.s / (2 * W_loc * W_loc));
+  const double iW = sqrt(Wminus2);
+  const double W_loc = 1.0 / iW;
+  const double rho_loc = cv.dens * iW;
+  const double Ye_loc = k.ye;
+  double eps_loc = W_loc - 1.0 + (1.0 - W_loc * W_loc) * x * iW +
+                   W_loc * (k.q - k.s + k.t * k.t / (2 * x * x) + 0.5 * k.s * Wminus2);
   if (cp.use_temp) {
     eps_loc = fmax(eps_loc, atmo.eps);
     eps_loc = fmin(eps_loc, eos.rgeps.max);
@@ -687,9 +693,10 @@ AXB_HD void palenzuela_solve(const EOS &eos, const C2PParams &cp, const Atmo &at
   }
   PalQRST k;
   k.q = cv.tau / cv.dens;
-  k.r = Ssq / pow(cv.dens, 2);
+  k.r = Ssq / (cv.dens * cv.dens);
   k.s = Bsq / cv.dens;
   k.t = BiSi / pow(cv.dens, 3. / 2.);
+  k.ye = cv.DYe / cv.dens;
   const double qP = cv.tau / cv.dens;
   const double sP = Bsq / cv.dens;
   double a = fmax(1e-10, 1.0 + qP - sP);
@@ -748,11 +755,11 @@ AXB_HD void palenzuela_solve(const EOS &eos, const C2PParams &cp, const Atmo &at
     cons_from_prim(ck, pv, glo);
     ck.unscale(sqrt_detg);
     const double small = 1e-50;
-    const double e0 = pow((ck.dens - cv.dens) / (cv.dens + small), 2.0);
-    const double e1 = pow((ck.mom[0] - cv.mom[0]) / (cv.mom[0] + small), 2.0);
-    const double e2 = pow((ck.mom[1] - cv.mom[1]) / (cv.mom[1] + small), 2.0);
-    const double e3 = pow((ck.mom[2] - cv.mom[2]) / (cv.mom[2] + small), 2.0);
-    const double e4 = pow((ck.tau - cv.tau) / (cv.tau + small), 2.0);
+    const double e0 = sq((ck.dens - cv.dens) / (cv.dens + small));
+    const double e1 = sq((ck.mom[0] - cv.mom[0]) / (cv.mom[0] + small));
+    const double e2 = sq((ck.mom[1] - cv.mom[1]) / (cv.mom[1] + small));
+    const double e3 = sq((ck.mom[2] - cv.mom[2]) / (cv.mom[2] + small));
+    const double e4 = sq((ck.tau - cv.tau) / (cv.tau + small));
     // std::max over an initializer list keeps the first of equal maxima and
     // never selects a NaN unless it is the first element
     double m = e0;
