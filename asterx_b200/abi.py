@@ -75,6 +75,47 @@ class Fields(C.Structure):
     _fields_ = [("gf", C.c_void_p * NUM_GF)]
 
 
+# independent cells for axb_c2p_cells / axb_mlp_features (axb_cells)
+CELL_INPUTS = ["dens", "momx", "momy", "momz", "tau", "DYe", "DEnt", "dBx", "dBy", "dBz",
+               "gxx", "gxy", "gxz", "gyy", "gyz", "gzz"]
+CELL_SEEDS = ["seed_rho", "seed_eps", "seed_Ye", "seed_velx", "seed_vely", "seed_velz",
+              "seed_temperature"]
+CELL_OUTPUTS = ["rho", "eps", "press", "velx", "vely", "velz", "w_lorentz", "Ye",
+                "temperature", "entropy", "iters", "flag"]
+
+
+class Cells(C.Structure):
+    _fields_ = [("n", C.c_int64), ("dens", C.c_void_p), ("mom", C.c_void_p * 3),
+                ("tau", C.c_void_p), ("DYe", C.c_void_p), ("DEnt", C.c_void_p),
+                ("dB", C.c_void_p * 3), ("g", C.c_void_p * 6),
+                ("seed_rho", C.c_void_p), ("seed_eps", C.c_void_p), ("seed_Ye", C.c_void_p),
+                ("seed_vel", C.c_void_p * 3), ("seed_temperature", C.c_void_p),
+                ("rho", C.c_void_p), ("eps", C.c_void_p), ("press", C.c_void_p),
+                ("vel", C.c_void_p * 3), ("w_lorentz", C.c_void_p), ("Ye", C.c_void_p),
+                ("temperature", C.c_void_p), ("entropy", C.c_void_p),
+                ("iters", C.c_void_p), ("flag", C.c_void_p)]
+
+
+def cells_struct(n, arrays: dict):
+    """axb_cells from a dict of device pointers (ints) keyed by the names of
+    CELL_INPUTS / CELL_SEEDS / CELL_OUTPUTS; missing names stay NULL."""
+    c = Cells()
+    c.n = int(n)
+    get = lambda k: arrays.get(k)
+    c.dens, c.tau, c.DYe, c.DEnt = get("dens"), get("tau"), get("DYe"), get("DEnt")
+    for q, ax in enumerate("xyz"):
+        c.mom[q] = get("mom" + ax)
+        c.dB[q] = get("dB" + ax)
+        c.seed_vel[q] = get("seed_vel" + ax)
+        c.vel[q] = get("vel" + ax)
+    for q, nm in enumerate(["gxx", "gxy", "gxz", "gyy", "gyz", "gzz"]):
+        c.g[q] = get(nm)
+    for nm in ("seed_rho", "seed_eps", "seed_Ye", "seed_temperature", "rho", "eps",
+               "press", "w_lorentz", "Ye", "temperature", "entropy", "iters", "flag"):
+        setattr(c, nm, get(nm))
+    return c
+
+
 _PARAM_INTS_1 = ["reconstruction_method", "loworder_method",
                  "reconstruct_with_temperature", "ppm_shock_detection",
                  "ppm_zone_flattening"]

@@ -65,10 +65,24 @@ def load_library(path=LIB_PATH):
                                 C.POINTER(Fields), C.POINTER(Params), _vp,
                                 C.c_double, C.c_double, C.c_double, C.c_double,
                                 C.c_int, _vp]
+    _fp = C.POINTER(C.c_float)
+    lib.axb_mlp_param_count.argtypes = [C.c_int]
+    lib.axb_mlp_param_count.restype = C.c_int64
+    lib.axb_mlp_create.argtypes = [C.c_int, _vp, C.c_uint64, C.c_double, C.POINTER(_vp)]
+    lib.axb_mlp_destroy.argtypes = [_vp]
+    lib.axb_mlp_get_params.argtypes = [_vp, _vp]
+    lib.axb_mlp_features.argtypes = [_vp, C.POINTER(abi.Cells), C.c_int, _vp, _vp]
+    lib.axb_mlp_forward.argtypes = [_vp, _vp, _vp, C.c_int64, _vp, _vp]
+    lib.axb_mlp_train_step.argtypes = [_vp, _vp, _vp, _vp, C.c_int64, C.c_float, C.c_float,
+                                       C.c_float, C.c_float, _vp, _vp, _vp]
+    lib.axb_c2p_cells.argtypes = [_vp, C.POINTER(abi.Cells), C.POINTER(Params), _vp, _vp,
+                                  _vp]
     lib.axb_timing_begin.argtypes = [_vp]
     lib.axb_timing_end.argtypes = [_vp, C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_int]
     for name in ("axb_con2prim_group", "axb_substep", "axb_rk_stage",
-                 "axb_sync_periodic", "axb_c2p_cells", "axb_eos_create_tabulated3d"):
+                 "axb_sync_periodic", "axb_c2p_cells", "axb_eos_create_tabulated3d",
+                 "axb_mlp_create", "axb_mlp_destroy", "axb_mlp_get_params",
+                 "axb_mlp_features", "axb_mlp_forward", "axb_mlp_train_step"):
         if hasattr(lib, name):
             getattr(lib, name).restype = C.c_int
     return lib
@@ -88,6 +102,7 @@ class Engine:
         self.ctx = _vp()
         self._check(self.lib.axb_ctx_create(device, C.byref(self.ctx)), "axb_ctx_create")
         self._eos = []
+        self._mlp = []
 
     def _check(self, rc, what):
         if rc != 0:
@@ -215,7 +230,61 @@ class Engine:
         return dict(error_word=ew.value, max_speed=ms.value, c2p_fail=nf.value,
                     iter_hist=np.array(hist[:], dtype=np.int64))
 
+    # -- independent cells and the learned guess -----------------------------
+    def cells(self, n, tensors: dict):
+        """axb_cells over torch device tensors (float64, length n) keyed by
+        abi.CELL_INPUTS / CELL_SEEDS / CELL_OUTPUTS names."""
+        ptrs = {}
+        for k, t in tensors.items():
+            if t is None:
+                continue
+            assert t.dtype == self.torch.float64 and t.is_cuda and t.numel() >= n, k
+            ptrs[k] = t.data_ptr()
+        return abi.cells_struct(n, ptrs)
+
+    def c2p_cells(self, cells, params: Params, eos, mlp=None, stream=None):
+        self._check(self.lib.axb_c2p_cells(self.ctx, C.byref(cells), C.byref(params), eos,
+                                           mlp, self.stream_ptr(stream)), "axb_c2p_cells")
+
+    def mlp_create(self, nf=8, params=None, seed=1, bracket=0.05):
+        h = _vp()
+        arr = None
+        if params is not None:
+            arr = np.ascontiguousarray(params, dtype=np.float32)
+            assert arr.size == self.lib.axb_mlp_param_count(nf)
+        self._check(self.lib.axb_mlp_create(nf, None if arr is None else arr.ctypes.data,
+                                            seed, bracket, C.byref(h)), "axb_mlp_create")
+        self._mlp.append(h)
+        return h
+
+    def mlp_params(self, mlp, nf):
+        out = np.zeros(self.lib.axb_mlp_param_count(nf), dtype=np.float32)
+        self._check(self.lib.axb_mlp_get_params(mlp, out.ctypes.data), "axb_mlp_get_params")
+        return out
+
+    def mlp_features(self, cells, nf, out, stream=None):
+        self._check(self.lib.axb_mlp_features(self.ctx, C.byref(cells), nf, out.data_ptr(),
+                                              self.stream_ptr(stream)), "axb_mlp_features")
+
+    def mlp_forward(self, mlp, features, out, stream=None):
+        n = features.shape[0]
+        self._check(self.lib.axb_mlp_forward(self.ctx, mlp, features.data_ptr(), n,
+                                             out.data_ptr(), self.stream_ptr(stream)),
+                    "axb_mlp_forward")
+
+    def mlp_train_step(self, mlp, features, targets, lr=1e-3, betas=(0.9, 0.999),
+                       eps=1e-8, loss=None, grad=None, stream=None):
+        n = features.shape[0]
+        self._check(self.lib.axb_mlp_train_step(
+            self.ctx, mlp, features.data_ptr(), targets.data_ptr(), n, lr, betas[0],
+            betas[1], eps, None if loss is None else loss.data_ptr(),
+            None if grad is None else grad.data_ptr(), self.stream_ptr(stream)),
+            "axb_mlp_train_step")
+
     def close(self):
+        for h in self._mlp:
+            self.lib.axb_mlp_destroy(h)
+        self._mlp = []
         for h in self._eos:
             self.lib.axb_eos_destroy(h)
         self._eos = []

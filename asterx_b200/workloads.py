@@ -367,39 +367,119 @@ def saved_from_prims(f, xp=None):
 
 def c2p_cells(ncells, seed=4, gamma=5.0 / 3.0, rho_range=(1e-12, 1e-2),
               eps_range=(1e-6, 10.0), w_range=(1.0, 50.0),
-              sigma_range=(1e-4, 100.0), metric_amp=0.05):
-    """Independent-cell primitive sample for the recovery benchmark:
-    rho, eps log-uniform, W uniform, magnetisation b^2/rho log-uniform,
-    isotropic velocity and field directions, random metric perturbation.
-    Returns dict of 1-D arrays: rho, eps, press, vel (3,N), B (3,N), g (6,N)."""
-    rng = np.random.default_rng(seed)
+              sigma_range=(1e-4, 100.0), metric_amp=0.05, device=None, ye=None):
+    """Independent cells of the recovery microbenchmark: rho and eps
+    log-uniform, W uniform, magnetisation b^2/rho log-uniform, isotropic
+    velocity and field directions, a random metric gamma_ij = delta_ij +
+    metric_amp * U(-1, 1) per component; ideal-gas pressure (Gamma `gamma`),
+    or the synthetic table's when `ye` = (lo, hi) gives a Ye range (then the
+    temperature is found from eps by bisection on the closed form).
+    Generated with torch on `device` (a torch.Generator seeded with `seed`)
+    when given, else with numpy.  Returns a dict of 1-D float64 arrays:
+    the primitives (rho, eps, press, velx.., Bvecx.., W, Ye, temperature,
+    entropy), the metric (gxx..gzz) and the densitised conserved variables
+    (dens, momx.., tau, DYe, DEnt, dBx..) from the exact Valencia map
+    (AsterX/src/prim2con.hxx:38-83), plus the learned-guess targets: the
+    position t_u of x = h W in the Palenzuela bracket, and ln W (t_lnw);
+    also ln(h W) (t_lnx)."""
     N = int(ncells)
-    lu = lambda a, b: np.exp(rng.uniform(np.log(a), np.log(b), N))
+    if device is None:
+        rng = np.random.default_rng(seed)
+        xp = np
+        uni = lambda lo, hi: rng.uniform(lo, hi, N)
+        nrm = lambda: rng.normal(size=(3, N))
+        stack = np.stack
+    else:
+        import torch
+        gen = torch.Generator(device=device)
+        gen.manual_seed(int(seed))
+        xp = torch
+        uni = lambda lo, hi: lo + (hi - lo) * torch.rand(N, generator=gen, device=device,
+                                                           dtype=torch.float64)
+        nrm = lambda: torch.randn((3, N), generator=gen, device=device, dtype=torch.float64)
+        stack = torch.stack
+    lu = lambda a, b: xp.exp(uni(math.log(a), math.log(b)))
     rho = lu(*rho_range)
     eps = lu(*eps_range)
-    W = rng.uniform(*w_range, N)
+    W = uni(*w_range)
     sigma = lu(*sigma_range)
-    g = np.zeros((6, N))
-    g[[0, 3, 5]] = 1.0
-    g += metric_amp * rng.uniform(-1, 1, (6, N))
-    gd = np.array([[g[0], g[1], g[2]], [g[1], g[3], g[4]], [g[2], g[4], g[5]]])
+    g = [1.0 + metric_amp * uni(-1, 1), metric_amp * uni(-1, 1), metric_amp * uni(-1, 1),
+         1.0 + metric_amp * uni(-1, 1), metric_amp * uni(-1, 1), 1.0 + metric_amp * uni(-1, 1)]
+    gd = [[g[0], g[1], g[2]], [g[1], g[3], g[4]], [g[2], g[4], g[5]]]
 
-    def unit(n):
-        v = rng.normal(size=(3, n))
-        return v / np.linalg.norm(v, axis=0)
+    def lower(v):
+        return [gd[i][0] * v[0] + gd[i][1] * v[1] + gd[i][2] * v[2] for i in range(3)]
 
-    dv = unit(N)
-    nrm = np.einsum("i...,ij...,j...->...", dv, gd, dv)
-    vel = dv * np.sqrt(1.0 - 1.0 / W ** 2) / np.sqrt(nrm)
-    db = unit(N)
-    # choose |B| so that b^2 = sigma * rho exactly
-    vlow = np.einsum("ij...,j...->i...", gd, vel)
-    Bsq1 = np.einsum("i...,ij...,j...->...", db, gd, db)
-    vB1 = np.einsum("i...,i...->...", vlow, db)
-    b2_per = Bsq1 / W ** 2 + vB1 ** 2
-    B = db * np.sqrt(sigma * rho / b2_per)
-    press = (gamma - 1.0) * rho * eps
-    return dict(rho=rho, eps=eps, press=press, vel=vel, B=B, g=g, W=W)
+    def dot(a, b):
+        return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]
+
+    def unit():
+        v = nrm()
+        n = xp.sqrt(v[0] ** 2 + v[1] ** 2 + v[2] ** 2)
+        return [v[0] / n, v[1] / n, v[2] / n]
+
+    dv = unit()
+    nn = dot(dv, lower(dv))
+    vmag = xp.sqrt(1.0 - 1.0 / W ** 2) / xp.sqrt(nn)
+    vel = [d * vmag for d in dv]
+    db = unit()
+    vlow = lower(vel)
+    b2_per = dot(db, lower(db)) / W ** 2 + dot(vlow, db) ** 2
+    bmag = xp.sqrt(sigma * rho / b2_per)
+    B = [d * bmag for d in db]
+    if ye is None:
+        Ye = rho * 0 + 0.5
+        press = (gamma - 1.0) * rho * eps
+        temp = (gamma - 1.0) * eps
+        ent = (gamma - 1.0) * eps * rho ** (1.0 - gamma)
+    else:
+        Ye = uni(*ye)
+        # invert eps(rho, T, Ye) of the synthetic table by bisection in ln T
+        lo = rho * 0 + math.log(0.01)
+        hi = rho * 0 + math.log(100.0)
+        for _ in range(80):
+            mid = 0.5 * (lo + hi)
+            e_mid = tab_thermo(rho, xp.exp(mid), Ye, xp)[1]
+            up = e_mid > eps
+            hi = xp.where(up, mid, hi)
+            lo = xp.where(up, lo, mid)
+        temp = xp.exp(0.5 * (lo + hi))
+        press, eps, ent, _ = tab_thermo(rho, temp, Ye, xp)
+    det = (g[0] * (g[3] * g[5] - g[4] ** 2) - g[1] * (g[1] * g[5] - g[4] * g[2])
+           + g[2] * (g[1] * g[4] - g[3] * g[2]))
+    sq = xp.sqrt(det)
+    Bl = lower(B)
+    Wc = 1.0 / xp.sqrt(1.0 - dot(vlow, vel))
+    bst = Wc * dot(B, vlow)
+    bl = [Bl[i] / Wc + bst * vlow[i] for i in range(3)]
+    bs2 = (dot(B, Bl) + bst * bst) / (Wc * Wc)
+    hW2 = Wc * Wc * (rho * (1.0 + eps) + press + bs2)
+    out = dict(rho=rho, eps=eps, press=press, W=Wc, Ye=Ye, temperature=temp, entropy=ent)
+    for q, ax in enumerate("xyz"):
+        out["vel" + ax] = vel[q]
+        out["Bvec" + ax] = B[q]
+        out["mom" + ax] = sq * (hW2 * vlow[q] - bst * bl[q])
+        out["dB" + ax] = sq * B[q]
+    for q, nm in enumerate(["gxx", "gxy", "gxz", "gyy", "gyz", "gzz"]):
+        out[nm] = g[q]
+    out["dens"] = sq * rho * Wc
+    out["tau"] = sq * (hW2 - (press + 0.5 * bs2) - bst * bst) - out["dens"]
+    out["DYe"] = out["dens"] * Ye
+    out["DEnt"] = out["dens"] * ent
+    h = 1.0 + eps + press / rho
+    x = h * Wc
+    # position of x = h W in the Palenzuela scheme's initial bracket
+    # [max(1e-10, 1 + q - s), 2 + 2 q - s] (c2p_1DPalenzuela.hxx:395-398),
+    # q = tau / D, s = B^2 / D with undensitised D, tau, B
+    D = rho * Wc
+    q = (out["tau"] / sq) / D
+    s_ = dot(B, Bl) / D
+    lo = xp.maximum(q * 0 + 1e-10, 1.0 + q - s_)
+    hi = 2.0 + 2.0 * q - s_
+    out["t_u"] = (x - lo) / (hi - lo)
+    out["t_lnx"] = xp.log(x)
+    out["t_lnw"] = xp.log(Wc)
+    return out
 
 
 def cons_from_prims(L: Layout, f: dict, xp=None):

@@ -304,6 +304,95 @@ AXB_API int axb_substep(axb_ctx *ctx, const axb_box *box,
                         double alpha, double beta, double gamma, double dt,
                         int periodic, void *stream);
 
+/* ------------------------------------------------------------------------ */
+/* independent-cell primitive recovery and the learned initial guess         */
+/* ------------------------------------------------------------------------ */
+
+/* Structure-of-arrays view of `n` independent cells (device pointers, one
+ * double per cell each).  Conserved variables are densitized as the
+ * reference's cons_vars (Con2PrimFactory/src/cons.hxx:48-91): dens, mom_i,
+ * tau, DYe, DEnt, dB^i; g holds the cell's gamma_ij (xx xy xz yy yz zz).
+ * Seeds (saved primitives: rho, eps, Ye, vel^i, temperature) may all be NULL
+ * for a cold start: v = 0, eps = the atmosphere's eps, Ye = DYe/dens.
+ * Outputs (any may be NULL): rho, eps, press, vel^i, w_lorentz, Ye,
+ * temperature, entropy, the iteration count of the first solver (double),
+ * and the con2prim flag (AXB_C2P_* code, as double). */
+typedef struct axb_cells {
+  int64_t n;
+  const double *dens, *mom[3], *tau, *DYe, *DEnt, *dB[3];
+  const double *g[6];
+  const double *seed_rho, *seed_eps, *seed_Ye, *seed_vel[3], *seed_temperature;
+  double *rho, *eps, *press, *vel[3], *w_lorentz, *Ye, *temperature, *entropy;
+  double *iters, *flag;
+} axb_cells;
+
+/* Learned initial guess: an MLP nf -> 64 -> 64 -> 64 -> 2 (SiLU hidden
+ * activations; nf = 8, or 9 with Ye for a tabulated EOS) evaluated in BF16
+ * on the tensor cores with FP32 accumulation, inside the recovery kernel.
+ * Outputs: y0 = the position of x = h W in the Palenzuela scheme's
+ * initial bracket [max(1e-10, 1 + q - s), 2 + 2 q - s]
+ * (c2p_1DPalenzuela.hxx:395-398), y1 = ln W.  The Noble scheme starts from
+ * Z = D x and v^2 = 1 - W^-2 instead of its saved-primitive seeds
+ * (c2p_2DNoble.hxx:374-393), the Palenzuela scheme brackets x by
+ * [x (1 - bracket), x (1 + bracket)] when that interval brackets the root
+ * and otherwise keeps its own bracket (c2p_1DPalenzuela.hxx:395-401).
+ * No counterpart in the reference. */
+typedef struct axb_mlp axb_mlp;
+
+#define AXB_MLP_HIDDEN 64
+#define AXB_MLP_MAXF 16
+
+/* Number of parameters of an MLP with `nf` inputs:
+ * W1 [nf x 64], b1 [64], W2 [64 x 64], b2, W3 [64 x 64], b3, W4 [64 x 2], b4 [2]
+ * in that order, row-major (input index outer). */
+AXB_API int64_t axb_mlp_param_count(int nf);
+
+/* Create an MLP on the current device from FP32 parameters (host memory, in
+ * the order above), or with seeded random initial values when `params` is
+ * NULL.  `bracket` is the relative half-width of the Palenzuela bracket. */
+AXB_API int axb_mlp_create(int nf, const float *params, uint64_t seed,
+                           double bracket, axb_mlp **out);
+AXB_API int axb_mlp_destroy(axb_mlp *mlp);
+/* Copy the FP32 master parameters to host memory (param_count floats). */
+AXB_API int axb_mlp_get_params(const axb_mlp *mlp, float *params);
+
+/* The MLP input features of each cell (n x nf FP32, row-major, device), as
+ * the recovery kernel computes them: with sqrt(gamma)-undensitized D, S_i,
+ * tau, B^i and q = tau/D, r = S^2/D^2, s = B^2/D, t = B.S/D^1.5:
+ * ln D / 10, ln(1+q), ln(1+r)/2, ln(1+s), t^2/(r s), r/(1+q+s)^2, s/(1+q+s),
+ * ln(1+q) - ln(1+r)/2 [, Ye = DYe/dens]. */
+AXB_API int axb_mlp_features(axb_ctx *ctx, const axb_cells *cells, int nf,
+                             float *features, void *stream);
+
+/* The network's outputs (n x 2 FP32, device) for given features (n x nf
+ * FP32, device), through the same tensor-core code the recovery kernel
+ * runs. */
+AXB_API int axb_mlp_forward(axb_ctx *ctx, const axb_mlp *mlp, const float *features,
+                            int64_t n, float *out, void *stream);
+
+/* One optimisation step on a batch: forward with BF16-rounded weights and
+ * activations (as the tensor-core inference sees them) and FP32 accumulation,
+ * mean-squared error against `targets` (n x 2 FP32, device), backward in
+ * FP32, Adam (lr, beta1, beta2, eps) on the FP32 master parameters.  The
+ * batch loss is written to `loss` (device FP32, may be NULL).  If `grad` is
+ * non-NULL the parameter gradient (param_count floats, device) is written
+ * there and no update is made. */
+AXB_API int axb_mlp_train_step(axb_ctx *ctx, axb_mlp *mlp, const float *features,
+                               const float *targets, int64_t n, float lr,
+                               float beta1, float beta2, float adam_eps,
+                               float *loss, float *grad, void *stream);
+
+/* The primitive recovery of AsterX_Con2Prim_typeEoS (con2prim.cxx:137-416)
+ * for independent cells: cons floors, the c2p_prime -> c2p_second cascade
+ * with atmosphere on double failure, and a uniform atmosphere built from
+ * `params` (rho_abs_min etc., as for a box inside r_atmo).  With `mlp`
+ * non-NULL the learned guess replaces the seeds as described above.  The
+ * iteration histogram and failure count accumulate into the context status.
+ * No mask/excision. */
+AXB_API int axb_c2p_cells(axb_ctx *ctx, const axb_cells *cells,
+                          const axb_params *params, const axb_eos *eos,
+                          const axb_mlp *mlp, void *stream);
+
 /* axb_rhs_group for callers that cannot allocate device memory (a host
  * framework that owns every device allocation, a tool that may not call
  * cudaMalloc on a shared device, a driver whose footprint is fixed after

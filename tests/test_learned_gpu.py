@@ -1,0 +1,171 @@
+"""Independent-cell recovery and the learned initial guess on the GPU.
+
+* axb_c2p_cells (plain, cold-start seeds) against the reference's Noble and
+  Palenzuela functors compiled on the host, cell by cell: same outcome,
+  primitives within 1e-10 (the primitive tolerance of the parity tests).
+* The input features, the tensor-core forward pass and the training
+  gradient against the numpy checker (oracle/mlp_ref.py).
+* A briefly trained guess: the recovered primitives equal the plain ones
+  within 1e-10 and the Noble iteration count drops.
+"""
+import numpy as np
+import pytest
+
+from asterx_b200 import abi
+from asterx_b200 import workloads as W
+from oracle import mlp_ref
+
+GAMMA = 5.0 / 3.0
+EOS_KW = dict(rho=(1e-40, 1e10), eps=(0.0, 1e10))
+PARAMS = dict(c2p_tol=1e-12, max_iter=100, vw_lim=60.0, B_lim=1e8, rho_abs_min=1e-20,
+              atmo_tol=1e-3)
+OUT = ["rho", "eps", "press", "velx", "vely", "velz", "w_lorentz", "iters", "flag"]
+
+
+def device_cells(engine, cells, n, outputs=OUT):
+    torch = engine.torch
+    t = {k: torch.as_tensor(np.ascontiguousarray(cells[k]), device=engine.device)
+         for k in abi.CELL_INPUTS}
+    for k in outputs:
+        t[k] = torch.full((n,), float("nan"), dtype=torch.float64, device=engine.device)
+    return t
+
+
+def relerr(a, b):
+    return np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("solver", ["noble", "palenzuela"])
+def test_c2p_cells_matches_reference(engine, ref, solver):
+    n = 512
+    cells = W.c2p_cells(n, seed=11, gamma=GAMMA, w_range=(1.0, 20.0))
+    # Palenzuela's answer is the midpoint of its final bracket, so two
+    # evaluations of its root function that differ in the last ulp give
+    # answers that differ by up to ~W^2 times the bracket tolerance; the
+    # box-level tests use 1e-14 for it as well
+    kw = dict(PARAMS, c2p_tol=1e-14) if solver == "palenzuela" else PARAMS
+    p = abi.default_params(c2p_prime=solver, c2p_second="none", **kw)
+    eos = engine.eos_idealgas(GAMMA, **EOS_KW)
+    t = device_cells(engine, cells, n)
+    engine.c2p_cells(engine.cells(n, t), p, eos)
+    got = {k: t[k].cpu().numpy() for k in OUT}
+    ref.setup(W.Layout((4, 4, 4), 3, (1, 1, 1), (0, 0, 0)), p, {})
+    ref.eos_idealgas(GAMMA, **EOS_KW)
+    # the kernel's uniform atmosphere (rho_abs_min, thermal, t_atmo)
+    rho_atm = max(1e-40, PARAMS["rho_abs_min"])
+    eps_atm = p.t_atmo / (GAMMA - 1.0)
+    atmo = [rho_atm, eps_atm, p.Ye_atmo, (GAMMA - 1.0) * rho_atm * eps_atm, p.t_atmo,
+            (GAMMA - 1.0) * eps_atm * rho_atm ** (1.0 - GAMMA), rho_atm * (1 + p.atmo_tol)]
+    ok = 0
+    for i in range(n):
+        cons = [cells[k][i] for k in ("dens", "momx", "momy", "momz", "tau", "DYe", "DEnt",
+                                      "dBx", "dBy", "dBz")]
+        g6 = [cells[k][i] for k in ("gxx", "gxy", "gxz", "gyy", "gyz", "gzz")]
+        sq = np.sqrt(np.linalg.det(np.array([[g6[0], g6[1], g6[2]], [g6[1], g6[3], g6[4]],
+                                             [g6[2], g6[4], g6[5]]])))
+        seed = [cons[0] / sq, eps_atm, cons[5] / cons[0], 0.0, p.t_atmo, 0.0, 0.0, 0.0, 0.0]
+        prim, _, rep = ref.c2p_point(abi.C2P[solver], cons, g6, seed, atmo)
+        success = rep[0] == 0
+        if success:
+            assert got["flag"][i] == abi.C2P_PRIME, i
+            if solver == "noble":
+                assert got["iters"][i] == rep[1], (i, got["iters"][i], rep[1])
+            # (Brent's iteration count in the Palenzuela scheme depends on
+            # last-ulp values of the root function, which the engine evaluates
+            # without pow; the bracket it returns meets the same tolerance)
+            for k, j in (("rho", 0), ("eps", 1), ("press", 3), ("velx", 6), ("vely", 7),
+                         ("velz", 8), ("w_lorentz", 9)):
+                assert relerr(got[k][i], prim[j]) <= 1e-10 or abs(got[k][i] - prim[j]) <= 1e-14, \
+                    (i, k, got[k][i], prim[j])
+            ok += 1
+        else:
+            assert got["flag"][i] == abi.C2P_FAIL, i
+    assert ok > 0.9 * n
+
+
+@pytest.mark.gpu
+def test_mlp_features_forward_and_gradient(engine):
+    torch = engine.torch
+    n = 4096
+    cells = W.c2p_cells(n, seed=12, gamma=GAMMA)
+    t = device_cells(engine, cells, n, outputs=[])
+    feats = torch.zeros((n, 8), dtype=torch.float32, device=engine.device)
+    engine.mlp_features(engine.cells(n, t), 8, feats)
+    want = mlp_ref.features(cells, 8)
+    got = feats.cpu().numpy()
+    assert np.allclose(got, want, rtol=1e-6, atol=1e-6)
+
+    mlp = engine.mlp_create(8, seed=5)
+    params = engine.mlp_params(mlp, 8)
+    out = torch.zeros((n, 2), dtype=torch.float32, device=engine.device)
+    engine.mlp_forward(mlp, feats, out)
+    y_gpu = out.cpu().numpy()
+    y_ref, _ = mlp_ref.forward(params, want)
+    err = np.abs(y_gpu - y_ref)
+    # identical rounding points; differences come from the FP32 summation
+    # order (and, rarely, a hidden activation landing on the other side of
+    # a BF16 rounding boundary)
+    assert np.median(err) <= 1e-5 and err.max() <= 2e-2, (np.median(err), err.max())
+
+    tgt = np.stack([cells["t_u"], cells["t_lnw"]], axis=1).astype(np.float32)
+    tg = torch.as_tensor(tgt, device=engine.device)
+    grad = torch.zeros(params.size, dtype=torch.float32, device=engine.device)
+    loss = torch.zeros(1, dtype=torch.float32, device=engine.device)
+    engine.mlp_train_step(mlp, feats, tg, loss=loss, grad=grad)
+    l_ref, g_ref = mlp_ref.loss_and_grad(params, want, tgt)
+    g = grad.cpu().numpy()
+    assert abs(loss.item() - l_ref) <= 1e-4 * l_ref
+    assert np.linalg.norm(g - g_ref) <= 2e-3 * np.linalg.norm(g_ref)
+    # the step with grad=None changes the parameters
+    engine.mlp_train_step(mlp, feats, tg, lr=1e-3)
+    assert not np.array_equal(engine.mlp_params(mlp, 8), params)
+
+
+@pytest.mark.gpu
+def test_learned_guess_same_answer_fewer_iterations(engine):
+    torch = engine.torch
+    dev = engine.device
+    nt = 1 << 17
+    train = W.c2p_cells(nt, seed=101, gamma=GAMMA, device=dev)
+    tt = {k: train[k] for k in abi.CELL_INPUTS}
+    feats = torch.zeros((nt, 8), dtype=torch.float32, device=dev)
+    engine.mlp_features(engine.cells(nt, tt), 8, feats)
+    tgt = torch.stack([train["t_u"], train["t_lnw"]], dim=1).float().contiguous()
+    mlp = engine.mlp_create(8, seed=7, bracket=0.05)
+    loss = torch.zeros(1, dtype=torch.float32, device=dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    bs = 8192
+    for step in range(1500):
+        idx = torch.randint(0, nt, (bs,), generator=g, device=dev)
+        lr = 3e-3 if step < 1000 else 1e-3
+        engine.mlp_train_step(mlp, feats[idx].contiguous(), tgt[idx].contiguous(), lr=lr,
+                              loss=loss)
+    final = loss.item()
+    assert final < 0.2, final
+
+    n = 1 << 14
+    cells = W.c2p_cells(n, seed=202, gamma=GAMMA, device=dev)
+    p = abi.default_params(c2p_prime="noble", c2p_second="palenzuela", **PARAMS)
+    eos = engine.eos_idealgas(GAMMA, **EOS_KW)
+    res = {}
+    for name, m in (("plain", None), ("learned", mlp)):
+        t = {k: cells[k] for k in abi.CELL_INPUTS}
+        for k in OUT:
+            t[k] = torch.full((n,), float("nan"), dtype=torch.float64, device=dev)
+        engine.c2p_cells(engine.cells(n, t), p, eos, mlp=m)
+        res[name] = {k: t[k].cpu().numpy() for k in OUT}
+    a, b = res["plain"], res["learned"]
+    both = (a["flag"] == abi.C2P_PRIME) & (b["flag"] == abi.C2P_PRIME)
+    assert both.mean() > 0.9
+    for k in ("rho", "w_lorentz", "velx", "vely", "velz"):
+        assert relerr(b[k][both], a[k][both]).max() <= 1e-10, k
+    # eps comes out of Z / (rho W^2) - 1 and is only defined to ~1e-16 on
+    # the scale of 1 + eps (both runs); compare it, and p, on that scale
+    ea, eb = a["eps"][both], b["eps"][both]
+    assert (np.abs(eb - ea) / (1.0 + np.abs(ea))).max() <= 1e-10
+    ra = a["rho"][both]
+    scale = ra * (1.0 + ea) + a["press"][both]
+    assert (np.abs(b["press"][both] - a["press"][both]) / scale).max() <= 1e-10
+    assert b["iters"][both].mean() < a["iters"][both].mean()
