@@ -93,7 +93,7 @@ class Cells(C.Structure):
                 ("rho", C.c_void_p), ("eps", C.c_void_p), ("press", C.c_void_p),
                 ("vel", C.c_void_p * 3), ("w_lorentz", C.c_void_p), ("Ye", C.c_void_p),
                 ("temperature", C.c_void_p), ("entropy", C.c_void_p),
-                ("iters", C.c_void_p), ("flag", C.c_void_p)]
+                ("iters", C.c_void_p), ("flag", C.c_void_p), ("guess", C.c_void_p)]
 
 
 def cells_struct(n, arrays: dict):
@@ -111,7 +111,8 @@ def cells_struct(n, arrays: dict):
     for q, nm in enumerate(["gxx", "gxy", "gxz", "gyy", "gyz", "gzz"]):
         c.g[q] = get(nm)
     for nm in ("seed_rho", "seed_eps", "seed_Ye", "seed_temperature", "rho", "eps",
-               "press", "w_lorentz", "Ye", "temperature", "entropy", "iters", "flag"):
+               "press", "w_lorentz", "Ye", "temperature", "entropy", "iters", "flag",
+               "guess"):
         setattr(c, nm, get(nm))
     return c
 

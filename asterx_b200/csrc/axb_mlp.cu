@@ -149,20 +149,65 @@ __global__ void k_mlp_features(const axb_cells c, int nf, float *out) {
     out[i * nf + k] = f[k];
 }
 
-// tensor-core forward on given features (the recovery kernel's code path)
-__global__ void __launch_bounds__(128) k_mlp_forward(const MlpDev m, const float *feat,
+// tensor-core forward on given features (the code path of k_mlp_guess)
+__global__ void __launch_bounds__(256) k_mlp_forward(const MlpDev m, const float *feat,
                                                      long long n, float *out) {
-  __shared__ uint32_t stage[4][32 * 8];
+  __shared__ MlpSmem w;
+  __shared__ uint32_t stage[8][32 * 8];
+  mlp_stage_weights(m, w);
+  __syncthreads();
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   float f[MLP_K1];
 #pragma unroll
   for (int k = 0; k < MLP_K1; ++k)
     f[k] = (i < n && k < m.nf) ? feat[i * m.nf + k] : 0.0f;
   float y0, y1;
-  mlp_forward_warp(m, f, stage[threadIdx.x >> 5], y0, y1);
+  mlp_forward_warp(w, f, stage[threadIdx.x >> 5], y0, y1);
   if (i < n) {
     out[2 * i] = y0;
     out[2 * i + 1] = y1;
+  }
+}
+
+// Learned guess of independent cells: features from the conserved
+// variables and metric, the network, and the decoded guess (x = h W, W) per
+// cell.  A persistent grid: each CTA stages the weights once and its warps
+// walk chunks of 32 cells.
+__global__ void __launch_bounds__(256) k_mlp_guess(const axb_cells c, const MlpDev m,
+                                                   float2 *guess) {
+  __shared__ MlpSmem w;
+  __shared__ uint32_t stage[8][32 * 8];
+  mlp_stage_weights(m, w);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  const long long nchunks = (c.n + 31) / 32;
+  for (long long ch = warp0; ch < nchunks; ch += nwarps) { // warp-uniform
+    const long long i = ch * 32 + lane;
+    const bool valid = i < c.n;
+    float f[MLP_K1];
+#pragma unroll
+    for (int k = 0; k < MLP_K1; ++k)
+      f[k] = 0.0f;
+    CellInvariants inv{1.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (valid) {
+      const sym3 glo{c.g[0][i], c.g[1][i], c.g[2][i], c.g[3][i], c.g[4][i], c.g[5][i]};
+      const double mom[3] = {c.mom[0][i], c.mom[1][i], c.mom[2][i]};
+      const double dB[3] = {c.dB[0][i], c.dB[1][i], c.dB[2][i]};
+      inv = cell_invariants(c.dens[i], mom, c.tau[i], c.DYe[i], dB, glo);
+      mlp_features(inv, m.nf, f);
+    }
+    float y0, y1;
+    mlp_forward_warp(w, f, stage[threadIdx.x >> 5], y0, y1);
+    if (valid) {
+      // y0 places x = h W in the Palenzuela scheme's initial bracket
+      // (c2p_1DPalenzuela.hxx:395-398)
+      const double lo = fmax(1e-10, 1.0 + inv.q - inv.s), hi = 2.0 + 2.0 * inv.q - inv.s;
+      const double x = lo + double(y0) * (hi - lo);
+      const double W = fmax(exp(double(y1)), 1.0);
+      guess[i] = make_float2(float(x), float(W));
+    }
   }
 }
 
@@ -495,11 +540,27 @@ AXB_API int axb_mlp_forward(axb_ctx *c, const axb_mlp *m, const float *features,
     return AXB_ERR_ARG;
   if (n == 0)
     return AXB_OK;
-  const long long blocks = (n + 127) / 128;
-  k_mlp_forward<<<(unsigned)blocks, 128, 0, (cudaStream_t)stream>>>(m->dev(), features, n,
+  const long long blocks = (n + 255) / 256;
+  k_mlp_forward<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(m->dev(), features, n,
                                                                      out);
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
 }
+
+namespace axb {
+int launch_mlp_guess(const axb_cells &c, const axb_mlp *m, float2 *guess, cudaStream_t s) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long chunks = (c.n + 31) / 32;
+  long long blocks = (chunks + 7) / 8;
+  if (blocks > 4LL * sms) // persistent: a few CTAs per SM amortise the weight copy
+    blocks = 4LL * sms;
+  if (blocks < 1)
+    return AXB_OK;
+  k_mlp_guess<<<(unsigned)blocks, 256, 0, s>>>(c, m->dev(), guess);
+  return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+}
+} // namespace axb
 
 AXB_API int axb_mlp_train_step(axb_ctx *c, axb_mlp *m, const float *features,
                                const float *targets, int64_t n, float lr, float beta1,

@@ -2,15 +2,14 @@
 // warp-level MLP forward pass on the tensor cores.
 //
 // Network: nf -> 64 -> 64 -> 64 -> 2, SiLU on the hidden layers, BF16
-// weights and activations, FP32 accumulation and biases.  One warp evaluates
-// 32 cells (one per lane) as two 16-row tiles of mma.sync m16n8k16: the
-// recovery is FP64-bound and the network costs ~18 kflop per cell, so the
-// warp-synchronous MMA keeps the evaluation inside the recovery kernel (no
-// staging through memory, no block barrier) at a few percent of its time.
-// Hidden C fragments become the next layer's A fragments in registers (the
-// m16n8 accumulator layout of two adjacent n-tiles is the m16k16 operand
-// layout); only the input features pass through 1 KB of shared memory per
-// warp to reach the fragment layout.
+// weights and activations, FP32 accumulation and biases.  A CTA stages the
+// ~20 KB of weights in shared memory once (rows padded so that the B
+// fragments load without bank conflicts) and each warp evaluates 32 cells
+// (one per lane) as two 16-row tiles of mma.sync m16n8k16.  Hidden
+// accumulator fragments become the next layer's A fragments in registers
+// (the m16n8 accumulator layout of two adjacent n-tiles is the m16k16
+// operand layout); only the input features pass through 1 KB of shared
+// memory per warp to reach the fragment layout.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -103,16 +102,60 @@ AXB_D void mma_bf16_16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, ui
                : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-AXB_D float silu(float z) { return z / (1.0f + __expf(-z)); }
+// SiLU as z (1 + tanh(z/2)) / 2 with the hardware tanh approximation: one
+// special-function instruction per activation instead of an exponential and
+// a reciprocal (the special-function unit is what bounds this network).  Its
+// relative error (~2^-11) is below the BF16 rounding that follows.
+AXB_D float tanh_approx(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+AXB_D float silu(float z) {
+  const float hz = 0.5f * z;
+  return fmaf(hz, tanh_approx(hz), hz);
+}
 
-// B fragment words for n-tile nt, k-block kb of a weight stored wT[n][K].
-AXB_D void load_b(const __nv_bfloat16 *wT, int K, int nt, int kb, int lane, uint32_t &b0,
+// Weights in shared memory, n-major with padded rows (K + 8 bf16): the
+// eight rows a B-fragment load touches then fall in distinct banks.
+constexpr int MLP_LD1 = MLP_K1 + 8; // 24
+constexpr int MLP_LDH = MLP_H + 8;  // 72
+struct MlpSmem {
+  __nv_bfloat16 w1[MLP_H * MLP_LD1];
+  __nv_bfloat16 w2[MLP_H * MLP_LDH];
+  __nv_bfloat16 w3[MLP_H * MLP_LDH];
+  __nv_bfloat16 w4[MLP_N4 * MLP_LDH];
+  float b1[MLP_H], b2[MLP_H], b3[MLP_H], b4[MLP_N4];
+};
+
+// Cooperative copy of the device weights into shared memory (all threads
+// of the block; a __syncthreads must follow).
+AXB_D void mlp_stage_weights(const MlpDev &m, MlpSmem &w) {
+  for (int e = threadIdx.x; e < MLP_H * MLP_K1; e += blockDim.x)
+    w.w1[(e / MLP_K1) * MLP_LD1 + e % MLP_K1] = m.w1[e];
+  for (int e = threadIdx.x; e < MLP_H * MLP_H; e += blockDim.x) {
+    w.w2[(e / MLP_H) * MLP_LDH + e % MLP_H] = m.w2[e];
+    w.w3[(e / MLP_H) * MLP_LDH + e % MLP_H] = m.w3[e];
+  }
+  for (int e = threadIdx.x; e < MLP_N4 * MLP_H; e += blockDim.x)
+    w.w4[(e / MLP_H) * MLP_LDH + e % MLP_H] = m.w4[e];
+  for (int e = threadIdx.x; e < MLP_H; e += blockDim.x) {
+    w.b1[e] = m.b1[e];
+    w.b2[e] = m.b2[e];
+    w.b3[e] = m.b3[e];
+  }
+  if (threadIdx.x < MLP_N4)
+    w.b4[threadIdx.x] = m.b4[threadIdx.x];
+}
+
+// B fragment words for n-tile nt, k-block kb of a weight stored wT[n][ld].
+AXB_D void load_b(const __nv_bfloat16 *wT, int ld, int nt, int kb, int lane, uint32_t &b0,
                   uint32_t &b1) {
   const int n = nt * 8 + (lane >> 2);
   const int k = kb * 16 + (lane & 3) * 2;
-  const uint32_t *p = reinterpret_cast<const uint32_t *>(wT + (size_t)n * K + k);
-  b0 = __ldg(p);
-  b1 = __ldg(p + 4); // k + 8
+  const uint32_t *p = reinterpret_cast<const uint32_t *>(wT + n * ld + k);
+  b0 = p[0];
+  b1 = p[4]; // k + 8
 }
 
 // Hidden layer: A (4 k-blocks of 16) x W [64 x 64] -> 8 n-tiles, bias, SiLU,
@@ -126,7 +169,7 @@ AXB_D void mlp_hidden64(const __nv_bfloat16 *wT, const float *bias, int lane,
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int nt = 2 * kb + h;
-      const float bl = __ldg(bias + nt * 8 + t2), bh = __ldg(bias + nt * 8 + t2 + 1);
+      const float bl = bias[nt * 8 + t2], bh = bias[nt * 8 + t2 + 1];
       c[h][0] = bl;
       c[h][1] = bh;
       c[h][2] = bl;
@@ -134,7 +177,7 @@ AXB_D void mlp_hidden64(const __nv_bfloat16 *wT, const float *bias, int lane,
 #pragma unroll
       for (int kk = 0; kk < 4; ++kk) {
         uint32_t b0, b1;
-        load_b(wT, 64, nt, kk, lane, b0, b1);
+        load_b(wT, MLP_LDH, nt, kk, lane, b0, b1);
         mma_bf16_16816(c[h], ain[kk], b0, b1);
       }
     }
@@ -147,7 +190,7 @@ AXB_D void mlp_hidden64(const __nv_bfloat16 *wT, const float *bias, int lane,
 
 // One 16-row tile (rows 16 mt .. 16 mt + 15 of the warp's cells): returns
 // the layer-4 accumulator fragment (outputs in columns 0 and 1).
-AXB_D void mlp_tile(const MlpDev &m, const uint32_t *stage, int mt, int lane,
+AXB_D void mlp_tile(const MlpSmem &w, const uint32_t *stage, int mt, int lane,
                     float (&c)[4]) {
   const int g = lane >> 2, t = lane & 3, t2 = t * 2;
   const int r0 = mt * 16 + g, r1 = r0 + 8;
@@ -161,13 +204,13 @@ AXB_D void mlp_tile(const MlpDev &m, const uint32_t *stage, int mt, int lane,
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       const int nt = 2 * kb + h;
-      const float bl = __ldg(m.b1 + nt * 8 + t2), bh = __ldg(m.b1 + nt * 8 + t2 + 1);
+      const float bl = w.b1[nt * 8 + t2], bh = w.b1[nt * 8 + t2 + 1];
       cc[h][0] = bl;
       cc[h][1] = bh;
       cc[h][2] = bl;
       cc[h][3] = bh;
       uint32_t b0, b1;
-      load_b(m.w1, MLP_K1, nt, 0, lane, b0, b1);
+      load_b(w.w1, MLP_LD1, nt, 0, lane, b0, b1);
       mma_bf16_16816(cc[h], a1, b0, b1);
     }
     h1[kb][0] = pack_bf16x2(silu(cc[0][0]), silu(cc[0][1]));
@@ -176,10 +219,10 @@ AXB_D void mlp_tile(const MlpDev &m, const uint32_t *stage, int mt, int lane,
     h1[kb][3] = pack_bf16x2(silu(cc[1][2]), silu(cc[1][3]));
   }
   uint32_t h2[4][4], h3[4][4];
-  mlp_hidden64(m.w2, m.b2, lane, h1, h2);
-  mlp_hidden64(m.w3, m.b3, lane, h2, h3);
+  mlp_hidden64(w.w2, w.b2, lane, h1, h2);
+  mlp_hidden64(w.w3, w.b3, lane, h2, h3);
   // layer 4: [16 x 64] x [64 x 8]
-  const float bl = __ldg(m.b4 + t2), bh = __ldg(m.b4 + t2 + 1);
+  const float bl = w.b4[t2], bh = w.b4[t2 + 1];
   c[0] = bl;
   c[1] = bh;
   c[2] = bl;
@@ -187,8 +230,99 @@ AXB_D void mlp_tile(const MlpDev &m, const uint32_t *stage, int mt, int lane,
 #pragma unroll
   for (int kk = 0; kk < 4; ++kk) {
     uint32_t b0, b1;
-    load_b(m.w4, 64, 0, kk, lane, b0, b1);
+    load_b(w.w4, MLP_LDH, 0, kk, lane, b0, b1);
     mma_bf16_16816(c, h3[kk], b0, b1);
+  }
+}
+
+// Hidden layer for both 16-row tiles at once: the two accumulator chains
+// are independent, which doubles the MMAs in flight per warp and reuses
+// each B fragment for both tiles.
+AXB_D void mlp_hidden64x2(const __nv_bfloat16 *wT, const float *bias, int lane,
+                          const uint32_t (&ain0)[4][4], const uint32_t (&ain1)[4][4],
+                          uint32_t (&aout0)[4][4], uint32_t (&aout1)[4][4]) {
+  const int t2 = (lane & 3) * 2;
+#pragma unroll
+  for (int kb = 0; kb < 4; ++kb) {
+    float c0[2][4], c1[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int nt = 2 * kb + h;
+      const float bl = bias[nt * 8 + t2], bh = bias[nt * 8 + t2 + 1];
+      c0[h][0] = c1[h][0] = bl;
+      c0[h][1] = c1[h][1] = bh;
+      c0[h][2] = c1[h][2] = bl;
+      c0[h][3] = c1[h][3] = bh;
+#pragma unroll
+      for (int kk = 0; kk < 4; ++kk) {
+        uint32_t b0, b1;
+        load_b(wT, MLP_LDH, nt, kk, lane, b0, b1);
+        mma_bf16_16816(c0[h], ain0[kk], b0, b1);
+        mma_bf16_16816(c1[h], ain1[kk], b0, b1);
+      }
+    }
+    aout0[kb][0] = pack_bf16x2(silu(c0[0][0]), silu(c0[0][1]));
+    aout0[kb][1] = pack_bf16x2(silu(c0[0][2]), silu(c0[0][3]));
+    aout0[kb][2] = pack_bf16x2(silu(c0[1][0]), silu(c0[1][1]));
+    aout0[kb][3] = pack_bf16x2(silu(c0[1][2]), silu(c0[1][3]));
+    aout1[kb][0] = pack_bf16x2(silu(c1[0][0]), silu(c1[0][1]));
+    aout1[kb][1] = pack_bf16x2(silu(c1[0][2]), silu(c1[0][3]));
+    aout1[kb][2] = pack_bf16x2(silu(c1[1][0]), silu(c1[1][1]));
+    aout1[kb][3] = pack_bf16x2(silu(c1[1][2]), silu(c1[1][3]));
+  }
+}
+
+// Layer 1 of one tile (K = 16 features).
+AXB_D void mlp_layer1(const MlpSmem &w, const uint32_t (&a1)[4], int lane,
+                      uint32_t (&h1)[4][4]) {
+  const int t2 = (lane & 3) * 2;
+#pragma unroll
+  for (int kb = 0; kb < 4; ++kb) {
+    float cc[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int nt = 2 * kb + h;
+      const float bl = w.b1[nt * 8 + t2], bh = w.b1[nt * 8 + t2 + 1];
+      cc[h][0] = bl;
+      cc[h][1] = bh;
+      cc[h][2] = bl;
+      cc[h][3] = bh;
+      uint32_t b0, b1;
+      load_b(w.w1, MLP_LD1, nt, 0, lane, b0, b1);
+      mma_bf16_16816(cc[h], a1, b0, b1);
+    }
+    h1[kb][0] = pack_bf16x2(silu(cc[0][0]), silu(cc[0][1]));
+    h1[kb][1] = pack_bf16x2(silu(cc[0][2]), silu(cc[0][3]));
+    h1[kb][2] = pack_bf16x2(silu(cc[1][0]), silu(cc[1][1]));
+    h1[kb][3] = pack_bf16x2(silu(cc[1][2]), silu(cc[1][3]));
+  }
+}
+
+// Both tiles of the warp through the whole network; o0 / o1 are the layer-4
+// accumulator fragments of rows 0-15 and 16-31.
+AXB_D void mlp_tile2(const MlpSmem &w, const uint32_t *stage, int lane, float (&o0)[4],
+                     float (&o1)[4]) {
+  const int g = lane >> 2, t = lane & 3, t2 = t * 2;
+  uint32_t x0[4] = {stage[g * 8 + t], stage[(g + 8) * 8 + t], stage[g * 8 + t + 4],
+                    stage[(g + 8) * 8 + t + 4]};
+  uint32_t x1[4] = {stage[(g + 16) * 8 + t], stage[(g + 24) * 8 + t],
+                    stage[(g + 16) * 8 + t + 4], stage[(g + 24) * 8 + t + 4]};
+  uint32_t p0[4][4], p1[4][4], q0[4][4], q1[4][4];
+  mlp_layer1(w, x0, lane, p0);
+  mlp_layer1(w, x1, lane, p1);
+  mlp_hidden64x2(w.w2, w.b2, lane, p0, p1, q0, q1);
+  mlp_hidden64x2(w.w3, w.b3, lane, q0, q1, p0, p1);
+  const float bl = w.b4[t2], bh = w.b4[t2 + 1];
+  o0[0] = o1[0] = bl;
+  o0[1] = o1[1] = bh;
+  o0[2] = o1[2] = bl;
+  o0[3] = o1[3] = bh;
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    uint32_t b0, b1;
+    load_b(w.w4, MLP_LDH, 0, kk, lane, b0, b1);
+    mma_bf16_16816(o0, p0[kk], b0, b1);
+    mma_bf16_16816(o1, p1[kk], b0, b1);
   }
 }
 
@@ -196,16 +330,15 @@ AXB_D void mlp_tile(const MlpDev &m, const uint32_t *stage, int mt, int lane,
 // (MLP_K1 floats, zero beyond nf); `stage` is 32 x 8 words of shared memory
 // owned by this warp.  Returns this lane's two outputs.  Must be called by
 // all 32 lanes of the warp.
-AXB_D void mlp_forward_warp(const MlpDev &m, const float (&f)[MLP_K1], uint32_t *stage,
+AXB_D void mlp_forward_warp(const MlpSmem &w, const float (&f)[MLP_K1], uint32_t *stage,
                             float &y0, float &y1) {
   const int lane = threadIdx.x & 31;
 #pragma unroll
-  for (int w = 0; w < 8; ++w)
-    stage[lane * 8 + w] = pack_bf16x2(f[2 * w], f[2 * w + 1]);
+  for (int q = 0; q < 8; ++q)
+    stage[lane * 8 + q] = pack_bf16x2(f[2 * q], f[2 * q + 1]);
   __syncwarp();
   float o0[4], o1[4];
-  mlp_tile(m, stage, 0, lane, o0);
-  mlp_tile(m, stage, 1, lane, o1);
+  mlp_tile2(w, stage, lane, o0, o1);
   __syncwarp();
   // outputs 0, 1 of row r sit in lane 4 (r mod 8), registers 0/1 (r < 8) or
   // 2/3 (r >= 8) of the row's tile

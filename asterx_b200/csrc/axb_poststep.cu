@@ -542,6 +542,7 @@ AXB_API int axb_con2prim_group(axb_ctx *c, const axb_box *box,
 namespace axb {
 MlpDev mlp_device_view(const axb_mlp *m);
 int mlp_nf(const axb_mlp *m);
+int launch_mlp_guess(const axb_cells &c, const axb_mlp *m, float2 *guess, cudaStream_t s);
 
 struct C2PCellsArgs {
   axb_cells c;
@@ -550,7 +551,7 @@ struct C2PCellsArgs {
   Atmo atmo;
   double gamma_noble, Zmin;
   int use_mlp;
-  MlpDev mlp;
+  double bracket;
   DevStatus *status;
 };
 
@@ -569,7 +570,6 @@ template <class EOS>
 __global__ void __launch_bounds__(128, AXB_C2P_MINB)
     k_c2p_cells(const C2PCellsArgs a, const EOS eos) {
   __shared__ unsigned int s_hist[64];
-  __shared__ uint32_t s_stage[4][32 * 8];
   for (int q = threadIdx.x; q < 64; q += blockDim.x)
     s_hist[q] = 0;
   __syncthreads();
@@ -589,33 +589,17 @@ __global__ void __launch_bounds__(128, AXB_C2P_MINB)
     cv.DEnt = c.DEnt ? c.DEnt[i] : 0.0;
     glo = sym3{c.g[0][i], c.g[1][i], c.g[2][i], c.g[3][i], c.g[4][i], c.g[5][i]};
   }
-  // learned guess: all lanes of the warp take part in the MMA
+  // learned guess (x = h W, W) from k_mlp_guess
   double zguess = -1.0, vsqguess = -1.0, xlo = -1.0, xhi = -1.0;
-  if (a.use_mlp) {
-    float f[MLP_K1];
-#pragma unroll
-    for (int k = 0; k < MLP_K1; ++k)
-      f[k] = 0.0f;
-    CellInvariants inv{1.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    if (valid) {
-      inv = cell_invariants(cv.dens, cv.mom, cv.tau, cv.DYe, cv.dBvec, glo);
-      mlp_features(inv, a.mlp.nf, f);
-    }
-    float y0, y1;
-    mlp_forward_warp(a.mlp, f, s_stage[threadIdx.x >> 5], y0, y1);
-    if (valid) {
-      // y0 places x = h W in the Palenzuela scheme's initial bracket
-      // (c2p_1DPalenzuela.hxx:395-398)
-      const double lo = fmax(1e-10, 1.0 + inv.q - inv.s), hi = 2.0 + 2.0 * inv.q - inv.s;
-      const double x = lo + double(y0) * (hi - lo);
-      const double W = fmax(exp(double(y1)), 1.0);
-      zguess = inv.D * x; // Z = rho h W^2 = D (h W)
-      vsqguess = 1.0 - 1.0 / (W * W);
-      xlo = x * (1.0 - a.mlp.bracket);
-      xhi = x * (1.0 + a.mlp.bracket);
-      if (!(zguess > 0.0 && zguess < 1e300 && vsqguess >= 0.0 && vsqguess < 1.0))
-        zguess = vsqguess = xlo = xhi = -1.0;
-    }
+  if (a.use_mlp && valid) {
+    const float2 gs = reinterpret_cast<const float2 *>(c.guess)[i];
+    const double x = gs.x, W = gs.y;
+    zguess = cv.dens / sqrt(det3(glo)) * x; // Z = rho h W^2 = D (h W)
+    vsqguess = 1.0 - 1.0 / (W * W);
+    xlo = x * (1.0 - a.bracket);
+    xhi = x * (1.0 + a.bracket);
+    if (!(zguess > 0.0 && zguess < 1e300 && vsqguess >= 0.0 && vsqguess < 1.0))
+      zguess = vsqguess = xlo = xhi = -1.0;
   }
   int iters_first = -1;
   bool failed = false;
@@ -757,8 +741,11 @@ AXB_API int axb_c2p_cells(axb_ctx *ctx, const axb_cells *cells, const axb_params
   a.c2p_second = p->c2p_second;
   a.status = ctx->status;
   a.use_mlp = mlp != nullptr;
+  a.bracket = 0.0;
   if (mlp) {
-    a.mlp = mlp_device_view(mlp);
+    if (!cells->guess)
+      return AXB_ERR_ARG;
+    a.bracket = mlp_device_view(mlp).bracket;
     if (eos->kind == 1 && mlp_nf(mlp) != 9)
       return AXB_ERR_ARG; // the tabulated guess takes Ye as a ninth input
   }
@@ -791,6 +778,13 @@ AXB_API int axb_c2p_cells(axb_ctx *ctx, const axb_cells *cells, const axb_params
   if (blocks > 0x7fffffffLL)
     return AXB_ERR_TOO_LARGE;
   cudaStream_t s = (cudaStream_t)stream;
+  if (mlp) {
+    axb_mark(ctx, AXB_R_MLP, s, true);
+    const int rc = launch_mlp_guess(*cells, mlp, reinterpret_cast<float2 *>(cells->guess), s);
+    axb_mark(ctx, AXB_R_MLP, s, false);
+    if (rc)
+      return rc;
+  }
   axb_mark(ctx, AXB_R_C2P_CELLS, s, true);
   if (eos->kind == 1)
     k_c2p_cells<<<(unsigned)blocks, 128, 0, s>>>(a, tab_for_launch(*eos, a.status));

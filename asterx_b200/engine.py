@@ -243,6 +243,14 @@ class Engine:
         return abi.cells_struct(n, ptrs)
 
     def c2p_cells(self, cells, params: Params, eos, mlp=None, stream=None):
+        if mlp is not None and not cells.guess:
+            # scratch for the learned guess, kept for later calls of this size
+            n = int(cells.n)
+            buf = getattr(self, "_guess_buf", None)
+            if buf is None or buf.numel() < 2 * n:
+                buf = self.torch.empty(2 * n, dtype=self.torch.float32, device=self.device)
+                self._guess_buf = buf
+            cells.guess = buf.data_ptr()
         self._check(self.lib.axb_c2p_cells(self.ctx, C.byref(cells), C.byref(params), eos,
                                            mlp, self.stream_ptr(stream)), "axb_c2p_cells")
 

@@ -66,6 +66,14 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the reference baseline sample")
+    ap.add_argument("--workload", default="substep", choices=["substep", "c2p"],
+                    help="substep: the RK3 substep of one box (the headline); "
+                         "c2p: the independent-cell recovery microbenchmark, "
+                         "plain seeds vs the learned guess")
+    ap.add_argument("--cells", type=int, default=1 << 26,
+                    help="cells of the recovery microbenchmark")
+    ap.add_argument("--train-pairs", type=int, default=1 << 24)
+    ap.add_argument("--train-epochs", type=float, default=4.0)
     return ap.parse_args()
 
 
@@ -140,7 +148,34 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # reference CPU code (the checker build of the reference sources)
 # ---------------------------------------------------------------------------
+class _StdoutToStderr:
+    """Send file descriptor 1 to stderr while the reference code runs: its
+    Palenzuela scheme prints from inside the solver when a bracket fails,
+    and the benchmark's stdout must carry exactly one JSON line."""
+
+    def __enter__(self):
+        import ctypes
+        sys.stdout.flush()
+        self._libc = ctypes.CDLL(None)
+        self._libc.fflush(None)
+        self._saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        self._libc.fflush(None)
+        sys.stdout.flush()
+        os.dup2(self._saved, 1)
+        os.close(self._saved)
+        return False
+
+
 def reference_substep_rate(seconds, recon, seed=2, start_n=24):
+    with _StdoutToStderr():
+        return _reference_substep_rate(seconds, recon, seed, start_n)
+
+
+def _reference_substep_rate(seconds, recon, seed=2, start_n=24):
     """Time the reference's scheduled routines (AsterX_Fluxes,
     AsterX_SourceTerms, AsterX_RHS, the stage update, AsterX_ComputedBstagFromA,
     AsterX_ComputedBFromdBstag, AsterX_Con2Prim) on one box of the workload,
@@ -395,10 +430,141 @@ def ours(args):
     return 0
 
 
+def c2p_bench(args):
+    """Recovery microbenchmark: 2^26 independent cells (rho log-U[1e-12, 1e-2],
+    eps log-U[1e-6, 10], W U[1, 50], b^2/rho log-U[1e-4, 100], isotropic
+    directions, random metric), conserved variables from the exact FP64
+    prim->cons map; Noble with Palenzuela backup at c2p_tol 1e-10.  The MLP
+    guess is trained first on separately seeded pairs (not timed).  Reports
+    cells/s of both, the Noble iteration histogram, the fallback rate and
+    the maximum relative error of the recovered primitives against the truth."""
+    import numpy as np
+    import torch
+
+    from asterx_b200 import abi
+    from asterx_b200 import workloads as W
+    from asterx_b200.engine import Engine
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    eng = Engine(0)
+    gamma = 5.0 / 3.0
+    eos = eng.eos_idealgas(gamma, rho=(1e-40, 1e10), eps=(0.0, 1e10))
+    # floors and ceilings set so that they do not alter the truth: W up to 50,
+    # eps down to 1e-6 (temperature floor t_atmo below it), rho down to 1e-12
+    params = abi.default_params(c2p_prime="noble", c2p_second="palenzuela", c2p_tol=1e-10,
+                                max_iter=100, vw_lim=60.0, B_lim=1e8, rho_abs_min=1e-20,
+                                t_atmo=1e-12)
+    # training (separately seeded pairs)
+    t_train = time.time()
+    nt = args.train_pairs
+    tr = W.c2p_cells(nt, seed=1001, gamma=gamma, device=dev)
+    feats = torch.empty((nt, 8), dtype=torch.float32, device=dev)
+    eng.mlp_features(eng.cells(nt, {k: tr[k] for k in abi.CELL_INPUTS}), 8, feats)
+    tgt = torch.stack([tr["t_u"], tr["t_lnw"]], dim=1).float().contiguous()
+    del tr
+    mlp = eng.mlp_create(8, seed=7, bracket=0.02)
+    loss = torch.zeros(1, dtype=torch.float32, device=dev)
+    bs = 65536
+    nsteps = max(1, int(args.train_epochs * nt / bs))
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(3)
+    for step in range(nsteps):
+        idx = torch.randint(0, nt, (bs,), generator=gen, device=dev)
+        lr = 3e-3 if step < 0.7 * nsteps else 5e-4
+        eng.mlp_train_step(mlp, feats[idx], tgt[idx], lr=lr, loss=loss)
+    torch.cuda.synchronize()
+    train_s = time.time() - t_train
+    train_loss = loss.item()
+    del feats, tgt
+
+    n = args.cells
+    cells = W.c2p_cells(n, seed=2002, gamma=gamma, device=dev)
+    truth = {k: cells[k] for k in ("rho", "eps", "press", "W")}
+    t = {k: cells[k] for k in abi.CELL_INPUTS}
+    outs = ["rho", "eps", "press", "w_lorentz", "iters", "flag"]
+    for k in outs:
+        t[k] = torch.empty(n, dtype=torch.float64, device=dev)
+    guess = torch.empty(2 * n, dtype=torch.float32, device=dev)
+    cstruct = eng.cells(n, t)
+    cstruct.guess = guess.data_ptr()
+    stream = torch.cuda.current_stream(dev)
+    res = {}
+    for name, m in (("plain", None), ("learned", mlp)):
+        for _ in range(args.warmup):
+            eng.c2p_cells(cstruct, params, eos, mlp=m)
+        torch.cuda.synchronize()
+        eng.status_reset()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        eng.timing_begin()
+        e0.record(stream)
+        for _ in range(args.steps):
+            eng.c2p_cells(cstruct, params, eos, mlp=m)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        region_ms, region_n = eng.timing_end(len(REGIONS))
+        ms = e0.elapsed_time(e1) / args.steps
+        st = eng.status()
+        flag = t["flag"]
+        ok = flag == abi.C2P_PRIME
+        errs = {}
+        for k, tk in (("rho", "rho"), ("eps", "eps"), ("press", "press"), ("w_lorentz", "W")):
+            e = ((t[k] - truth[tk]).abs() / truth[tk].abs())[ok]
+            errs[k] = float(e.max().item()) if e.numel() else None
+        # cells that converged to a state away from the truth (a wrong root)
+        bad = (((t["rho"] - truth["rho"]).abs() / truth["rho"]) > 1e-6) & ok
+        errs["cells_rho_off_by_1e-6"] = int(bad.sum().item())
+        hist = st["iter_hist"] / max(1, args.steps)
+        it = np.arange(64)
+        res[name] = {
+            "cells_per_s": n / (ms / 1e3), "ms": ms,
+            "mean_iters": float((hist * it).sum() / max(1, hist.sum())),
+            "iter_hist": {int(i): int(v) for i, v in enumerate(hist) if v},
+            "fallback_rate": float((~ok).double().mean().item()),
+            "fail_rate": float((flag == abi.C2P_FAIL).double().mean().item()),
+            "max_rel_err": errs,
+            "recovery_kernel_ms": region_ms[REGIONS.index("c2p_cells")] / max(1, args.steps),
+            "mlp_kernel_ms": region_ms[REGIONS.index("mlp")] / max(1, args.steps),
+            "gpu_launches": int(sum(region_n)),
+        }
+    alg = 8 * (16 + 8)  # bytes per cell: 16 inputs read, 8 outputs written
+    peak, peak_kind = peak_hbm()
+    lr_ = res["learned"]
+    rk = lr_["recovery_kernel_ms"]
+    line = {
+        "metric": "c2p cells/s (learned guess)", "value": lr_["cells_per_s"],
+        "unit": "cells/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": lr_["ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64 (MLP bf16/f32)",
+        "data": "synthetic (seeded cells of the configuration)",
+        "config": {"workload": f"{n} independent cells, Noble (Palenzuela backup), "
+                               "ideal gas Gamma=5/3, c2p_tol 1e-10, MLP 8-64-64-64-2 "
+                               f"trained on {nt} pairs",
+                   "cells": n, "l2": "inputs larger than L2"},
+        "plain": res["plain"], "learned": res["learned"],
+        "speedup_learned_vs_plain": lr_["cells_per_s"] / res["plain"]["cells_per_s"],
+        "training": {"pairs": nt, "steps": nsteps, "batch": bs, "final_loss": train_loss,
+                     "seconds": train_s},
+        "roofline": {"bound": "hbm", "kernel": "c2p_cells",
+                     "achieved": alg * n / (rk / 1e3) / 1e9, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": alg * n / (rk / 1e3) / 1e9 / peak, "traffic": None},
+        "gpu_launches": lr_["gpu_launches"],
+    }
+    print(json.dumps(line), flush=True)
+    eng.close()
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.workload == "c2p":
+        return c2p_bench(args)
     return ours(args)
 
 

@@ -324,6 +324,7 @@ typedef struct axb_cells {
   const double *seed_rho, *seed_eps, *seed_Ye, *seed_vel[3], *seed_temperature;
   double *rho, *eps, *press, *vel[3], *w_lorentz, *Ye, *temperature, *entropy;
   double *iters, *flag;
+  float *guess; /* scratch, 2 floats per cell; required with a learned guess */
 } axb_cells;
 
 /* Learned initial guess: an MLP nf -> 64 -> 64 -> 64 -> 2 (SiLU hidden
@@ -336,6 +337,9 @@ typedef struct axb_cells {
  * (c2p_2DNoble.hxx:374-393), the Palenzuela scheme brackets x by
  * [x (1 - bracket), x (1 + bracket)] when that interval brackets the root
  * and otherwise keeps its own bracket (c2p_1DPalenzuela.hxx:395-401).
+ * The network runs in its own kernel before the recovery (a persistent
+ * grid whose CTAs stage the weights in shared memory once) and leaves
+ * (x, W) per cell in the caller's `guess` scratch.
  * No counterpart in the reference. */
 typedef struct axb_mlp axb_mlp;
 

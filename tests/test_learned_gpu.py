@@ -104,9 +104,10 @@ def test_mlp_features_forward_and_gradient(engine):
     y_ref, _ = mlp_ref.forward(params, want)
     err = np.abs(y_gpu - y_ref)
     # identical rounding points; differences come from the FP32 summation
-    # order (and, rarely, a hidden activation landing on the other side of
-    # a BF16 rounding boundary)
-    assert np.median(err) <= 1e-5 and err.max() <= 2e-2, (np.median(err), err.max())
+    # order and the hardware tanh in the inference SiLU (relative error
+    # ~2^-11, below the BF16 rounding of each activation), which moves some
+    # activations to the neighbouring BF16 value
+    assert np.median(err) <= 1e-3 and err.max() <= 5e-2, (np.median(err), err.max())
 
     tgt = np.stack([cells["t_u"], cells["t_lnw"]], axis=1).astype(np.float32)
     tg = torch.as_tensor(tgt, device=engine.device)
