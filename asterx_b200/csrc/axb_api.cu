@@ -6,6 +6,7 @@
 #include <limits>
 #include <new>
 
+#include "axb_batch.cuh"
 #include "axb_flux_launch.cuh"
 #include "axb_internal.hxx"
 #include "axb_rhs_misc.cuh"
@@ -528,6 +529,113 @@ int launch_rhs_misc(int which, const RhsArgs &a, cudaStream_t s) {
     k_ct_psi<<<grid, T, 0, s>>>(a);
   }
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+}
+} // namespace axb
+
+// ---------------------------------------------------------------------------
+// batched forms (see axb_batch.cuh)
+// ---------------------------------------------------------------------------
+namespace {
+template <int FD>
+__global__ void __launch_bounds__(128, AXB_SOURCES_MINB)
+    k_sources_batch(const RhsArgs *args, const TileTable t, unsigned long long *ctr) {
+  batch_loop(args, t, ctr, [&](const RhsArgs &a, const uint3 bid) { sources_body<FD>(a, bid); });
+}
+__global__ void __launch_bounds__(128) k_aux_batch(const RhsArgs *args, const TileTable t, unsigned long long *ctr) {
+  batch_loop(args, t, ctr, [&](const RhsArgs &a, const uint3 bid) { aux_body(a, bid); });
+}
+__global__ void __launch_bounds__(128) k_ct_psi_batch(const RhsArgs *args, const TileTable t, unsigned long long *ctr) {
+  batch_loop(args, t, ctr, [&](const RhsArgs &a, const uint3 bid) { ct_psi_body(a, bid); });
+}
+} // namespace
+
+namespace axb {
+// The per-box RHS argument blocks of a batch (checked as axb_rhs_group
+// checks them), in device memory.
+int batch_rhs_setup(axb_ctx *c, int nbox, const axb_box *boxes, const axb_fields *f,
+                    const axb_params *p, const axb_eos *eos, void **out) {
+  *out = nullptr;
+  RhsArgs *h = new (std::nothrow) RhsArgs[nbox];
+  if (!h)
+    return AXB_ERR_ARG;
+  for (int b = 0; b < nbox; ++b) {
+    int rc = fill_rhs_args(c, boxes + b, f + b, p, h[b]);
+    if (!rc && eos->kind == 1 && !h[b].rec_temp)
+      rc = AXB_ERR_UNSUPPORTED;
+    if (rc) {
+      delete[] h;
+      return rc;
+    }
+  }
+  int rc = AXB_OK;
+  if (cudaMalloc(out, nbox * sizeof(RhsArgs)) != cudaSuccess ||
+      cudaMemcpy(*out, h, nbox * sizeof(RhsArgs), cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = AXB_ERR_CUDA;
+  delete[] h;
+  return rc;
+}
+
+// single-box grids: 0 sources, 2 aux, 3 CT + Psi (as launch_rhs_misc)
+uint3 rhs_misc_grid(int which, const axb_box &b) {
+  const int T = 128;
+  if (which <= 1)
+    return make_uint3((b.n[0] + T - 1) / T, b.n[1], b.n[2]);
+  if (which == 2)
+    return make_uint3((b.n[0] + 5 + T - 1) / T, b.n[1] + 5, b.n[2] + 5);
+  return make_uint3((b.n[0] + 1 + T - 1) / T, b.n[1] + 1, b.n[2] + 1);
+}
+
+int launch_rhs_misc_batch(int which, const void *args, const TileTable &t,
+                          unsigned long long *ctr, int nblocks, cudaStream_t s) {
+  if (t.total == 0)
+    return AXB_OK;
+  const RhsArgs *a = static_cast<const RhsArgs *>(args);
+  if (which == 0)
+    k_sources_batch<2><<<nblocks, 128, 0, s>>>(a, t, ctr);
+  else if (which == 1)
+    k_sources_batch<4><<<nblocks, 128, 0, s>>>(a, t, ctr);
+  else if (which == 2)
+    k_aux_batch<<<nblocks, 128, 0, s>>>(a, t, ctr);
+  else
+    k_ct_psi_batch<<<nblocks, 128, 0, s>>>(a, t, ctr);
+  return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+}
+
+using Ctr = unsigned long long;
+int launch_flux_batch_ppm(int, const RhsArgs *, const TileTable &, Ctr *, const axb_eos &,
+                          DevStatus *, int, int, cudaStream_t);
+int launch_flux_batch_wenoz(int, const RhsArgs *, const TileTable &, Ctr *, const axb_eos &,
+                            DevStatus *, int, int, cudaStream_t);
+int launch_flux_batch_mp5(int, const RhsArgs *, const TileTable &, Ctr *, const axb_eos &,
+                          DevStatus *, int, int, cudaStream_t);
+int launch_flux_batch_low(int, int, const RhsArgs *, const TileTable &, Ctr *,
+                          const axb_eos &, DevStatus *, int, int, cudaStream_t);
+
+int launch_flux_batch(int recon, int dir, const RhsArgs *args, const TileTable &t, Ctr *ctr,
+                      const axb_eos &eos, DevStatus *st, int seglen, int nblocks,
+                      cudaStream_t s) {
+  switch (recon) {
+  case AXB_RECON_PPM:
+    return launch_flux_batch_ppm(dir, args, t, ctr, eos, st, seglen, nblocks, s);
+  case AXB_RECON_WENOZ:
+    return launch_flux_batch_wenoz(dir, args, t, ctr, eos, st, seglen, nblocks, s);
+  case AXB_RECON_MP5:
+    return launch_flux_batch_mp5(dir, args, t, ctr, eos, st, seglen, nblocks, s);
+  default:
+    return launch_flux_batch_low(recon, dir, args, t, ctr, eos, st, seglen, nblocks, s);
+  }
+}
+
+// single-box grid of a flux pass (as launch_flux_pass_eos; the x pass is a
+// 1-D grid of 4-warp blocks over the rows)
+uint3 flux_grid(int dir, const axb_box &b, int seglen) {
+  if (dir == 0) {
+    const long long warps = (long long)(b.n[1] + 2) * (b.n[2] + 2);
+    return make_uint3(unsigned((warps * 32 + 127) / 128), 1, 1);
+  }
+  const int T1 = dir == 2 ? 1 : 2;
+  return make_uint3((b.n[0] + 2 + 31) / 32, (b.n[T1] + 2 + 3) / 4,
+                    (b.n[dir] + seglen - 1) / seglen);
 }
 } // namespace axb
 

@@ -2,6 +2,7 @@
 // its own translation unit (axb_flux_<scheme>.cu) to keep builds parallel.
 #pragma once
 
+#include "axb_batch.cuh"
 #include "axb_internal.hxx"
 #include "axb_rhs_kernels.cuh"
 
@@ -40,6 +41,55 @@ int launch_flux_pass_t(int dir, const RhsArgs &a, const axb_eos &eos,
     return launch_flux_pass_eos<RECON>(dir, a, tab_for_launch(eos, a.status), seglen, s);
   return AXB_ERR_UNSUPPORTED;
 }
+
+// Batched flux passes over the boxes of a batch (tile tables built by the
+// batch with the grids of launch_flux_pass_eos).
+template <int DIR, int RECON, class EOS>
+__global__ void __launch_bounds__(128, AXB_FLUX_MINB)
+    k_flux_pass_batch(const RhsArgs *args, const TileTable t, unsigned long long *ctr, const EOS eos, const int seglen) {
+  batch_loop(args, t, ctr, [&](const RhsArgs &a, const uint3 bid) {
+    flux_pass_body<DIR, RECON, EOS>(a, eos, seglen, bid);
+  });
+}
+
+template <int RECON, class EOS>
+__global__ void __launch_bounds__(128, AXB_FLUX_X_MINB)
+    k_flux_x_batch(const RhsArgs *args, const TileTable t, unsigned long long *ctr, const EOS eos) {
+  batch_loop(args, t, ctr, [&](const RhsArgs &a, const uint3 bid) {
+    flux_x_body<RECON, EOS>(a, eos, bid);
+  });
+}
+
+template <int RECON, class EOS>
+int launch_flux_batch_eos(int dir, const RhsArgs *args, const TileTable &t,
+                          unsigned long long *ctr, const EOS &eos, int seglen, int nblocks,
+                          cudaStream_t s) {
+  if (t.total == 0)
+    return AXB_OK;
+  if (dir == 0)
+    k_flux_x_batch<RECON, EOS><<<nblocks, 128, 0, s>>>(args, t, ctr, eos);
+  else if (dir == 1)
+    k_flux_pass_batch<1, RECON, EOS><<<nblocks, dim3(32, 4), 0, s>>>(args, t, ctr, eos, seglen);
+  else
+    k_flux_pass_batch<2, RECON, EOS><<<nblocks, dim3(32, 4), 0, s>>>(args, t, ctr, eos, seglen);
+  return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+}
+
+template <int RECON>
+int launch_flux_batch_t(int dir, const RhsArgs *args, const TileTable &t,
+                        unsigned long long *ctr, const axb_eos &eos, DevStatus *status,
+                        int seglen, int nblocks, cudaStream_t s) {
+  if (eos.kind == 0)
+    return launch_flux_batch_eos<RECON>(dir, args, t, ctr, eos.ideal, seglen, nblocks, s);
+  if (eos.kind == 1)
+    return launch_flux_batch_eos<RECON>(dir, args, t, ctr, tab_for_launch(eos, status), seglen,
+                                        nblocks, s);
+  return AXB_ERR_UNSUPPORTED;
+}
+
+int launch_flux_batch(int recon, int dir, const RhsArgs *args, const TileTable &t,
+                      unsigned long long *ctr, const axb_eos &eos, DevStatus *status,
+                      int seglen, int nblocks, cudaStream_t s);
 
 int launch_flux_ppm(int dir, const RhsArgs &a, const axb_eos &eos, int seglen, cudaStream_t s);
 int launch_flux_wenoz(int dir, const RhsArgs &a, const axb_eos &eos, int seglen, cudaStream_t s);

@@ -14,4 +14,18 @@ int launch_flux_low(int recon, int dir, const RhsArgs &a, const axb_eos &eos,
   }
   return AXB_ERR_UNSUPPORTED;
 }
+int launch_flux_batch_low(int recon, int dir, const RhsArgs *args, const TileTable &t,
+                          unsigned long long *ctr, const axb_eos &eos, DevStatus *st,
+                          int seglen, int nblocks, cudaStream_t s) {
+  switch (recon) {
+  case AXB_RECON_GODUNOV:
+    return launch_flux_batch_t<AXB_RECON_GODUNOV>(dir, args, t, ctr, eos, st, seglen, nblocks, s);
+  case AXB_RECON_MINMOD:
+    return launch_flux_batch_t<AXB_RECON_MINMOD>(dir, args, t, ctr, eos, st, seglen, nblocks, s);
+  case AXB_RECON_MONOCENTRAL:
+    return launch_flux_batch_t<AXB_RECON_MONOCENTRAL>(dir, args, t, ctr, eos, st, seglen, nblocks,
+                                                      s);
+  }
+  return AXB_ERR_UNSUPPORTED;
+}
 } // namespace axb

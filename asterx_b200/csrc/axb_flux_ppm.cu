@@ -5,4 +5,9 @@ int launch_flux_ppm(int dir, const RhsArgs &a, const axb_eos &eos, int seglen,
                    cudaStream_t s) {
   return launch_flux_pass_t<AXB_RECON_PPM>(dir, a, eos, seglen, s);
 }
+int launch_flux_batch_ppm(int dir, const RhsArgs *args, const TileTable &t,
+                          unsigned long long *ctr, const axb_eos &eos, DevStatus *st,
+                          int seglen, int nblocks, cudaStream_t s) {
+  return launch_flux_batch_t<AXB_RECON_PPM>(dir, args, t, ctr, eos, st, seglen, nblocks, s);
+}
 } // namespace axb

@@ -4,8 +4,10 @@
 // Also the RK stage update and the periodic ghost fill of one box.
 #include <cmath>
 #include <cstring>
+#include <new>
 #include <limits>
 
+#include "axb_batch.cuh"
 #include "axb_c2p.cuh"
 #include "axb_internal.hxx"
 #include "axb_mlp.cuh"
@@ -40,12 +42,12 @@ struct C2PBoxArgs {
 // ComputeStaggeredB<dir> (AsterX/src/computeBfromA.cxx:20-56) on the faces
 // [ng, ng+n] along d and [ng-1, ng+n] across (one ghost layer, which the next
 // RHS needs and the reference obtains by SYNC).
-__global__ void __launch_bounds__(128) k_bstag(const C2PBoxArgs a) {
+AXB_D void bstag_body(const C2PBoxArgs &a, const uint3 bid) {
   const BoxDev &b = a.b;
   const int ng = b.ng;
-  const int i = ng - 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = ng - 1 + blockIdx.y;
-  const int k = ng - 1 + blockIdx.z;
+  const int i = ng - 1 + bid.x * blockDim.x + threadIdx.x;
+  const int j = ng - 1 + bid.y;
+  const int k = ng - 1 + bid.z;
   if (i > ng + b.n[0])
     return;
   const long long I = b.at(i, j, k);
@@ -61,6 +63,10 @@ __global__ void __launch_bounds__(128) k_bstag(const C2PBoxArgs a) {
     a.dBstag[1][I] = b.idx[2] * (Ax[ijkp] - Ax[I]) - b.idx[0] * (Az[ipjk] - Az[I]);
   if (in_k && i <= ng + b.n[0] && j <= ng + b.n[1])
     a.dBstag[2][I] = b.idx[0] * (Ay[ipjk] - Ay[I]) - b.idx[1] * (Ax[ijpk] - Ax[I]);
+}
+__global__ void __launch_bounds__(128)
+    k_bstag(const C2PBoxArgs a) {
+  bstag_body(a, blockIdx);
 }
 
 template <class EOS>
@@ -112,8 +118,7 @@ AXB_D void run_solver(int which, const EOS &eos, const C2PBoxArgs &a,
 #define AXB_C2P_MINB 4 // resident CTAs per SM the register budget must allow
 #endif
 template <class EOS>
-__global__ void __launch_bounds__(128, AXB_C2P_MINB)
-    k_c2p_box(const C2PBoxArgs a, const EOS eos) {
+AXB_D void c2p_box_body(const C2PBoxArgs &a, const EOS &eos, const uint3 bid) {
   __shared__ unsigned int s_hist[64];
   const BoxDev &b = a.b;
   if (a.want_hist) {
@@ -121,9 +126,9 @@ __global__ void __launch_bounds__(128, AXB_C2P_MINB)
       s_hist[q] = 0;
     __syncthreads();
   }
-  const int i = b.ng + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = b.ng + blockIdx.y;
-  const int k = b.ng + blockIdx.z;
+  const int i = b.ng + bid.x * blockDim.x + threadIdx.x;
+  const int j = b.ng + bid.y;
+  const int k = b.ng + bid.z;
   int iters_first = -1;
   bool failed = false;
   if (i < b.ng + b.n[0]) {
@@ -300,6 +305,11 @@ __global__ void __launch_bounds__(128, AXB_C2P_MINB)
       if (s_hist[q])
         atomicAdd(&a.status->c2p_iter_hist[q], (unsigned long long)s_hist[q]);
   }
+}
+template <class EOS>
+__global__ void __launch_bounds__(128, AXB_C2P_MINB)
+    k_c2p_box(const C2PBoxArgs a, const EOS eos) {
+  c2p_box_body<EOS>(a, eos, blockIdx);
 }
 
 } // namespace axb
@@ -499,6 +509,70 @@ int fill_c2p_args(axb_ctx *c, const axb_box *box, const axb_fields *f,
 }
 
 } // namespace
+
+// ---------------------------------------------------------------------------
+// batched forms (see axb_batch.cuh)
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void __launch_bounds__(128) k_bstag_batch(const C2PBoxArgs *args, const TileTable t, unsigned long long *ctr) {
+  batch_loop(args, t, ctr, [&](const C2PBoxArgs &a, const uint3 bid) { bstag_body(a, bid); });
+}
+template <class EOS>
+__global__ void __launch_bounds__(128, AXB_C2P_MINB)
+    k_c2p_box_batch(const C2PBoxArgs *args, const TileTable t, unsigned long long *ctr, const EOS eos) {
+  batch_loop(args, t, ctr, [&](const C2PBoxArgs &a, const uint3 bid) {
+    c2p_box_body<EOS>(a, eos, bid);
+  });
+}
+} // namespace
+
+namespace axb {
+// The per-box post-step argument blocks of a batch (checked as
+// axb_con2prim_group checks them), in device memory.
+int batch_c2p_setup(axb_ctx *c, int nbox, const axb_box *boxes, const axb_fields *f,
+                    const axb_params *p, const axb_eos *eos, void **out) {
+  *out = nullptr;
+  C2PBoxArgs *h = new (std::nothrow) C2PBoxArgs[nbox];
+  if (!h)
+    return AXB_ERR_ARG;
+  for (int b = 0; b < nbox; ++b) {
+    const int rc = fill_c2p_args(c, boxes + b, f + b, p, eos, h[b]);
+    if (rc) {
+      delete[] h;
+      return rc;
+    }
+  }
+  int rc = AXB_OK;
+  if (cudaMalloc(out, nbox * sizeof(C2PBoxArgs)) != cudaSuccess ||
+      cudaMemcpy(*out, h, nbox * sizeof(C2PBoxArgs), cudaMemcpyHostToDevice) != cudaSuccess)
+    rc = AXB_ERR_CUDA;
+  delete[] h;
+  return rc;
+}
+
+// single-box grids of the face curl (0) and the recovery (1)
+uint3 c2p_grid(int which, const axb_box &b) {
+  const int T = 128;
+  if (which == 0)
+    return make_uint3((b.n[0] + 2 + T - 1) / T, b.n[1] + 2, b.n[2] + 2);
+  return make_uint3((b.n[0] + T - 1) / T, b.n[1], b.n[2]);
+}
+
+int launch_c2p_batch(int which, const void *args, const TileTable &t,
+                     unsigned long long *ctr, const axb_eos &eos, DevStatus *status,
+                     int nblocks, cudaStream_t s) {
+  if (t.total == 0)
+    return AXB_OK;
+  const C2PBoxArgs *a = static_cast<const C2PBoxArgs *>(args);
+  if (which == 0)
+    k_bstag_batch<<<nblocks, 128, 0, s>>>(a, t, ctr);
+  else if (eos.kind == 1)
+    k_c2p_box_batch<<<nblocks, 128, 0, s>>>(a, t, ctr, tab_for_launch(eos, status));
+  else
+    k_c2p_box_batch<<<nblocks, 128, 0, s>>>(a, t, ctr, eos.ideal);
+  return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+}
+} // namespace axb
 
 // AsterX_Con2PrimGroup on one box (AsterX/schedule.ccl:119-165): replaces
 // AsterX_ComputedBstagFromA (computeBfromA.cxx:58-65),

@@ -156,23 +156,22 @@ AXB_D void flux_status(const RhsArgs &a, double smax, bool bad) {
 // by the edge electric field); faces along DIR: [ng, ng+n].
 // ---------------------------------------------------------------------------
 template <int DIR, int RECON, class EOS>
-__global__ void __launch_bounds__(128, AXB_FLUX_MINB)
-    k_flux_pass(const RhsArgs a, const EOS eos, const int seglen) {
+AXB_D void flux_pass_body(const RhsArgs &a, const EOS &eos, const int &seglen, const uint3 bid) {
   static_assert(DIR != 0, "the x pass is k_flux_x");
   constexpr int D1 = (DIR + 1) % 3, D2 = (DIR + 2) % 3;
   constexpr int T0 = 0;
   constexpr int T1 = (DIR == 2) ? 1 : 2;
   const BoxDev &b = a.b;
   const int ng = b.ng;
-  const int t0 = ng - 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int t1 = ng - 1 + blockIdx.y * blockDim.y + threadIdx.y;
+  const int t0 = ng - 1 + bid.x * blockDim.x + threadIdx.x;
+  const int t1 = ng - 1 + bid.y * blockDim.y + threadIdx.y;
   const bool active = (t0 <= ng + b.n[T0]) && (t1 <= ng + b.n[T1]);
   double smax = 0.0;
   bool bad = false;
   if (active) {
     const bool trans_int = (t0 >= ng) && (t0 < ng + b.n[T0]) && (t1 >= ng) &&
                            (t1 < ng + b.n[T1]);
-    const int f0 = ng + blockIdx.z * seglen;
+    const int f0 = ng + bid.z * seglen;
     const int flast = min(f0 + seglen, ng + b.n[DIR]);
     const long long sd = b.stride(DIR);
     int ijk[3];
@@ -216,6 +215,11 @@ __global__ void __launch_bounds__(128, AXB_FLUX_MINB)
   }
   flux_status(a, smax, bad);
 }
+template <int DIR, int RECON, class EOS>
+__global__ void __launch_bounds__(128, AXB_FLUX_MINB)
+    k_flux_pass(const RhsArgs a, const EOS eos, const int seglen) {
+  flux_pass_body<DIR, RECON, EOS>(a, eos, seglen, blockIdx);
+}
 
 // ---------------------------------------------------------------------------
 // k_flux_x: the x pass with the lanes of a warp along x, so that every
@@ -229,12 +233,11 @@ __global__ void __launch_bounds__(128, AXB_FLUX_MINB)
 // advances 30 cells.
 // ---------------------------------------------------------------------------
 template <int RECON, class EOS>
-__global__ void __launch_bounds__(128, AXB_FLUX_X_MINB)
-    k_flux_x(const RhsArgs a, const EOS eos) {
+AXB_D void flux_x_body(const RhsArgs &a, const EOS &eos, const uint3 bid) {
   const BoxDev &b = a.b;
   const int ng = b.ng;
   const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int warp = (bid.x * blockDim.x + threadIdx.x) >> 5;
   const int ny = b.n[1] + 2; // rows j, k in [ng-1, ng+n]
   const int nz = b.n[2] + 2;
   double smax = 0.0;
@@ -286,6 +289,11 @@ __global__ void __launch_bounds__(128, AXB_FLUX_X_MINB)
     }
   }
   flux_status(a, smax, bad);
+}
+template <int RECON, class EOS>
+__global__ void __launch_bounds__(128, AXB_FLUX_X_MINB)
+    k_flux_x(const RhsArgs a, const EOS eos) {
+  flux_x_body<RECON, EOS>(a, eos, blockIdx);
 }
 
 } // namespace axb

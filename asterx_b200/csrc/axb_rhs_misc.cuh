@@ -89,11 +89,11 @@ AXB_HD double sym_get(const sym3 &m, int p, int q) { return m(p, q); }
 #define AXB_SOURCES_MINB 1
 #endif
 template <int FD>
-__global__ void __launch_bounds__(128, AXB_SOURCES_MINB) k_sources(const RhsArgs a) {
+AXB_D void sources_body(const RhsArgs &a, const uint3 bid) {
   const BoxDev &b = a.b;
-  const int i = b.ng + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = b.ng + blockIdx.y;
-  const int k = b.ng + blockIdx.z;
+  const int i = b.ng + bid.x * blockDim.x + threadIdx.x;
+  const int j = b.ng + bid.y;
+  const int k = b.ng + bid.z;
   if (i >= b.ng + b.n[0])
     return;
   const long long I = b.at(i, j, k);
@@ -222,16 +222,21 @@ __global__ void __launch_bounds__(128, AXB_SOURCES_MINB) k_sources(const RhsArgs
   a.rhs[V_TAU][I] = as * tau_source;
   a.rhs[V_DYE][I] = 0.0;
 }
+template <int FD>
+__global__ void __launch_bounds__(128, AXB_SOURCES_MINB)
+    k_sources(const RhsArgs a) {
+  sources_body<FD>(a, blockIdx);
+}
 
 // ---------------------------------------------------------------------------
 // k_aux: vertex auxiliaries of the A/Psi RHS (fluxes.cxx:798-826) on the
 // vertices [ng-2, ng+n+2] (the Psi RHS reads F at +-1 and Fbeta at +-2).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_aux(const RhsArgs a) {
+AXB_D void aux_body(const RhsArgs &a, const uint3 bid) {
   const BoxDev &b = a.b;
-  const int i = b.ng - 2 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = b.ng - 2 + blockIdx.y;
-  const int k = b.ng - 2 + blockIdx.z;
+  const int i = b.ng - 2 + bid.x * blockDim.x + threadIdx.x;
+  const int j = b.ng - 2 + bid.y;
+  const int k = b.ng - 2 + bid.z;
   if (i > b.ng + b.n[0] + 2)
     return;
   const long long I = b.at(i, j, k);
@@ -258,6 +263,10 @@ __global__ void __launch_bounds__(128) k_aux(const RhsArgs a) {
   a.aux[5][I] = be[2] * psi;
   a.aux[6][I] = alp * psi / sqrtg - dot3(be, Av);
 }
+__global__ void __launch_bounds__(128)
+    k_aux(const RhsArgs a) {
+  aux_body(a, blockIdx);
+}
 
 // ---------------------------------------------------------------------------
 // k_ct_psi: on every interior vertex (i,j,k): the x-, y-, z-edge starting
@@ -265,12 +274,12 @@ __global__ void __launch_bounds__(128) k_aux(const RhsArgs a) {
 // stored face B fluxes, rhs.cxx:171-185), and the vertex gets Psi_rhs
 // (rhs.cxx:227-252).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_ct_psi(const RhsArgs a) {
+AXB_D void ct_psi_body(const RhsArgs &a, const uint3 bid) {
   const BoxDev &b = a.b;
   const int ng = b.ng;
-  const int i = ng + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = ng + blockIdx.y;
-  const int k = ng + blockIdx.z;
+  const int i = ng + bid.x * blockDim.x + threadIdx.x;
+  const int j = ng + bid.y;
+  const int k = ng + bid.z;
   if (i > ng + b.n[0])
     return;
   const long long I = b.at(i, j, k);
@@ -317,6 +326,10 @@ __global__ void __launch_bounds__(128) k_ct_psi(const RhsArgs a) {
   } else {
     a.Psi_rhs[I] = 0.0;
   }
+}
+__global__ void __launch_bounds__(128)
+    k_ct_psi(const RhsArgs a) {
+  ct_psi_body(a, blockIdx);
 }
 
 } // namespace axb

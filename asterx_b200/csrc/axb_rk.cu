@@ -1,7 +1,9 @@
 // Runge-Kutta stage update of the evolved variables and the periodic ghost
 // fill of one box (the single-box form of the driver's SYNC).
 #include <cstring>
+#include <vector>
 
+#include "axb_batch.cuh"
 #include "axb_internal.hxx"
 
 using namespace axb;
@@ -31,11 +33,12 @@ struct StageArgs {
 
 // U_out = alpha U_n + beta U_k + (gamma dt) RHS on the interior of each
 // field's centring (cells for hydro, edges for A, vertices for Psi).
-__global__ void __launch_bounds__(128) k_rk_stage(const StageArgs a) {
+AXB_D void rk_stage_body(const StageArgs &a, double alpha, double beta, double gdt,
+                         const uint3 bid) {
   const BoxDev &b = a.b;
-  const int i = b.ng + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = b.ng + blockIdx.y;
-  const int k = b.ng + blockIdx.z;
+  const int i = b.ng + bid.x * blockDim.x + threadIdx.x;
+  const int j = b.ng + bid.y;
+  const int k = b.ng + bid.z;
   if (i > b.ng + b.n[0])
     return;
   const long long I = b.at(i, j, k);
@@ -47,8 +50,12 @@ __global__ void __launch_bounds__(128) k_rk_stage(const StageArgs a) {
     for (int d = 0; d < 3; ++d)
       in &= ijk[d] < b.ng + b.n[d] + (a.cent[v][d] ? 0 : 1);
     if (in)
-      a.out[v][I] = a.alpha * a.un[v][I] + a.beta * a.uk[v][I] + a.gdt * a.rhs[v][I];
+      a.out[v][I] = alpha * a.un[v][I] + beta * a.uk[v][I] + gdt * a.rhs[v][I];
   }
+}
+__global__ void __launch_bounds__(128)
+    k_rk_stage(const StageArgs a) {
+  rk_stage_body(a, a.alpha, a.beta, a.gdt, blockIdx);
 }
 
 struct SyncArgs {
@@ -68,11 +75,11 @@ AXB_D int wrap(int i, int ng, int n) {
 // Periodic ghost fill: every point outside the interior of its centring
 // takes the value of its periodic image inside the interior.  One block
 // handles one (j, k) row of one field.
-__global__ void __launch_bounds__(128) k_sync_periodic(const SyncArgs a) {
+AXB_D void sync_periodic_body(const SyncArgs &a, const uint3 bid) {
   const BoxDev &b = a.b;
-  const int v = blockIdx.z;
-  const int j = blockIdx.x;
-  const int k = blockIdx.y;
+  const int v = bid.z;
+  const int j = bid.x;
+  const int k = bid.y;
   double *f = a.f[v];
   const int *c = a.cent[v];
   const int ng = b.ng;
@@ -91,6 +98,10 @@ __global__ void __launch_bounds__(128) k_sync_periodic(const SyncArgs a) {
     const int is = i_in ? i : wrap(i, ng, b.n[0]);
     f[b.at(i, j, k)] = f[b.at(is, js, ks)];
   }
+}
+__global__ void __launch_bounds__(128)
+    k_sync_periodic(const SyncArgs a) {
+  sync_periodic_body(a, blockIdx);
 }
 
 int centring_of(int gf, int c[3]) {
@@ -176,3 +187,115 @@ AXB_API int axb_sync_periodic(axb_ctx *c, const axb_box *box,
   axb_mark(c, AXB_R_SYNC, (cudaStream_t)stream, false);
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
 }
+
+// ---------------------------------------------------------------------------
+// batched forms (see axb_batch.cuh)
+// ---------------------------------------------------------------------------
+namespace {
+
+__global__ void __launch_bounds__(128)
+    k_rk_stage_batch(const StageArgs *args, const TileTable t, unsigned long long *ctr, double alpha, double beta,
+                     double gdt) {
+  batch_loop(args, t, ctr, [&](const StageArgs &a, const uint3 bid) {
+    rk_stage_body(a, alpha, beta, gdt, bid);
+  });
+}
+
+__global__ void __launch_bounds__(128)
+    k_sync_batch(const SyncArgs *args, const TileTable t, unsigned long long *ctr) {
+  batch_loop(args, t, ctr, [&](const SyncArgs &a, const uint3 bid) { sync_periodic_body(a, bid); });
+}
+
+template <class T> int upload(const std::vector<T> &h, void **out) {
+  *out = nullptr;
+  if (h.empty())
+    return AXB_OK;
+  if (cudaMalloc(out, h.size() * sizeof(T)) != cudaSuccess)
+    return AXB_ERR_CUDA;
+  if (cudaMemcpy(*out, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice) !=
+      cudaSuccess)
+    return AXB_ERR_CUDA;
+  return AXB_OK;
+}
+
+} // namespace
+
+namespace axb {
+
+// Per-box stage and ghost-fill argument blocks of a batch, in device memory.
+int batch_rk_setup(int nbox, const axb_box *boxes, const axb_fields *f, const axb_fields *fn,
+                   void **stage_args, void **sync_evolved, void **sync_prims) {
+  static const int prims[12] = {AXB_GF_rho,   AXB_GF_velx, AXB_GF_vely,        AXB_GF_velz,
+                                AXB_GF_eps,   AXB_GF_press, AXB_GF_temperature, AXB_GF_Ye,
+                                AXB_GF_entropy, AXB_GF_Bvecx, AXB_GF_Bvecy,     AXB_GF_Bvecz};
+  std::vector<StageArgs> st(nbox);
+  std::vector<SyncArgs> se(nbox), sp(nbox);
+  for (int b = 0; b < nbox; ++b) {
+    const axb_box &box = boxes[b];
+    if (box.ng < 1)
+      return AXB_ERR_GHOSTS;
+    for (int d = 0; d < 3; ++d)
+      if (box.n[d] < box.ng)
+        return AXB_ERR_ARG;
+    StageArgs &a = st[b];
+    std::memset(&a, 0, sizeof a);
+    a.b = make_box(box);
+    for (int v = 0; v < NEVOLVED; ++v) {
+      a.out[v] = f[b].gf[kEvolved[v]];
+      a.un[v] = fn[b].gf[kEvolved[v]];
+      a.uk[v] = f[b].gf[kEvolved[v]];
+      a.rhs[v] = f[b].gf[kEvolvedRhs[v]];
+      if (!a.out[v] || !a.un[v] || !a.rhs[v])
+        return AXB_ERR_ARG;
+      for (int d = 0; d < 3; ++d)
+        a.cent[v][d] = kCent[v][d];
+    }
+    for (int pass = 0; pass < 2; ++pass) {
+      SyncArgs &y = pass ? sp[b] : se[b];
+      std::memset(&y, 0, sizeof y);
+      y.b = make_box(box);
+      const int nf = pass ? 12 : NEVOLVED;
+      y.nf = nf;
+      for (int q = 0; q < nf; ++q) {
+        const int id = pass ? prims[q] : kEvolved[q];
+        y.f[q] = f[b].gf[id];
+        if (!y.f[q])
+          return AXB_ERR_ARG;
+        centring_of(id, y.cent[q]);
+      }
+    }
+  }
+  int rc = upload(st, stage_args);
+  if (!rc)
+    rc = upload(se, sync_evolved);
+  if (!rc)
+    rc = upload(sp, sync_prims);
+  return rc;
+}
+
+// single-box grids of the stage update and the ghost fill of nf fields
+uint3 stage_grid(const axb_box &b) {
+  return make_uint3((b.n[0] + 1 + 127) / 128, b.n[1] + 1, b.n[2] + 1);
+}
+uint3 sync_grid(const axb_box &b, int nf) {
+  return make_uint3(b.n[1] + 2 * b.ng + 1, b.n[2] + 2 * b.ng + 1, nf);
+}
+
+int launch_stage_batch(const void *args, const TileTable &t, unsigned long long *ctr,
+                       double alpha, double beta, double gdt, int nblocks, cudaStream_t s) {
+  if (t.total == 0)
+    return AXB_OK;
+  k_rk_stage_batch<<<nblocks, 128, 0, s>>>(static_cast<const StageArgs *>(args), t, ctr,
+                                           alpha, beta, gdt);
+  return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+}
+
+int launch_sync_batch(const void *args, const TileTable &t, unsigned long long *ctr,
+                      int nblocks, cudaStream_t s) {
+  if (t.total == 0)
+    return AXB_OK;
+  k_sync_batch<<<nblocks, 128, 0, s>>>(static_cast<const SyncArgs *>(args), t, ctr);
+  return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+}
+
+} // namespace axb

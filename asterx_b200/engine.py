@@ -77,12 +77,20 @@ def load_library(path=LIB_PATH):
                                        C.c_float, C.c_float, _vp, _vp, _vp]
     lib.axb_c2p_cells.argtypes = [_vp, C.POINTER(abi.Cells), C.POINTER(Params), _vp, _vp,
                                   _vp]
+    lib.axb_batch_create.argtypes = [_vp, C.c_int, C.POINTER(Box), C.POINTER(Fields),
+                                     C.POINTER(Fields), C.POINTER(Params), _vp, C.POINTER(_vp)]
+    lib.axb_batch_destroy.argtypes = [_vp]
+    lib.axb_batch_substep.argtypes = [_vp, _vp, C.c_double, C.c_double, C.c_double,
+                                      C.c_double, C.c_int, _vp]
+    lib.axb_batch_autotune.argtypes = [_vp, _vp, C.POINTER(C.c_int), _vp]
     lib.axb_timing_begin.argtypes = [_vp]
     lib.axb_timing_end.argtypes = [_vp, C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_int]
     for name in ("axb_con2prim_group", "axb_substep", "axb_rk_stage",
                  "axb_sync_periodic", "axb_c2p_cells", "axb_eos_create_tabulated3d",
                  "axb_mlp_create", "axb_mlp_destroy", "axb_mlp_get_params",
-                 "axb_mlp_features", "axb_mlp_forward", "axb_mlp_train_step"):
+                 "axb_mlp_features", "axb_mlp_forward", "axb_mlp_train_step",
+                 "axb_batch_create", "axb_batch_destroy", "axb_batch_substep",
+                 "axb_batch_autotune"):
         if hasattr(lib, name):
             getattr(lib, name).restype = C.c_int
     return lib
@@ -103,6 +111,7 @@ class Engine:
         self._check(self.lib.axb_ctx_create(device, C.byref(self.ctx)), "axb_ctx_create")
         self._eos = []
         self._mlp = []
+        self._batches = []
 
     def _check(self, rc, what):
         if rc != 0:
@@ -289,7 +298,39 @@ class Engine:
             None if grad is None else grad.data_ptr(), self.stream_ptr(stream)),
             "axb_mlp_train_step")
 
+    # -- batched level --------------------------------------------------------
+    def batch_create(self, layouts, tensors, tensors_n, params: Params, eos):
+        """A batch over boxes (Layouts) with their device tensors (U_k) and the
+        U_n tensors of the evolved variables."""
+        n = len(layouts)
+        boxes = (Box * n)(*[L.box() for L in layouts])
+        fs = (Fields * n)(*[self.fields_struct(t) for t in tensors])
+        fns = (Fields * n)(*[self.fields_struct(t) for t in tensors_n])
+        h = _vp()
+        self._check(self.lib.axb_batch_create(self.ctx, n, boxes, fs, fns, C.byref(params),
+                                              eos, C.byref(h)), "axb_batch_create")
+        self._batches.append(h)
+        return h
+
+    def batch_substep(self, batch, alpha, beta, gamma, dt, periodic=True, stream=None):
+        self._check(self.lib.axb_batch_substep(self.ctx, batch, alpha, beta, gamma, dt,
+                                               int(periodic), self.stream_ptr(stream)),
+                    "axb_batch_substep")
+
+    def batch_autotune(self, batch, stream=None):
+        out = (C.c_int * 3)()
+        self._check(self.lib.axb_batch_autotune(self.ctx, batch, out, self.stream_ptr(stream)),
+                    "axb_batch_autotune")
+        return dict(seg_y=out[0], seg_z=out[1], ctas_per_sm=out[2])
+
+    def batch_destroy(self, batch):
+        self.lib.axb_batch_destroy(batch)
+        self._batches = [b for b in self._batches if b.value != batch.value]
+
     def close(self):
+        for h in self._batches:
+            self.lib.axb_batch_destroy(h)
+        self._batches = []
         for h in self._mlp:
             self.lib.axb_mlp_destroy(h)
         self._mlp = []

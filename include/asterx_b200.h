@@ -305,6 +305,41 @@ AXB_API int axb_substep(axb_ctx *ctx, const axb_box *box,
                         int periodic, void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* batched substep over the boxes of a refinement level                      */
+/* ------------------------------------------------------------------------ */
+
+/* A level of boxes advanced together.  CarpetX runs each scheduled routine
+ * of AsterX_RHSGroup and AsterX_Con2PrimGroup (AsterX/schedule.ccl:119-228)
+ * as one loop launch per box; a batch runs each phase of the substep as ONE
+ * persistent launch over the tiles of all its boxes, with results
+ * bit-identical to axb_substep on every box.  axb_batch_create checks every
+ * box as axb_rhs_group / axb_con2prim_group would, copies the per-box
+ * argument blocks and tile tables to the device (its only allocations), and
+ * keeps `eos` by reference: it must outlive the batch.  Field pointers are
+ * fixed at creation (U_k in fields[b], U_n in fields_n[b]). */
+typedef struct axb_batch axb_batch;
+AXB_API int axb_batch_create(axb_ctx *ctx, int nbox, const axb_box *boxes,
+                             const axb_fields *fields, const axb_fields *fields_n,
+                             const axb_params *params, const axb_eos *eos,
+                             axb_batch **out);
+AXB_API int axb_batch_destroy(axb_batch *batch);
+
+/* One RK substep of every box (axb_substep semantics), as 12 stream-ordered
+ * launches and one memset, allocation-free: a caller may capture it in a
+ * CUDA graph. */
+AXB_API int axb_batch_substep(axb_ctx *ctx, axb_batch *batch, double alpha,
+                              double beta, double gamma, double dt, int periodic,
+                              void *stream);
+
+/* Autotuner: times the RHS phases on the batch's own boxes for pencil
+ * segments {8, 16, 32, 64} of the y and z flux passes and persistent grids
+ * of {2, 4, 8, 16} CTAs per SM, and keeps the fastest.  Leaves the RHS grid
+ * functions as one RHS evaluation would.  Synchronous; not for use inside a
+ * stream capture.  out (may be NULL, 3 ints): y segment, z segment, CTAs per
+ * SM of the flux passes.  No counterpart in the reference. */
+AXB_API int axb_batch_autotune(axb_ctx *ctx, axb_batch *batch, int *out, void *stream);
+
+/* ------------------------------------------------------------------------ */
 /* independent-cell primitive recovery and the learned initial guess         */
 /* ------------------------------------------------------------------------ */
 
