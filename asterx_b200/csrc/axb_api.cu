@@ -560,6 +560,7 @@ int batch_rhs_setup(axb_ctx *c, int nbox, const axb_box *boxes, const axb_fields
     return AXB_ERR_ARG;
   for (int b = 0; b < nbox; ++b) {
     int rc = fill_rhs_args(c, boxes + b, f + b, p, h[b]);
+    h[b].b.packed = 1;
     if (!rc && eos->kind == 1 && !h[b].rec_temp)
       rc = AXB_ERR_UNSUPPORTED;
     if (rc) {
@@ -575,14 +576,12 @@ int batch_rhs_setup(axb_ctx *c, int nbox, const axb_box *boxes, const axb_fields
   return rc;
 }
 
-// single-box grids: 0 sources, 2 aux, 3 CT + Psi (as launch_rhs_misc)
+// batched grids over packed (i, j) planes: 0 sources, 2 aux, 3 CT + Psi
 uint3 rhs_misc_grid(int which, const axb_box &b) {
   const int T = 128;
-  if (which <= 1)
-    return make_uint3((b.n[0] + T - 1) / T, b.n[1], b.n[2]);
-  if (which == 2)
-    return make_uint3((b.n[0] + 5 + T - 1) / T, b.n[1] + 5, b.n[2] + 5);
-  return make_uint3((b.n[0] + 1 + T - 1) / T, b.n[1] + 1, b.n[2] + 1);
+  const int e = which <= 1 ? 0 : which == 2 ? 5 : 1;
+  const long long plane = (long long)(b.n[0] + e) * (b.n[1] + e);
+  return make_uint3(unsigned((plane + T - 1) / T), 1, b.n[2] + e);
 }
 
 int launch_rhs_misc_batch(int which, const void *args, const TileTable &t,
@@ -626,16 +625,17 @@ int launch_flux_batch(int recon, int dir, const RhsArgs *args, const TileTable &
   }
 }
 
-// single-box grid of a flux pass (as launch_flux_pass_eos; the x pass is a
-// 1-D grid of 4-warp blocks over the rows)
+// batched grid of a flux pass: the x pass as launch_flux_pass_eos (a 1-D
+// grid of 4-warp blocks over the rows), the y and z passes over the packed
+// transverse plane (128 pencils per block) times the segments along dir
 uint3 flux_grid(int dir, const axb_box &b, int seglen) {
   if (dir == 0) {
     const long long warps = (long long)(b.n[1] + 2) * (b.n[2] + 2);
     return make_uint3(unsigned((warps * 32 + 127) / 128), 1, 1);
   }
   const int T1 = dir == 2 ? 1 : 2;
-  return make_uint3((b.n[0] + 2 + 31) / 32, (b.n[T1] + 2 + 3) / 4,
-                    (b.n[dir] + seglen - 1) / seglen);
+  const long long plane = (long long)(b.n[0] + 2) * (b.n[T1] + 2);
+  return make_uint3(unsigned((plane + 127) / 128), 1, (b.n[dir] + seglen - 1) / seglen);
 }
 } // namespace axb
 

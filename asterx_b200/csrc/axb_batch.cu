@@ -32,7 +32,7 @@ int batch_rk_setup(int nbox, const axb_box *boxes, const axb_fields *f, const ax
 uint3 rhs_misc_grid(int which, const axb_box &b);
 uint3 flux_grid(int dir, const axb_box &b, int seglen);
 uint3 stage_grid(const axb_box &b);
-uint3 sync_grid(const axb_box &b, int nf);
+uint3 sync_grid(const axb_box &b, int set);
 uint3 c2p_grid(int which, const axb_box &b);
 int launch_rhs_misc_batch(int which, const void *args, const TileTable &t,
                           unsigned long long *ctr, int nblocks, cudaStream_t s);
@@ -135,7 +135,7 @@ uint3 g_aux(const axb_box &b, int) { return rhs_misc_grid(2, b); }
 uint3 g_ct(const axb_box &b, int) { return rhs_misc_grid(3, b); }
 uint3 g_flux(const axb_box &b, int dir_seg) { return flux_grid(dir_seg & 3, b, dir_seg >> 2); }
 uint3 g_stage(const axb_box &b, int) { return stage_grid(b); }
-uint3 g_sync(const axb_box &b, int nf) { return sync_grid(b, nf); }
+uint3 g_sync(const axb_box &b, int set) { return sync_grid(b, set); }
 uint3 g_c2p(const axb_box &b, int which) { return c2p_grid(which, b); }
 
 int nblocks_for(const axb_batch *B, int phase, long long total) {
@@ -255,13 +255,13 @@ AXB_API int axb_batch_create(axb_ctx *c, int nbox, const axb_box *boxes,
   if (!rc)
     rc = make_table(bx, g_stage, 0, B->tab[P_STAGE]);
   if (!rc)
-    rc = make_table(bx, g_sync, 11, B->tab[P_SYNC_E]);
+    rc = make_table(bx, g_sync, 0, B->tab[P_SYNC_E]);
   if (!rc)
     rc = make_table(bx, g_c2p, 0, B->tab[P_BSTAG]);
   if (!rc)
     rc = make_table(bx, g_c2p, 1, B->tab[P_C2P]);
   if (!rc)
-    rc = make_table(bx, g_sync, 12, B->tab[P_SYNC_P]);
+    rc = make_table(bx, g_sync, 1, B->tab[P_SYNC_P]);
   if (!rc && cudaMalloc(&B->ctr, NPHASE * sizeof(unsigned long long)) != cudaSuccess)
     rc = AXB_ERR_CUDA;
   if (rc) {

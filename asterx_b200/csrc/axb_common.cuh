@@ -15,6 +15,11 @@
 
 #define AXB_HD __host__ __device__ __forceinline__
 #define AXB_D __device__ __forceinline__
+#ifdef __CUDACC__
+#define AXB_D_ __device__ __forceinline__
+#else
+#define AXB_D_ inline
+#endif
 
 namespace axb {
 
@@ -25,6 +30,24 @@ struct BoxDev {
   long long sy, sz;
   double dx[3], idx[3];
   double xmin[3];
+  // 0: a block covers one row (block x along i, bid.y = j); 1 (batched
+  // launches over small boxes): the blocks of a k-plane cover its (i, j)
+  // points row after row, so short rows do not leave threads idle
+  int packed;
+
+  // the (i, j) of this thread for a range [li, li + ni) x [lj, lj + nj);
+  // false outside it
+  AXB_D_ bool row_ij(int li, int ni, int lj, int nj, const uint3 bid, int &i, int &j) const {
+    if (packed) {
+      const int flat = bid.x * blockDim.x + threadIdx.x;
+      i = li + flat % ni;
+      j = lj + flat / ni;
+      return flat < ni * nj;
+    }
+    i = li + bid.x * blockDim.x + threadIdx.x;
+    j = lj + bid.y;
+    return i < li + ni;
+  }
 
   AXB_HD long long at(int i, int j, int k) const {
     return (long long)i + sy * j + sz * k;
@@ -43,6 +66,7 @@ inline BoxDev make_box(const axb_box &b) {
   r.ng = b.ng;
   r.sy = b.sy;
   r.sz = b.sz;
+  r.packed = 0;
   return r;
 }
 

@@ -45,10 +45,9 @@ struct C2PBoxArgs {
 AXB_D void bstag_body(const C2PBoxArgs &a, const uint3 bid) {
   const BoxDev &b = a.b;
   const int ng = b.ng;
-  const int i = ng - 1 + bid.x * blockDim.x + threadIdx.x;
-  const int j = ng - 1 + bid.y;
+  int i, j;
   const int k = ng - 1 + bid.z;
-  if (i > ng + b.n[0])
+  if (!b.row_ij(ng - 1, b.n[0] + 2, ng - 1, b.n[1] + 2, bid, i, j))
     return;
   const long long I = b.at(i, j, k);
   const long long ipjk = I + 1, ijpk = I + b.sy, ijkp = I + b.sz;
@@ -126,12 +125,12 @@ AXB_D void c2p_box_body(const C2PBoxArgs &a, const EOS &eos, const uint3 bid) {
       s_hist[q] = 0;
     __syncthreads();
   }
-  const int i = b.ng + bid.x * blockDim.x + threadIdx.x;
-  const int j = b.ng + bid.y;
+  int i, j;
   const int k = b.ng + bid.z;
+  const bool in_range = b.row_ij(b.ng, b.n[0], b.ng, b.n[1], bid, i, j);
   int iters_first = -1;
   bool failed = false;
-  if (i < b.ng + b.n[0]) {
+  if (in_range) {
     const long long I = b.at(i, j, k);
     double dB[3];
     dB[0] = 0.5 * (a.dBstag[0][I] + a.dBstag[0][I + 1]);
@@ -537,6 +536,7 @@ int batch_c2p_setup(axb_ctx *c, int nbox, const axb_box *boxes, const axb_fields
     return AXB_ERR_ARG;
   for (int b = 0; b < nbox; ++b) {
     const int rc = fill_c2p_args(c, boxes + b, f + b, p, eos, h[b]);
+    h[b].b.packed = 1;
     if (rc) {
       delete[] h;
       return rc;
@@ -550,12 +550,12 @@ int batch_c2p_setup(axb_ctx *c, int nbox, const axb_box *boxes, const axb_fields
   return rc;
 }
 
-// single-box grids of the face curl (0) and the recovery (1)
+// batched grids over packed (i, j) planes: face curl (0), recovery (1)
 uint3 c2p_grid(int which, const axb_box &b) {
   const int T = 128;
-  if (which == 0)
-    return make_uint3((b.n[0] + 2 + T - 1) / T, b.n[1] + 2, b.n[2] + 2);
-  return make_uint3((b.n[0] + T - 1) / T, b.n[1], b.n[2]);
+  const int e = which == 0 ? 2 : 0;
+  const long long plane = (long long)(b.n[0] + e) * (b.n[1] + e);
+  return make_uint3(unsigned((plane + T - 1) / T), 1, b.n[2] + e);
 }
 
 int launch_c2p_batch(int which, const void *args, const TileTable &t,

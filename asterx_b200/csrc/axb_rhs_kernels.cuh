@@ -163,9 +163,21 @@ AXB_D void flux_pass_body(const RhsArgs &a, const EOS &eos, const int &seglen, c
   constexpr int T1 = (DIR == 2) ? 1 : 2;
   const BoxDev &b = a.b;
   const int ng = b.ng;
-  const int t0 = ng - 1 + bid.x * blockDim.x + threadIdx.x;
-  const int t1 = ng - 1 + bid.y * blockDim.y + threadIdx.y;
-  const bool active = (t0 <= ng + b.n[T0]) && (t1 <= ng + b.n[T1]);
+  int t0, t1;
+  bool active;
+  if (b.packed) {
+    // (batched small boxes) the block's threads walk the transverse plane
+    // [ng-1, ng+n]^2 row after row, so short rows leave no lane idle
+    const int w0 = b.n[T0] + 2;
+    const int flat = bid.x * (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x;
+    t0 = ng - 1 + flat % w0;
+    t1 = ng - 1 + flat / w0;
+    active = flat < w0 * (b.n[T1] + 2);
+  } else {
+    t0 = ng - 1 + bid.x * blockDim.x + threadIdx.x;
+    t1 = ng - 1 + bid.y * blockDim.y + threadIdx.y;
+    active = (t0 <= ng + b.n[T0]) && (t1 <= ng + b.n[T1]);
+  }
   double smax = 0.0;
   bool bad = false;
   if (active) {

@@ -91,10 +91,9 @@ AXB_HD double sym_get(const sym3 &m, int p, int q) { return m(p, q); }
 template <int FD>
 AXB_D void sources_body(const RhsArgs &a, const uint3 bid) {
   const BoxDev &b = a.b;
-  const int i = b.ng + bid.x * blockDim.x + threadIdx.x;
-  const int j = b.ng + bid.y;
+  int i, j;
   const int k = b.ng + bid.z;
-  if (i >= b.ng + b.n[0])
+  if (!b.row_ij(b.ng, b.n[0], b.ng, b.n[1], bid, i, j))
     return;
   const long long I = b.at(i, j, k);
   const long long sy = b.sy, sz = b.sz;
@@ -234,10 +233,9 @@ __global__ void __launch_bounds__(128, AXB_SOURCES_MINB)
 // ---------------------------------------------------------------------------
 AXB_D void aux_body(const RhsArgs &a, const uint3 bid) {
   const BoxDev &b = a.b;
-  const int i = b.ng - 2 + bid.x * blockDim.x + threadIdx.x;
-  const int j = b.ng - 2 + bid.y;
+  int i, j;
   const int k = b.ng - 2 + bid.z;
-  if (i > b.ng + b.n[0] + 2)
+  if (!b.row_ij(b.ng - 2, b.n[0] + 5, b.ng - 2, b.n[1] + 5, bid, i, j))
     return;
   const long long I = b.at(i, j, k);
   double Av[3];
@@ -277,10 +275,9 @@ __global__ void __launch_bounds__(128)
 AXB_D void ct_psi_body(const RhsArgs &a, const uint3 bid) {
   const BoxDev &b = a.b;
   const int ng = b.ng;
-  const int i = ng + bid.x * blockDim.x + threadIdx.x;
-  const int j = ng + bid.y;
+  int i, j;
   const int k = ng + bid.z;
-  if (i > ng + b.n[0])
+  if (!b.row_ij(ng, b.n[0] + 1, ng, b.n[1] + 1, bid, i, j))
     return;
   const long long I = b.at(i, j, k);
   const int ijk[3] = {i, j, k};

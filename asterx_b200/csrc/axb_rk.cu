@@ -1,5 +1,6 @@
 // Runge-Kutta stage update of the evolved variables and the periodic ghost
 // fill of one box (the single-box form of the driver's SYNC).
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -36,10 +37,9 @@ struct StageArgs {
 AXB_D void rk_stage_body(const StageArgs &a, double alpha, double beta, double gdt,
                          const uint3 bid) {
   const BoxDev &b = a.b;
-  const int i = b.ng + bid.x * blockDim.x + threadIdx.x;
-  const int j = b.ng + bid.y;
+  int i, j;
   const int k = b.ng + bid.z;
-  if (i > b.ng + b.n[0])
+  if (!b.row_ij(b.ng, b.n[0] + 1, b.ng, b.n[1] + 1, bid, i, j))
     return;
   const long long I = b.at(i, j, k);
   const int ijk[3] = {i, j, k};
@@ -201,9 +201,75 @@ __global__ void __launch_bounds__(128)
   });
 }
 
+// Periodic ghost fill enumerating only the ghost points: for small boxes
+// most points of a row are interior, so one thread per ghost point (slab
+// below, slab above, then the ghost rows and row ends of the middle planes)
+// keeps the threads busy.  Same points, same images as sync_periodic_body.
+struct Shell {
+  long long A, B, Cm, G;
+  int N[3], hi[3], ng;
+  AXB_HD Shell(const BoxDev &b, const int c[3]) {
+    ng = b.ng;
+    for (int d = 0; d < 3; ++d) {
+      N[d] = b.n[d] + 2 * ng + (c[d] ? 0 : 1);
+      hi[d] = ng + b.n[d] + (c[d] ? 0 : 1);
+    }
+    const long long plane = (long long)N[0] * N[1];
+    A = ng * plane;
+    B = (long long)(N[2] - hi[2]) * plane;
+    Cm = (long long)(ng + N[1] - hi[1]) * N[0] + (long long)(hi[1] - ng) * (ng + N[0] - hi[0]);
+    G = A + B + (long long)(hi[2] - ng) * Cm;
+  }
+  AXB_HD void point(long long g, int &i, int &j, int &k) const {
+    const long long plane = (long long)N[0] * N[1];
+    if (g < A + B) {
+      k = g < A ? int(g / plane) : hi[2] + int((g - A) / plane);
+      const long long r = g < A ? g % plane : (g - A) % plane;
+      j = int(r / N[0]);
+      i = int(r % N[0]);
+      return;
+    }
+    g -= A + B;
+    k = ng + int(g / Cm);
+    long long r = g % Cm;
+    const long long lowrows = (long long)ng * N[0], highrows = (long long)(N[1] - hi[1]) * N[0];
+    if (r < lowrows) {
+      j = int(r / N[0]);
+      i = int(r % N[0]);
+    } else if (r < lowrows + highrows) {
+      r -= lowrows;
+      j = hi[1] + int(r / N[0]);
+      i = int(r % N[0]);
+    } else {
+      r -= lowrows + highrows;
+      const int per = ng + N[0] - hi[0];
+      j = ng + int(r / per);
+      const int q = int(r % per);
+      i = q < ng ? q : hi[0] + (q - ng);
+    }
+  }
+};
+
+AXB_D void sync_shell_body(const SyncArgs &a, const uint3 bid) {
+  const BoxDev &b = a.b;
+  const int v = bid.z;
+  const Shell sh(b, a.cent[v]);
+  const long long g = (long long)bid.x * blockDim.x + threadIdx.x;
+  if (g >= sh.G)
+    return;
+  int i, j, k;
+  sh.point(g, i, j, k);
+  const int ng = b.ng;
+  const int is = (i >= ng && i < sh.hi[0]) ? i : wrap(i, ng, b.n[0]);
+  const int js = (j >= ng && j < sh.hi[1]) ? j : wrap(j, ng, b.n[1]);
+  const int ks = (k >= ng && k < sh.hi[2]) ? k : wrap(k, ng, b.n[2]);
+  double *f = a.f[v];
+  f[b.at(i, j, k)] = f[b.at(is, js, ks)];
+}
+
 __global__ void __launch_bounds__(128)
     k_sync_batch(const SyncArgs *args, const TileTable t, unsigned long long *ctr) {
-  batch_loop(args, t, ctr, [&](const SyncArgs &a, const uint3 bid) { sync_periodic_body(a, bid); });
+  batch_loop(args, t, ctr, [&](const SyncArgs &a, const uint3 bid) { sync_shell_body(a, bid); });
 }
 
 template <class T> int upload(const std::vector<T> &h, void **out) {
@@ -240,6 +306,7 @@ int batch_rk_setup(int nbox, const axb_box *boxes, const axb_fields *f, const ax
     StageArgs &a = st[b];
     std::memset(&a, 0, sizeof a);
     a.b = make_box(box);
+    a.b.packed = 1;
     for (int v = 0; v < NEVOLVED; ++v) {
       a.out[v] = f[b].gf[kEvolved[v]];
       a.un[v] = fn[b].gf[kEvolved[v]];
@@ -273,12 +340,26 @@ int batch_rk_setup(int nbox, const axb_box *boxes, const axb_fields *f, const ax
   return rc;
 }
 
-// single-box grids of the stage update and the ghost fill of nf fields
+// batched grids: the stage update over packed (i, j) planes, and the ghost
+// fill over the ghost points of the largest centring of the set (0: the 11
+// evolved variables, 1: the 12 cell-centred primitives)
 uint3 stage_grid(const axb_box &b) {
-  return make_uint3((b.n[0] + 1 + 127) / 128, b.n[1] + 1, b.n[2] + 1);
+  const long long plane = (long long)(b.n[0] + 1) * (b.n[1] + 1);
+  return make_uint3(unsigned((plane + 127) / 128), 1, b.n[2] + 1);
 }
-uint3 sync_grid(const axb_box &b, int nf) {
-  return make_uint3(b.n[1] + 2 * b.ng + 1, b.n[2] + 2 * b.ng + 1, nf);
+uint3 sync_grid(const axb_box &b, int set) {
+  const BoxDev bd = make_box(b);
+  long long g = 0;
+  const int nf = set ? 12 : NEVOLVED;
+  for (int q = 0; q < nf; ++q) {
+    int c[3] = {1, 1, 1};
+    if (!set)
+      for (int d = 0; d < 3; ++d)
+        c[d] = kCent[q][d];
+    const Shell sh(bd, c);
+    g = std::max(g, sh.G);
+  }
+  return make_uint3(unsigned((g + 127) / 128), 1, nf);
 }
 
 int launch_stage_batch(const void *args, const TileTable &t, unsigned long long *ctr,

@@ -66,10 +66,12 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the reference baseline sample")
-    ap.add_argument("--workload", default="substep", choices=["substep", "c2p"],
+    ap.add_argument("--workload", default="substep", choices=["substep", "c2p", "amr"],
                     help="substep: the RK3 substep of one box (the headline); "
                          "c2p: the independent-cell recovery microbenchmark, "
-                         "plain seeds vs the learned guess")
+                         "plain seeds vs the learned guess; amr: a level of boxes of "
+                         "uneven sizes, batched + CUDA graph vs one launch per box")
+    ap.add_argument("--boxes", type=int, default=512, help="boxes of the amr workload")
     ap.add_argument("--cells", type=int, default=1 << 26,
                     help="cells of the recovery microbenchmark")
     ap.add_argument("--train-pairs", type=int, default=1 << 24)
@@ -559,12 +561,164 @@ def c2p_bench(args):
     return 0
 
 
+def amr_bench(args):
+    """Batched AMR level: `boxes` boxes (512) with interior edges drawn
+    log-uniformly from 16 to 64 per axis, 3 ghosts, the curved-metric physics
+    of the 256^3 workload (WENO-Z + HLLE, Palenzuela with Noble backup,
+    Gamma 4/3), each box periodic on itself.  Times SSP-RK3 substeps done
+    (a) as one axb_substep per box (each phase launched once per box, as the
+    reference's driver does) and (b) as axb_batch_substep (one persistent
+    launch per phase over all boxes, tuned by the autotuner) replayed from a
+    CUDA graph holding one full RK3 step.  U_n of the evolved variables lives
+    in one arena, so its copy at the start of each RK3 step is one copy."""
+    import math
+
+    import numpy as np
+    import torch
+
+    from asterx_b200 import abi
+    from asterx_b200 import workloads as W
+    from asterx_b200.engine import Engine
+
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    eng = Engine(0)
+    xp = W._XP(torch, dev)
+    rng = np.random.default_rng(33)
+    shapes = [tuple(int(round(math.exp(rng.uniform(math.log(16), math.log(64)))))
+                    for _ in range(3)) for _ in range(args.boxes)]
+    evolved = abi.CONS + ["Avec_x", "Avec_y", "Avec_z", "Psi"]
+    skip = {"zvec_x", "zvec_y", "zvec_z", "svec_x", "svec_y", "svec_z", "dBx", "dBy", "dBz"}
+    layouts, fields = [], []
+    for b, n in enumerate(shapes):
+        L, f = W.curved_box(n=n, ng=3, seed=1000 + b, wmax=10.0, xp=xp)
+        W.cons_from_prims(L, f, xp=xp)
+        W.saved_from_prims(f, xp=xp)
+        for name in abi.GF_NAMES:
+            if name not in f and name not in skip:
+                f[name] = torch.zeros(L.size, dtype=torch.float64, device=dev)
+        layouts.append(L)
+        fields.append(f)
+    # evolved variables and their U_n copies as views of two arenas
+    sizes = [L.size for L in layouts]
+    total = sum(sizes) * len(evolved)
+    arena = torch.empty(total, dtype=torch.float64, device=dev)
+    arena_n = torch.empty(total, dtype=torch.float64, device=dev)
+    fields_n = []
+    off = 0
+    for L, f in zip(layouts, fields):
+        fn = {}
+        for k in evolved:
+            v = arena[off:off + L.size]
+            v.copy_(f[k])
+            f[k] = v
+            fn[k] = arena_n[off:off + L.size]
+            off += L.size
+        fields_n.append(fn)
+    zones = sum(n[0] * n[1] * n[2] for n in shapes)
+    params = abi.default_params(reconstruction_method=args.recon, flux_type="hlle",
+                                c2p_prime="palenzuela", c2p_second="noble")
+    eos = eng.eos_idealgas(GAMMA, **EOS_KW)
+    dt = 0.25 / 64
+    stream = torch.cuda.current_stream(dev)
+    # keep a pristine copy so both modes start from the same state
+    pristine = arena.clone()
+
+    def per_box_step():
+        arena_n.copy_(arena)
+        for a_, b_, g_ in SSPRK3:
+            for L, f, fn in zip(layouts, fields, fields_n):
+                eng.substep(L, f, fn, params, eos, a_, b_, g_, dt, periodic=True)
+
+    batch = eng.batch_create(layouts, fields, fields_n, params, eos)
+
+    def batched_step():
+        arena_n.copy_(arena)
+        for a_, b_, g_ in SSPRK3:
+            eng.batch_substep(batch, a_, b_, g_, dt, periodic=True)
+
+    def timed(fn, nsteps):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(nsteps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    nrk = max(1, args.steps // 3)  # timed RK3 steps (3 substeps each)
+    # (a) one launch per box and phase
+    for _ in range(max(1, args.warmup // 3)):
+        per_box_step()
+    t0 = time.perf_counter()
+    ms_a = timed(per_box_step, nrk)
+    wall_a = time.perf_counter() - t0
+    # (b) batched, tuned, replayed from a CUDA graph
+    arena.copy_(pristine)
+    tuning = eng.batch_autotune(batch)
+    for _ in range(max(1, args.warmup // 3)):
+        batched_step()
+    ms_b_nograph = timed(batched_step, nrk)
+    graph = torch.cuda.CUDAGraph()
+    torch.cuda.synchronize()
+    with torch.cuda.graph(graph):
+        batched_step()
+    graph.replay()
+    torch.cuda.synchronize()
+    eng.status_reset()
+    sampler = ClockSampler(0)
+    sampler.start()
+    ms_b = timed(graph.replay, nrk)
+    clocks = sampler.stop()
+    st = eng.status()
+    # one substep traced per kernel region (outside the graph)
+    eng.timing_begin()
+    eng.batch_substep(batch, *SSPRK3[1], dt, periodic=True)
+    region_ms, region_n = eng.timing_end(len(REGIONS))
+    sub = 3 * nrk
+    v_b = zones * sub / (ms_b / 1e3)
+    v_a = zones * sub / (ms_a / 1e3)
+    line = {
+        "metric": "Zone-updates/s per RK3 substep (batched AMR level)", "value": v_b,
+        "unit": UNIT, "n_gpus": 1, "steps": sub, "warmup": args.warmup,
+        "ms_per_step": ms_b / sub, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded boxes of the level)",
+        "config": {"workload": f"{args.boxes} boxes, edges log-uniform in [16, 64] per axis, "
+                               f"3 ghosts, curved metric, {args.recon}+HLLE, Palenzuela c2p, "
+                               "Gamma=4/3, SSP-RK3; batched persistent launches in a CUDA "
+                               "graph vs one launch per box",
+                   "boxes": args.boxes, "zones": zones, "recon": args.recon,
+                   "l2": "level data far larger than L2"},
+        "per_box_launch": {"value": v_a, "ms_per_step": ms_a / sub,
+                           "host_wall_s": wall_a, "launches_per_substep": 11 * args.boxes},
+        "batched_no_graph": {"value": zones * sub / (ms_b_nograph / 1e3),
+                             "ms_per_step": ms_b_nograph / sub},
+        "speedup_batched_graph_vs_per_box": v_b / v_a,
+        "autotune": tuning,
+        "kernels_ms_per_substep": {REGIONS[i]: region_ms[i] for i in range(len(REGIONS))
+                                   if region_n[i]},
+        "gpu_launches": int(sum(region_n)) * sub,
+        "clocks": clocks,
+        "error_word": st["error_word"], "c2p_fail_cells": st["c2p_fail"],
+    }
+    print(json.dumps(line), flush=True)
+    del graph
+    eng.close()
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return reference_arm(args)
     if args.workload == "c2p":
         return c2p_bench(args)
+    if args.workload == "amr":
+        return amr_bench(args)
     return ours(args)
 
 
