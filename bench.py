@@ -72,6 +72,11 @@ def parse_args():
                          "plain seeds vs the learned guess; amr: a level of boxes of "
                          "uneven sizes, batched + CUDA graph vs one launch per box")
     ap.add_argument("--boxes", type=int, default=512, help="boxes of the amr workload")
+    ap.add_argument("--decomp", default="boxes", choices=["boxes", "slab"],
+                    help="with several GPUs: boxes = one independent periodic box per rank "
+                         "(no data-path collective); slab = the ranks' boxes are z-slabs of "
+                         "one periodic patch, with a ghost-plane exchange (NCCL send/recv) "
+                         "after each ghost fill")
     ap.add_argument("--cells", type=int, default=1 << 26,
                     help="cells of the recovery microbenchmark")
     ap.add_argument("--train-pairs", type=int, default=1 << 24)
@@ -299,12 +304,21 @@ def ours(args):
     zones = args.n ** 3
     stream = torch.cuda.current_stream(dev)
 
+    halo = None
+    if world > 1 and args.decomp == "slab":
+        from asterx_b200.distribute import SlabHalo
+        halo = SlabHalo(L, rank, world)
+
     def substep(s):
         a_, b_, g_ = SSPRK3[s % 3]
         if s % 3 == 0:
             for k in evolved:
                 fn[k].copy_(f[k])
-        eng.substep(L, f, fn, params, eos, a_, b_, g_, dt, periodic=True)
+        if halo is None:
+            eng.substep(L, f, fn, params, eos, a_, b_, g_, dt, periodic=True)
+        else:
+            from asterx_b200.distribute import slab_substep
+            slab_substep(eng, L, f, fn, params, eos, a_, b_, g_, dt, halo)
 
     for s in range(args.warmup):
         substep(s)
@@ -407,7 +421,8 @@ def ours(args):
                                    f"metric, {args.recon}+HLLE, flux-CT, Palenzuela c2p "
                                    f"(Noble backup), ideal gas Gamma=4/3, SSP-RK3 substeps",
                        "box": [args.n] * 3, "ghosts": 3, "recon": args.recon,
-                       "parallelism": f"one box per GPU x{world}",
+                       "parallelism": (f"one box per GPU x{world}" if halo is None else
+                                       f"z-slabs of one patch, halo exchange x{world}"),
                        "l2": "inputs larger than L2 (146 MB per field)"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved,
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
