@@ -575,8 +575,10 @@ AXB_HD void brent_bracket(const F &f, double a, double b, int minbits,
     ++iters;
     double s;
     if (fa != fc && fb != fc) {
-      s = a * fb * fc / ((fa - fb) * (fa - fc)) + b * fa * fc / ((fb - fa) * (fb - fc)) +
-          c * fa * fb / ((fc - fa) * (fc - fb));
+      // inverse quadratic interpolation over one common denominator
+      // (fa-fb)(fa-fc)(fb-fc) instead of three (last-ulp differences)
+      const double dab = fa - fb, dac = fa - fc, dbc = fb - fc;
+      s = (a * fb * fc * dbc - b * fa * fc * dac + c * fa * fb * dab) / (dab * dac * dbc);
     } else {
       s = b - fb * (b - a) / (fb - fa);
     }
@@ -623,21 +625,23 @@ struct PalQRST {
 
 // Root function of the Palenzuela scheme (c2p_1DPalenzuela.hxx:264-303).
 // W^-2 is clamped as in the reference; W = (W^-2)^(-1/2) is taken as
-// 1/sqrt instead of pow, and the divisions by W become products with its
-// square root (last-ulp differences; the bracket search converges to the
-// same tolerance).
+// 1/sqrt instead of pow, the divisions by W become products with its square
+// root, and 1/x and 1/(x (x+s)) come from one division (last-ulp
+// differences; the bracket search converges to the same tolerance).
 template <class EOS>
 AXB_HD double pal_froot(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
                         const PalQRST &k, double x, const Cons &cv) {
   const double xs = x + k.s;
-  double Wminus2 = 1.0 - (x * x * k.r + (2.0 * x + k.s) * k.t * k.t) / (x * x * xs * xs);
+  const double ixxs = 1.0 / (x * xs); // 1/(x (x+s)); 1/x = (x+s)/(x (x+s))
+  const double ix = xs * ixxs;
+  double Wminus2 = 1.0 - (x * x * k.r + (2.0 * x + k.s) * k.t * k.t) * (ixxs * ixxs);
   Wminus2 = fmin(fmax(Wminus2, 1e-10), 1);
   const double iW = sqrt(Wminus2);
   const double W_loc = 1.0 / iW;
   const double rho_loc = cv.dens * iW;
   const double Ye_loc = k.ye;
   double eps_loc = W_loc - 1.0 + (1.0 - W_loc * W_loc) * x * iW +
-                   W_loc * (k.q - k.s + k.t * k.t / (2 * x * x) + 0.5 * k.s * Wminus2);
+                   W_loc * (k.q - k.s + 0.5 * k.t * k.t * (ix * ix) + 0.5 * k.s * Wminus2);
   if (cp.use_temp) {
     eps_loc = fmax(eps_loc, atmo.eps);
     eps_loc = fmin(eps_loc, eos.rgeps.max);

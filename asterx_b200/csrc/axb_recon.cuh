@@ -128,10 +128,13 @@ AXB_HD CellLoUp recon_ppm(const double q[5], const double pr[5],
 }
 
 AXB_HD CellLoUp recon_wenoz(const double q[5], double weno_eps) {
-  // Same weights and candidate stencils as the reference; the divisions by
-  // the weight sums and by 6 are folded into one reciprocal per side, which
-  // changes results only at the last-ulp level (5 FP64 divisions per cell
-  // instead of 15).
+  // Same weights and candidate stencils as the reference, with its divisions
+  // regrouped: 1 + tau5 / (beta_k + eps) for the three k share one
+  // reciprocal of the product of the three denominators, and both weight
+  // normalisations (and the 1/6 of the stencils) share one reciprocal of
+  // the product of the two sums -- 2 FP64 divisions per cell instead of 15,
+  // last-ulp differences.  The products stay far from overflow for
+  // |values| < 1e50 (beta ~ value^2, eps = 1e-26 bounds them below).
   const double a = q[0], b = q[1], c = q[2], d = q[3], e = q[4];
   const double beta0 = (13.0 / 12.0) * sq(a - 2.0 * b + c) +
                        (1.0 / 4.0) * sq(a - 4.0 * b + 3.0 * c);
@@ -140,15 +143,18 @@ AXB_HD CellLoUp recon_wenoz(const double q[5], double weno_eps) {
   const double beta2 = (13.0 / 12.0) * sq(c - 2.0 * d + e) +
                        (1.0 / 4.0) * sq(3.0 * c - 4.0 * d + e);
   const double tau5 = fabs(beta0 - beta2);
-  const double aux0 = 1.0 + tau5 / (beta0 + weno_eps);
-  const double aux1 = 1.0 + tau5 / (beta1 + weno_eps);
-  const double aux2 = 1.0 + tau5 / (beta2 + weno_eps);
+  const double d0 = beta0 + weno_eps, d1 = beta1 + weno_eps, d2 = beta2 + weno_eps;
+  const double r = tau5 / (d0 * d1 * d2);
+  const double aux0 = 1.0 + r * (d1 * d2);
+  const double aux1 = 1.0 + r * (d0 * d2);
+  const double aux2 = 1.0 + r * (d0 * d1);
   const double w0 = 3.0 / 10.0, w1 = 3.0 / 5.0, w2 = 1.0 / 10.0;
   // minus side (lower value): weights w0, w1, w2; plus side: w2, w1, w0
   const double am0 = w0 * aux0, am1 = w1 * aux1, am2 = w2 * aux2;
   const double ap0 = w2 * aux0, ap1 = w1 * aux1, ap2 = w0 * aux2;
-  const double idm6 = 1.0 / (6.0 * (am0 + am1 + am2));
-  const double idp6 = 1.0 / (6.0 * (ap0 + ap1 + ap2));
+  const double sm = am0 + am1 + am2, sp = ap0 + ap1 + ap2;
+  const double rr = 1.0 / (6.0 * sm * sp);
+  const double idm6 = sp * rr, idp6 = sm * rr;
   const double var_m = (am2 * (2.0 * e - 7.0 * d + 11.0 * c) +
                         am1 * (-1.0 * d + 5.0 * c + 2.0 * b) +
                         am0 * (2.0 * c + 5.0 * b - 1.0 * a)) *

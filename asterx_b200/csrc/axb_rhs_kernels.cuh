@@ -144,6 +144,9 @@ AXB_D void flux_status(const RhsArgs &a, double smax, bool bad) {
 #ifndef AXB_FLUX_X_MINB
 #define AXB_FLUX_X_MINB 4
 #endif
+#ifndef AXB_FLUX_SMEM_CARRY
+#define AXB_FLUX_SMEM_CARRY 1
+#endif
 
 // ---------------------------------------------------------------------------
 // k_flux_pass (y and z): one thread marches one pencil segment along DIR.
@@ -195,8 +198,21 @@ AXB_D void flux_pass_body(const RhsArgs &a, const EOS &eos, const int &seglen, c
                                      a.vel[0], a.vel[1],  a.vel[2],   a.Bvec[D1],
                                      a.Bvec[D2]};
     const double idxd = b.idx[DIR];
+#if AXB_FLUX_SMEM_CARRY
+    // the state carried from one cell to the next (upper interface values
+    // of the previous cell, flux of the previous face) lives in shared
+    // memory: in registers it pushed the march beyond its register budget
+    // and into local-memory spills
+    __shared__ double s_carry[NREC + NHYDRO][128];
+    const int tl = threadIdx.y * blockDim.x + threadIdx.x;
+#define AXB_UPL(v) s_carry[v][tl]
+#define AXB_FPREV(v) s_carry[NREC + (v)][tl]
+#else
     double upL[NREC];
     double Fprev[NHYDRO];
+#define AXB_UPL(v) upL[v]
+#define AXB_FPREV(v) Fprev[v]
+#endif
     for (int c = f0 - 1; c <= flast; ++c, I += sd) {
       double lo[NREC], up[NREC];
       recon_cell_all<DIR, RECON>(a, fld, I, sd, lo, up);
@@ -205,25 +221,29 @@ AXB_D void flux_pass_body(const RhsArgs &a, const EOS &eos, const int &seglen, c
         double L[NREC], R[NREC], F[10];
 #pragma unroll
         for (int v = 0; v < NREC; ++v) {
-          L[v] = upL[v];
+          L[v] = AXB_UPL(v);
           R[v] = lo[v];
         }
         face_fluxes<DIR>(a, eos, fld, I, sd, L, R, F, smax, bad);
         if (c > f0 && trans_int) {
-          double Fc[NHYDRO];
+          double Fc[NHYDRO], Fp[NHYDRO];
 #pragma unroll
-          for (int v = 0; v < NHYDRO; ++v)
+          for (int v = 0; v < NHYDRO; ++v) {
             Fc[v] = F[v];
-          fold_divergence<DIR>(a, I - sd, idxd, Fc, Fprev);
+            Fp[v] = AXB_FPREV(v);
+          }
+          fold_divergence<DIR>(a, I - sd, idxd, Fc, Fp);
         }
 #pragma unroll
         for (int v = 0; v < NHYDRO; ++v)
-          Fprev[v] = F[v];
+          AXB_FPREV(v) = F[v];
       }
 #pragma unroll
       for (int v = 0; v < NREC; ++v)
-        upL[v] = up[v];
+        AXB_UPL(v) = up[v];
     }
+#undef AXB_UPL
+#undef AXB_FPREV
   }
   flux_status(a, smax, bad);
 }
