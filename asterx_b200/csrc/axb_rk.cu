@@ -73,35 +73,73 @@ AXB_D int wrap(int i, int ng, int n) {
 }
 
 // Periodic ghost fill: every point outside the interior of its centring
-// takes the value of its periodic image inside the interior.  One block
-// handles one (j, k) row of one field.
-AXB_D void sync_periodic_body(const SyncArgs &a, const uint3 bid) {
+// takes the value of its periodic image inside the interior.  One thread per
+// ghost point, enumerated slab below, slab above, then the ghost rows and
+// row ends of the middle planes, so no thread idles on interior points.
+struct Shell {
+  long long A, B, Cm, G;
+  int N[3], hi[3], ng;
+  AXB_HD Shell(const BoxDev &b, const int c[3]) {
+    ng = b.ng;
+    for (int d = 0; d < 3; ++d) {
+      N[d] = b.n[d] + 2 * ng + (c[d] ? 0 : 1);
+      hi[d] = ng + b.n[d] + (c[d] ? 0 : 1);
+    }
+    const long long plane = (long long)N[0] * N[1];
+    A = ng * plane;
+    B = (long long)(N[2] - hi[2]) * plane;
+    Cm = (long long)(ng + N[1] - hi[1]) * N[0] + (long long)(hi[1] - ng) * (ng + N[0] - hi[0]);
+    G = A + B + (long long)(hi[2] - ng) * Cm;
+  }
+  AXB_HD void point(long long g, int &i, int &j, int &k) const {
+    const long long plane = (long long)N[0] * N[1];
+    if (g < A + B) {
+      k = g < A ? int(g / plane) : hi[2] + int((g - A) / plane);
+      const long long r = g < A ? g % plane : (g - A) % plane;
+      j = int(r / N[0]);
+      i = int(r % N[0]);
+      return;
+    }
+    g -= A + B;
+    k = ng + int(g / Cm);
+    long long r = g % Cm;
+    const long long lowrows = (long long)ng * N[0], highrows = (long long)(N[1] - hi[1]) * N[0];
+    if (r < lowrows) {
+      j = int(r / N[0]);
+      i = int(r % N[0]);
+    } else if (r < lowrows + highrows) {
+      r -= lowrows;
+      j = hi[1] + int(r / N[0]);
+      i = int(r % N[0]);
+    } else {
+      r -= lowrows + highrows;
+      const int per = ng + N[0] - hi[0];
+      j = ng + int(r / per);
+      const int q = int(r % per);
+      i = q < ng ? q : hi[0] + (q - ng);
+    }
+  }
+};
+
+AXB_D void sync_shell_body(const SyncArgs &a, const uint3 bid) {
   const BoxDev &b = a.b;
   const int v = bid.z;
-  const int j = bid.x;
-  const int k = bid.y;
-  double *f = a.f[v];
-  const int *c = a.cent[v];
-  const int ng = b.ng;
-  const int hi[3] = {ng + b.n[0] + (c[0] ? 0 : 1), ng + b.n[1] + (c[1] ? 0 : 1),
-                     ng + b.n[2] + (c[2] ? 0 : 1)};
-  const int npts0 = b.n[0] + 2 * ng + (c[0] ? 0 : 1);
-  const bool row_in = j >= ng && j < hi[1] && k >= ng && k < hi[2];
-  const int js = (j >= ng && j < hi[1]) ? j : wrap(j, ng, b.n[1]);
-  const int ks = (k >= ng && k < hi[2]) ? k : wrap(k, ng, b.n[2]);
-  if (j >= b.n[1] + 2 * ng + (c[1] ? 0 : 1) || k >= b.n[2] + 2 * ng + (c[2] ? 0 : 1))
+  const Shell sh(b, a.cent[v]);
+  const long long g = (long long)bid.x * blockDim.x + threadIdx.x;
+  if (g >= sh.G)
     return;
-  for (int i = threadIdx.x; i < npts0; i += blockDim.x) {
-    const bool i_in = i >= ng && i < hi[0];
-    if (row_in && i_in)
-      continue;
-    const int is = i_in ? i : wrap(i, ng, b.n[0]);
-    f[b.at(i, j, k)] = f[b.at(is, js, ks)];
-  }
+  int i, j, k;
+  sh.point(g, i, j, k);
+  const int ng = b.ng;
+  const int is = (i >= ng && i < sh.hi[0]) ? i : wrap(i, ng, b.n[0]);
+  const int js = (j >= ng && j < sh.hi[1]) ? j : wrap(j, ng, b.n[1]);
+  const int ks = (k >= ng && k < sh.hi[2]) ? k : wrap(k, ng, b.n[2]);
+  double *f = a.f[v];
+  f[b.at(i, j, k)] = f[b.at(is, js, ks)];
 }
-__global__ void __launch_bounds__(128)
-    k_sync_periodic(const SyncArgs a) {
-  sync_periodic_body(a, blockIdx);
+
+__global__ void __launch_bounds__(128) k_sync_shell(const SyncArgs a) {
+  sync_shell_body(a, blockIdx);
 }
 
 int centring_of(int gf, int c[3]) {
@@ -181,9 +219,13 @@ AXB_API int axb_sync_periodic(axb_ctx *c, const axb_box *box,
     a.f[q] = f->gf[ids[q]];
     centring_of(ids[q], a.cent[q]);
   }
-  const dim3 grid(box->n[1] + 2 * box->ng + 1, box->n[2] + 2 * box->ng + 1, nids);
+  // one thread per ghost point of the largest centring among the fields
+  long long gmax = 0;
+  for (int q = 0; q < nids; ++q)
+    gmax = std::max(gmax, Shell(a.b, a.cent[q]).G);
+  const dim3 grid(unsigned((gmax + 127) / 128), 1, nids);
   axb_mark(c, AXB_R_SYNC, (cudaStream_t)stream, true);
-  k_sync_periodic<<<grid, 128, 0, (cudaStream_t)stream>>>(a);
+  k_sync_shell<<<grid, 128, 0, (cudaStream_t)stream>>>(a);
   axb_mark(c, AXB_R_SYNC, (cudaStream_t)stream, false);
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
 }
@@ -199,72 +241,6 @@ __global__ void __launch_bounds__(128)
   batch_loop(args, t, ctr, [&](const StageArgs &a, const uint3 bid) {
     rk_stage_body(a, alpha, beta, gdt, bid);
   });
-}
-
-// Periodic ghost fill enumerating only the ghost points: for small boxes
-// most points of a row are interior, so one thread per ghost point (slab
-// below, slab above, then the ghost rows and row ends of the middle planes)
-// keeps the threads busy.  Same points, same images as sync_periodic_body.
-struct Shell {
-  long long A, B, Cm, G;
-  int N[3], hi[3], ng;
-  AXB_HD Shell(const BoxDev &b, const int c[3]) {
-    ng = b.ng;
-    for (int d = 0; d < 3; ++d) {
-      N[d] = b.n[d] + 2 * ng + (c[d] ? 0 : 1);
-      hi[d] = ng + b.n[d] + (c[d] ? 0 : 1);
-    }
-    const long long plane = (long long)N[0] * N[1];
-    A = ng * plane;
-    B = (long long)(N[2] - hi[2]) * plane;
-    Cm = (long long)(ng + N[1] - hi[1]) * N[0] + (long long)(hi[1] - ng) * (ng + N[0] - hi[0]);
-    G = A + B + (long long)(hi[2] - ng) * Cm;
-  }
-  AXB_HD void point(long long g, int &i, int &j, int &k) const {
-    const long long plane = (long long)N[0] * N[1];
-    if (g < A + B) {
-      k = g < A ? int(g / plane) : hi[2] + int((g - A) / plane);
-      const long long r = g < A ? g % plane : (g - A) % plane;
-      j = int(r / N[0]);
-      i = int(r % N[0]);
-      return;
-    }
-    g -= A + B;
-    k = ng + int(g / Cm);
-    long long r = g % Cm;
-    const long long lowrows = (long long)ng * N[0], highrows = (long long)(N[1] - hi[1]) * N[0];
-    if (r < lowrows) {
-      j = int(r / N[0]);
-      i = int(r % N[0]);
-    } else if (r < lowrows + highrows) {
-      r -= lowrows;
-      j = hi[1] + int(r / N[0]);
-      i = int(r % N[0]);
-    } else {
-      r -= lowrows + highrows;
-      const int per = ng + N[0] - hi[0];
-      j = ng + int(r / per);
-      const int q = int(r % per);
-      i = q < ng ? q : hi[0] + (q - ng);
-    }
-  }
-};
-
-AXB_D void sync_shell_body(const SyncArgs &a, const uint3 bid) {
-  const BoxDev &b = a.b;
-  const int v = bid.z;
-  const Shell sh(b, a.cent[v]);
-  const long long g = (long long)bid.x * blockDim.x + threadIdx.x;
-  if (g >= sh.G)
-    return;
-  int i, j, k;
-  sh.point(g, i, j, k);
-  const int ng = b.ng;
-  const int is = (i >= ng && i < sh.hi[0]) ? i : wrap(i, ng, b.n[0]);
-  const int js = (j >= ng && j < sh.hi[1]) ? j : wrap(j, ng, b.n[1]);
-  const int ks = (k >= ng && k < sh.hi[2]) ? k : wrap(k, ng, b.n[2]);
-  double *f = a.f[v];
-  f[b.at(i, j, k)] = f[b.at(is, js, ks)];
 }
 
 __global__ void __launch_bounds__(128)
