@@ -624,9 +624,9 @@ struct PalQRST {
 };
 
 // Root function of the Palenzuela scheme (c2p_1DPalenzuela.hxx:264-303).
-// W^-2 is clamped as in the reference; W = (W^-2)^(-1/2) is taken as
-// 1/sqrt instead of pow, the divisions by W become products with its square
-// root, and 1/x and 1/(x (x+s)) come from one division (last-ulp
+// W^-2 is clamped as in the reference; W = (W^-2)^(-1/2) is taken as rsqrt
+// instead of pow and 1/W as W^-2 W, 1/x and 1/(x (x+s)) come from one
+// division, and P/rho comes from the EOS without a division (last-ulp
 // differences; the bracket search converges to the same tolerance).
 template <class EOS>
 AXB_HD double pal_froot(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
@@ -636,8 +636,8 @@ AXB_HD double pal_froot(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
   const double ix = xs * ixxs;
   double Wminus2 = 1.0 - (x * x * k.r + (2.0 * x + k.s) * k.t * k.t) * (ixxs * ixxs);
   Wminus2 = fmin(fmax(Wminus2, 1e-10), 1);
-  const double iW = sqrt(Wminus2);
-  const double W_loc = 1.0 / iW;
+  const double W_loc = rsqrt(Wminus2);
+  const double iW = Wminus2 * W_loc;
   const double rho_loc = cv.dens * iW;
   const double Ye_loc = k.ye;
   double eps_loc = W_loc - 1.0 + (1.0 - W_loc * W_loc) * x * iW +
@@ -646,8 +646,7 @@ AXB_HD double pal_froot(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
     eps_loc = fmax(eps_loc, atmo.eps);
     eps_loc = fmin(eps_loc, eos.rgeps.max);
   }
-  const double P_loc = eos.press_from_valid_rho_eps_ye(rho_loc, eps_loc, Ye_loc);
-  return (x - (1.0 + eps_loc + P_loc / rho_loc) * W_loc);
+  return (x - (1.0 + eps_loc + eos.press_over_rho(rho_loc, eps_loc, Ye_loc)) * W_loc);
 }
 
 // Palenzuela 1D (c2p_1DPalenzuela::solve, c2p_1DPalenzuela.hxx:306-556).
@@ -699,7 +698,7 @@ AXB_HD void palenzuela_solve(const EOS &eos, const C2PParams &cp, const Atmo &at
   k.q = cv.tau / cv.dens;
   k.r = Ssq / (cv.dens * cv.dens);
   k.s = Bsq / cv.dens;
-  k.t = BiSi / pow(cv.dens, 3. / 2.);
+  k.t = BiSi / (cv.dens * sqrt(cv.dens)); // dens^(3/2) without pow
   k.ye = cv.DYe / cv.dens;
   const double qP = cv.tau / cv.dens;
   const double sP = Bsq / cv.dens;
@@ -720,16 +719,18 @@ AXB_HD void palenzuela_solve(const EOS &eos, const C2PParams &cp, const Atmo &at
   double r0, r1;
   brent_bracket(fn, a, b, cp.minbits, cp.maxIter, rep.iters, r0, r1);
   const double x_sol = 0.5 * (r0 + r1);
-  // xPalenzuelaToPrim (c2p_1DPalenzuela.hxx:142-258)
+  // xPalenzuelaToPrim (c2p_1DPalenzuela.hxx:142-258); W = rsqrt(W^-2)
+  // instead of pow, the divisions by W and W^2 as products with W^-1 and
+  // W^-2 (last-ulp differences)
   {
     double Wminus2 = 1.0 - (x_sol * x_sol * k.r + (2.0 * x_sol + k.s) * k.t * k.t) /
                                (x_sol * x_sol * (x_sol + k.s) * (x_sol + k.s));
     Wminus2 = fmin(fmax(Wminus2, 1e-10), 1);
-    const double W_sol = pow(Wminus2, -0.5);
-    pv.rho = cv.dens / W_sol;
-    pv.eps = W_sol - 1.0 + (1.0 - W_sol * W_sol) * x_sol / W_sol +
-             W_sol * (k.q - k.s + k.t * k.t / (2 * x_sol * x_sol) +
-                      k.s / (2.0 * W_sol * W_sol));
+    const double W_sol = rsqrt(Wminus2);
+    const double iW = Wminus2 * W_sol;
+    pv.rho = cv.dens * iW;
+    pv.eps = W_sol - 1.0 + (1.0 - W_sol * W_sol) * x_sol * iW +
+             W_sol * (k.q - k.s + k.t * k.t / (2 * x_sol * x_sol) + 0.5 * k.s * Wminus2);
     if (cp.use_temp) {
       pv.eps = fmax(pv.eps, atmo.eps);
       pv.eps = fmin(pv.eps, eos.rgeps.max);

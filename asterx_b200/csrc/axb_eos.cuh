@@ -23,12 +23,18 @@ struct Range {
 struct EosIdeal {
   double gamma, gm1, inv_gamma, temp_over_eps;
   Range rgrho, rgye, rgtemp, rgeps;
+  // rho^(1-gamma) of the entropy without pow for the common adiabatic
+  // indices (set by make_ideal): 3 -> gamma = 4/3, rcbrt(rho); 5 -> 5/3,
+  // rcbrt(rho)^2; 2 -> gamma = 2, 1/rho; 0 -> pow (last-ulp differences)
+  int kappa_root;
 
   static constexpr bool kTabulated = false;
 
   AXB_HD double press_from_valid_rho_eps_ye(double rho, double &eps, double) const {
     return gm1 * rho * eps;
   }
+  // P / rho without the division (the root functions of the recovery)
+  AXB_HD double press_over_rho(double, double &eps, double) const { return gm1 * eps; }
   AXB_HD double eps_from_valid_rho_press_ye(double rho, double press, double) const {
     return press / (rho * gm1);
   }
@@ -46,7 +52,18 @@ struct EosIdeal {
     return press_from_valid_rho_eps_ye(rho, eps, ye);
   }
   AXB_HD double kappa_from_valid_rho_eps_ye(double rho, double &eps, double) const {
-    return (gamma - 1.0) * eps * pow(rho, 1.0 - gamma);
+    double r;
+    if (kappa_root == 3) {
+      r = rcbrt(rho);
+    } else if (kappa_root == 5) {
+      r = rcbrt(rho);
+      r *= r;
+    } else if (kappa_root == 2) {
+      r = 1.0 / rho;
+    } else {
+      r = pow(rho, 1.0 - gamma);
+    }
+    return (gamma - 1.0) * eps * r;
   }
 };
 
@@ -64,6 +81,11 @@ inline EosIdeal make_ideal(double gamma, double umass, Range rgeps, Range rgrho,
   e.rgrho = rgrho;
   e.rgye = rgye;
   e.temp_over_eps = e.gm1 * umass;
+  const double expo = 1 - gamma;
+  e.kappa_root = std::fabs(expo + 1.0 / 3) < 1e-14   ? 3
+                 : std::fabs(expo + 2.0 / 3) < 1e-14 ? 5
+                 : expo == -1.0                      ? 2
+                                                     : 0;
   e.rgtemp = Range{e.temp_over_eps * e.rgeps.min, e.temp_over_eps * e.rgeps.max};
   return e;
 }

@@ -167,6 +167,9 @@ struct EosTab {
   AXB_HD double lt_clamped(double temp) const {
     return log(fmin(fmax(temp, rgtemp.min), rgtemp.max));
   }
+  AXB_HD double press_over_rho(double rho, double &eps, double ye) const {
+    return press_from_valid_rho_eps_ye(rho, eps, ye) / rho;
+  }
   AXB_HD double press_from_valid_rho_eps_ye(double rho, double &eps, double ye) const {
     const double lr = lr_clamped(rho);
     const double lt = logtemp(rho, eps, ye);
