@@ -41,6 +41,10 @@ struct EosIdeal {
   AXB_HD double csnd_from_valid_rho_eps_ye(double, double &eps, double) const {
     return sqrt(gm1 * eps / (eps + inv_gamma));
   }
+  // the square of csnd_from_valid_rho_eps_ye without the square root
+  AXB_HD double csnd2_from_valid_rho_eps_ye(double, double &eps, double) const {
+    return gm1 * eps / (eps + inv_gamma);
+  }
   AXB_HD double temp_from_valid_rho_eps_ye(double, double &eps, double) const {
     return temp_over_eps * eps;
   }

@@ -48,7 +48,7 @@ struct RhsArgs {
 struct FaceMetric {
   double alp, beta[3];
   sym3 g;
-  double detg, sqrtg, uinv;
+  double detg, sqrtg, isqrtg, uinv;
 };
 
 template <int DIR>
@@ -77,9 +77,12 @@ AXB_D FaceMetric face_metric(const RhsArgs &a, long long I) {
   m.g.yz = avg_v2f<DIR>(a.g[4], I, s1, s2);
   m.g.zz = avg_v2f<DIR>(a.g[5], I, s1, s2);
   m.detg = det3(m.g);
-  m.sqrtg = sqrt(m.detg);
+  // sqrt(detg), 1/sqrt(detg) and 1/detg from one rsqrt instead of a square
+  // root and two divisions (last-ulp differences)
+  m.isqrtg = rsqrt(m.detg);
+  m.sqrtg = m.detg * m.isqrtg;
   // (dir,dir) element of calc_inv(g, detg)
-  const double idet = 1 / m.detg;
+  const double idet = m.isqrtg * m.isqrtg;
   if (DIR == 0)
     m.uinv = (m.g.yy * m.g.zz - m.g.yz * m.g.yz) * idet;
   else if (DIR == 1)
@@ -124,10 +127,11 @@ AXB_D void side_physics(const FaceMetric &m, const double *r, double Bdir,
   B[D2] = r[R_B2];
   double vlow[3];
   lower3(m.g, vel, vlow);
-  // 1/W is used in four places: take it as the square root itself and
-  // multiply (last-ulp differences from the reference's divisions by W)
-  const double iW = sqrt(1 - dot3(vlow, vel));
-  const double W = 1 / iW;
+  // W = rsqrt(1 - v^2) and 1/W = (1 - v^2) W, used in four places as a
+  // product (last-ulp differences from the reference's divisions by W)
+  const double omv2 = 1 - dot3(vlow, vel);
+  const double W = rsqrt(omv2);
+  const double iW = omv2 * W;
   double vt[3];
   for (int i = 0; i < 3; ++i)
     vt[i] = m.alp * vel[i] - m.beta[i];
@@ -142,12 +146,18 @@ AXB_D void side_physics(const FaceMetric &m, const double *r, double Bdir,
   // cs^2 as the product of two sound-speed queries (fluxes.cxx:556-560); the
   // first may clamp eps in place (tabulated), and only then can the second
   // differ from the first
-  const double eps_in = eps;
-  const double cs = eos.csnd_from_valid_rho_eps_ye(rho, eps, ye);
-  const double cs2 =
-      cs * ((EOS::kTabulated && !(eps == eps_in)) ? eos.csnd_from_valid_rho_eps_ye(rho, eps, ye)
-                                                  : cs);
-  const double h = 1 + eps + press / rho;
+  double cs2, h;
+  if constexpr (EOS::kTabulated) {
+    const double eps_in = eps;
+    const double cs = eos.csnd_from_valid_rho_eps_ye(rho, eps, ye);
+    cs2 = cs * (!(eps == eps_in) ? eos.csnd_from_valid_rho_eps_ye(rho, eps, ye) : cs);
+    h = 1 + eps + press / rho;
+  } else {
+    // ideal gas: cs^2 without the square root, P/rho without the division
+    // (last-ulp differences)
+    cs2 = eos.csnd2_from_valid_rho_eps_ye(rho, eps, ye);
+    h = 1 + eps + eos.press_over_rho(rho, eps, ye);
+  }
   const double dens = m.sqrtg * rho * W;
   const double DEnt = m.sqrtg * rho * W * ent;
   const double dhW = dens * h * W;

@@ -81,7 +81,7 @@ AXB_D void face_fluxes(const RhsArgs &a, const EOS &eos,
     }
   }
   const FaceMetric m = face_metric<DIR>(a, I);
-  const double Bdir = __ldg(a.dBstag[DIR] + I) / m.sqrtg;
+  const double Bdir = __ldg(a.dBstag[DIR] + I) * m.isqrtg;
   SideOut sL, sR;
   side_physics<DIR>(m, L, Bdir, eos, a.rec_temp, sL);
   side_physics<DIR>(m, R, Bdir, eos, a.rec_temp, sR);
