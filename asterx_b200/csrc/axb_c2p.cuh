@@ -51,14 +51,17 @@ struct Cons {
     DEnt *= s;
   }
   AXB_HD void unscale(double s) { // divide every component (undensitise)
-    dens /= s;
-    tau /= s;
+    // one division and eight products instead of eight divisions
+    // (last-ulp differences)
+    const double is = 1.0 / s;
+    dens *= is;
+    tau *= is;
     for (int i = 0; i < 3; ++i)
-      mom[i] /= s;
+      mom[i] *= is;
     for (int i = 0; i < 3; ++i)
-      dBvec[i] /= s;
-    DYe /= s;
-    DEnt /= s;
+      dBvec[i] *= is;
+    DYe *= is;
+    DEnt *= is;
   }
 };
 
@@ -338,11 +341,14 @@ AXB_HD void vel_from_Z(double Z_Sol, double W_Sol, double Bsq, double BiSi,
       pv.vel[i] = z[i] / SafeLor;
     pv.w_lor = SafeLor;
   } else {
+    // 1/(Z (Z+B^2)) and 1/(Z+B^2) from one division (last-ulp differences)
+    const double iZZB = 1.0 / (Z_Sol * (Z_Sol + Bsq));
+    const double iZB = Z_Sol * iZZB;
     for (int i = 0; i < 3; ++i) {
       const double gm = gup(i, 0) * cv.mom[0] + gup(i, 1) * cv.mom[1] +
                         gup(i, 2) * cv.mom[2];
-      pv.vel[i] = gm / (Z_Sol + Bsq);
-      pv.vel[i] += BiSi * cv.dBvec[i] / (Z_Sol * (Z_Sol + Bsq));
+      pv.vel[i] = gm * iZB;
+      pv.vel[i] += BiSi * cv.dBvec[i] * iZZB;
     }
     pv.w_lor = W_Sol;
   }
@@ -694,14 +700,17 @@ AXB_HD void palenzuela_solve(const EOS &eos, const C2PParams &cp, const Atmo &at
     cv.set_nan();
     return;
   }
+  // the invariants as products with 1/dens and dens^(-1/2) = rsqrt(dens)
+  // instead of five divisions and a pow (last-ulp differences)
+  const double idens = 1.0 / cv.dens;
   PalQRST k;
-  k.q = cv.tau / cv.dens;
-  k.r = Ssq / (cv.dens * cv.dens);
-  k.s = Bsq / cv.dens;
-  k.t = BiSi / (cv.dens * sqrt(cv.dens)); // dens^(3/2) without pow
-  k.ye = cv.DYe / cv.dens;
-  const double qP = cv.tau / cv.dens;
-  const double sP = Bsq / cv.dens;
+  k.q = cv.tau * idens;
+  k.r = Ssq * (idens * idens);
+  k.s = Bsq * idens;
+  k.t = BiSi * (idens * rsqrt(cv.dens));
+  k.ye = cv.DYe * idens;
+  const double qP = k.q;
+  const double sP = k.s;
   double a = fmax(1e-10, 1.0 + qP - sP);
   double b = 2.0 + 2.0 * qP - sP;
   auto fn = [&](double x) { return pal_froot(eos, cp, atmo, k, x, cv); };
@@ -723,14 +732,16 @@ AXB_HD void palenzuela_solve(const EOS &eos, const C2PParams &cp, const Atmo &at
   // instead of pow, the divisions by W and W^2 as products with W^-1 and
   // W^-2 (last-ulp differences)
   {
-    double Wminus2 = 1.0 - (x_sol * x_sol * k.r + (2.0 * x_sol + k.s) * k.t * k.t) /
-                               (x_sol * x_sol * (x_sol + k.s) * (x_sol + k.s));
+    // 1/x^2 = (x+s)^2 / (x^2 (x+s)^2): one division
+    const double xs2 = (x_sol + k.s) * (x_sol + k.s);
+    const double iden = 1.0 / (x_sol * x_sol * xs2);
+    double Wminus2 = 1.0 - (x_sol * x_sol * k.r + (2.0 * x_sol + k.s) * k.t * k.t) * iden;
     Wminus2 = fmin(fmax(Wminus2, 1e-10), 1);
     const double W_sol = rsqrt(Wminus2);
     const double iW = Wminus2 * W_sol;
     pv.rho = cv.dens * iW;
     pv.eps = W_sol - 1.0 + (1.0 - W_sol * W_sol) * x_sol * iW +
-             W_sol * (k.q - k.s + k.t * k.t / (2 * x_sol * x_sol) + 0.5 * k.s * Wminus2);
+             W_sol * (k.q - k.s + 0.5 * k.t * k.t * (xs2 * iden) + 0.5 * k.s * Wminus2);
     if (cp.use_temp) {
       pv.eps = fmax(pv.eps, atmo.eps);
       pv.eps = fmin(pv.eps, eos.rgeps.max);

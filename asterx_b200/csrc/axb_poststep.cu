@@ -190,8 +190,8 @@ AXB_D void c2p_box_body(const C2PBoxArgs &a, const EOS &eos, const uint3 bid) {
     cv.DEnt = a.DEnt[I];
     for (int q = 0; q < 3; ++q)
       cv.dBvec[q] = dB[q];
-    const double Bup[3] = {cv.dBvec[0] / sqrt_detg, cv.dBvec[1] / sqrt_detg,
-                           cv.dBvec[2] / sqrt_detg};
+    const double isg = 1.0 / sqrt_detg;
+    const double Bup[3] = {cv.dBvec[0] * isg, cv.dBvec[1] * isg, cv.dBvec[2] * isg};
     Prim pv;
     pv.set_nan();
     Prim seeds;
@@ -679,8 +679,8 @@ __global__ void __launch_bounds__(128, AXB_C2P_MINB)
   bool failed = false;
   if (valid) {
     const double sqrt_detg = sqrt(det3(glo));
-    const double Bup[3] = {cv.dBvec[0] / sqrt_detg, cv.dBvec[1] / sqrt_detg,
-                           cv.dBvec[2] / sqrt_detg};
+    const double isg = 1.0 / sqrt_detg;
+    const double Bup[3] = {cv.dBvec[0] * isg, cv.dBvec[1] * isg, cv.dBvec[2] * isg};
     Prim pv;
     pv.set_nan();
     Prim seeds;
