@@ -19,6 +19,8 @@
 //   godunov    ReconX/src/reconstruct.hxx:53-55 (cell value)
 #pragma once
 
+#include <cmath>
+
 #include "axb_common.cuh"
 
 namespace axb {
@@ -127,14 +129,27 @@ AXB_HD CellLoUp recon_ppm(const double q[5], const double pr[5],
   return {rc_low, rc_up};
 }
 
+// 2^-e for a positive normal x = m 2^e (1 <= m < 2): an exact rescaling
+AXB_HD double pow2_inv_exponent(double x) {
+#ifdef __CUDA_ARCH__
+  const long long E = (__double_as_longlong(x) >> 52) & 0x7ff;
+  return __longlong_as_double((2046 - E) << 52);
+#else
+  return std::ldexp(1.0, -std::ilogb(x));
+#endif
+}
+
 AXB_HD CellLoUp recon_wenoz(const double q[5], double weno_eps) {
   // Same weights and candidate stencils as the reference, with its divisions
-  // regrouped: 1 + tau5 / (beta_k + eps) for the three k share one
-  // reciprocal of the product of the three denominators, and both weight
-  // normalisations (and the 1/6 of the stencils) share one reciprocal of
-  // the product of the two sums -- 2 FP64 divisions per cell instead of 15,
-  // last-ulp differences.  The products stay far from overflow for
-  // |values| < 1e50 (beta ~ value^2, eps = 1e-26 bounds them below).
+  // regrouped into ONE per cell (last-ulp differences).  With
+  // d_k = beta_k + eps and P = d0 d1 d2, the unnormalised weight
+  // w_k (1 + tau5 / d_k) is w_k n_k / P with n_k = P + tau5 prod_{j != k} d_j;
+  // the common 1/P cancels in the normalisation, so both sides' weights (and
+  // the 1/6 of the stencils) share one reciprocal of the product of the two
+  // weight sums.  The n_k are scaled by an exact power of two that brings P
+  // to [1, 2), so n_k ~ 1 + tau5 / d_k as in the reference and the product of
+  // the sums stays far from overflow for |values| < 1e50 (eps = 1e-26 bounds
+  // d_k below).
   const double a = q[0], b = q[1], c = q[2], d = q[3], e = q[4];
   const double beta0 = (13.0 / 12.0) * sq(a - 2.0 * b + c) +
                        (1.0 / 4.0) * sq(a - 4.0 * b + 3.0 * c);
@@ -144,10 +159,12 @@ AXB_HD CellLoUp recon_wenoz(const double q[5], double weno_eps) {
                        (1.0 / 4.0) * sq(3.0 * c - 4.0 * d + e);
   const double tau5 = fabs(beta0 - beta2);
   const double d0 = beta0 + weno_eps, d1 = beta1 + weno_eps, d2 = beta2 + weno_eps;
-  const double r = tau5 / (d0 * d1 * d2);
-  const double aux0 = 1.0 + r * (d1 * d2);
-  const double aux1 = 1.0 + r * (d0 * d2);
-  const double aux2 = 1.0 + r * (d0 * d1);
+  const double P = d0 * d1 * d2;
+  const double sc = pow2_inv_exponent(P);
+  const double Ps = P * sc, ts = tau5 * sc;
+  const double aux0 = Ps + ts * (d1 * d2);
+  const double aux1 = Ps + ts * (d0 * d2);
+  const double aux2 = Ps + ts * (d0 * d1);
   const double w0 = 3.0 / 10.0, w1 = 3.0 / 5.0, w2 = 1.0 / 10.0;
   // minus side (lower value): weights w0, w1, w2; plus side: w2, w1, w0
   const double am0 = w0 * aux0, am1 = w1 * aux1, am2 = w2 * aux2;

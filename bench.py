@@ -268,6 +268,12 @@ def reference_arm(args):
 # ---------------------------------------------------------------------------
 # the engine
 # ---------------------------------------------------------------------------
+def _mean_iters(hist):
+    """Mean first-solver iteration count of a status histogram."""
+    tot = sum(int(v) for v in hist)
+    return sum(i * int(v) for i, v in enumerate(hist)) / tot if tot else None
+
+
 def ours(args):
     import torch
     import torch.distributed as dist
@@ -438,6 +444,7 @@ def ours(args):
             "clocks": clocks,
             "error_word": st["error_word"], "c2p_fail_cells": st["c2p_fail"],
             "max_char_speed": st["max_speed"],
+            "c2p_mean_iters": _mean_iters(st["iter_hist"]),
         }
         print(json.dumps(line), flush=True)
     eng.close()
