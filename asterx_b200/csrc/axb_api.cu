@@ -486,7 +486,10 @@ AXB_API int axb_rhs_group(axb_ctx *c, const axb_box *box, const axb_fields *f,
   if (eos->kind == 1 && !a.rec_temp)
     return AXB_ERR_UNSUPPORTED;
   cudaStream_t s = (cudaStream_t)stream;
-  const int seglen = 32;
+#ifndef AXB_FLUX_SEGLEN
+#define AXB_FLUX_SEGLEN 32 // cells per y/z pencil segment (one thread each)
+#endif
+  const int seglen = AXB_FLUX_SEGLEN;
   axb_mark(c, AXB_R_SOURCES, s, true);
   rc = launch_rhs_misc(p->local_spatial_order == 4 ? 1 : 0, a, s);
   axb_mark(c, AXB_R_SOURCES, s, false);
