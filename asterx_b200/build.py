@@ -22,6 +22,14 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
          "-Xcompiler", "-fPIC,-fvisibility=hidden", "-I" + os.path.join(REPO, "include")]
+# Per-file flags.  The recovery is compiled without multiply-add contraction:
+# every FP64 operation is rounded on its own, as written, so the same cell
+# gives the same bits whichever kernel (single box, fast pass, deferred
+# pass, batched level) inlines the recovery -- contraction choices depend on
+# the surrounding code, and the Brent bracket amplifies a last-bit
+# difference to the root-finder tolerance.  It also follows the per-operation
+# rounding of the reference's CPU build.
+FILE_FLAGS = {"axb_poststep.cu": ["-fmad=false"]}
 
 
 def _stale(target, deps):
@@ -32,7 +40,8 @@ def _stale(target, deps):
 
 
 def _compile(src, obj, extra):
-    cmd = [NVCC, *ARCH, *FLAGS, *extra, "-c", src, "-o", obj]
+    cmd = [NVCC, *ARCH, *FLAGS, *FILE_FLAGS.get(os.path.basename(src), []), *extra, "-c",
+           src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc failed for {src}:\n{r.stderr}")
@@ -51,7 +60,7 @@ def build(force=False, verbose=False, extra=()):
     for s in srcs:
         o = os.path.join(objdir, os.path.basename(s)[:-3] + ".o")
         objs.append(o)
-        if force or _stale(o, [s, *headers]):
+        if force or _stale(o, [s, *headers, os.path.abspath(__file__)]):
             jobs.append((s, o))
     if jobs:
         with cf.ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:

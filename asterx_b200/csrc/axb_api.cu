@@ -145,6 +145,10 @@ AXB_API int axb_ctx_destroy(axb_ctx *c) {
   }
   cudaFree(c->status);
   cudaFreeHost(c->status_host_pinned);
+  if (c->pool) {
+    cudaDeviceSynchronize(); // stream-ordered frees of the pool's blocks
+    cudaMemPoolDestroy(c->pool);
+  }
   delete c;
   return AXB_OK;
 }

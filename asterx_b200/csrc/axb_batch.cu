@@ -45,7 +45,9 @@ int launch_sync_batch(const void *args, const TileTable &t, unsigned long long *
                       int nblocks, cudaStream_t s);
 int launch_c2p_batch(int which, const void *args, const TileTable &t,
                      unsigned long long *ctr, const axb_eos &eos, DevStatus *status,
-                     int nblocks, cudaStream_t s);
+                     int nblocks, cudaStream_t s, unsigned long long *queue = nullptr,
+                     int deferred_blocks = 0);
+bool c2p_batch_fast_ok(int nbox, const axb_box *boxes, const axb_params *p);
 } // namespace axb
 
 namespace {
@@ -95,6 +97,8 @@ struct axb_batch {
   int seg[2] = {2, 2};        // index into kSeg (32)
   int ctas[NPHASE];           // CTAs per SM of each phase's persistent grid
   unsigned long long *ctr = nullptr; // one work counter per phase
+  // deferred-cell queue of the recovery's fast pass (null: full cascade)
+  unsigned long long *c2p_queue = nullptr;
   long long zones = 0;
 };
 
@@ -177,7 +181,10 @@ int launch_phase(axb_ctx *c, const axb_batch *B, int phase, double alpha, double
   case P_STAGE: rc = launch_stage_batch(B->stage_args, t, ctr, alpha, beta, gdt, nb, s); break;
   case P_SYNC_E: rc = launch_sync_batch(B->sync_e, t, ctr, nb, s); break;
   case P_BSTAG: rc = launch_c2p_batch(0, B->c2p_args, t, ctr, *B->eos, B->status, nb, s); break;
-  case P_C2P: rc = launch_c2p_batch(1, B->c2p_args, t, ctr, *B->eos, B->status, nb, s); break;
+  case P_C2P:
+    rc = launch_c2p_batch(1, B->c2p_args, t, ctr, *B->eos, B->status, nb, s, B->c2p_queue,
+                          4 * B->sms);
+    break;
   case P_SYNC_P: rc = launch_sync_batch(B->sync_p, t, ctr, nb, s); break;
   }
   axb_mark(c, kRegion[phase], s, false);
@@ -207,6 +214,7 @@ AXB_API int axb_batch_destroy(axb_batch *B) {
   cudaFree(B->sync_e);
   cudaFree(B->sync_p);
   cudaFree(B->ctr);
+  cudaFree(B->c2p_queue);
   for (auto &t : B->tab)
     free_table(t);
   for (auto &d : B->flux_seg)
@@ -263,6 +271,9 @@ AXB_API int axb_batch_create(axb_ctx *c, int nbox, const axb_box *boxes,
   if (!rc)
     rc = make_table(bx, g_sync, 1, B->tab[P_SYNC_P]);
   if (!rc && cudaMalloc(&B->ctr, NPHASE * sizeof(unsigned long long)) != cudaSuccess)
+    rc = AXB_ERR_CUDA;
+  if (!rc && c2p_batch_fast_ok(nbox, boxes, p) &&
+      cudaMalloc(&B->c2p_queue, (B->zones + 1) * sizeof(unsigned long long)) != cudaSuccess)
     rc = AXB_ERR_CUDA;
   if (rc) {
     axb_batch_destroy(B);

@@ -11,6 +11,8 @@
 // into shared memory when it moves on to the next box.
 #pragma once
 
+#include <type_traits>
+
 #include "axb_common.cuh"
 
 namespace axb {
@@ -80,7 +82,11 @@ AXB_D void batch_loop(const Args *__restrict__ args, const TileTable &t,
         __syncthreads();
         cur = bx;
       }
-      f(a, tile_bid(t.grid[bx], item - __ldg(t.prefix + bx)));
+      const uint3 bid = tile_bid(t.grid[bx], item - __ldg(t.prefix + bx));
+      if constexpr (std::is_invocable_v<F &, const Args &, uint3, int>)
+        f(a, bid, bx); // bodies that need the box index
+      else
+        f(a, bid);
     }
   }
 }

@@ -80,7 +80,9 @@ enum RepStatus {
   REP_ROOT_FAIL_BRACKET,
   REP_PREP_ROOT_FAIL_CONV,
   REP_PREP_ROOT_FAIL_BRACKET,
-  REP_NOT_SET
+  REP_NOT_SET,
+  // (engine only) the fast pass left the cell to the full cascade
+  REP_DEFER
 };
 struct Report {
   int status = REP_NOT_SET;
@@ -549,12 +551,15 @@ AXB_HD void noble_solve(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
 // reference checker (inverse quadratic / secant / bisection, R. P. Brent
 // 1973).
 // ---------------------------------------------------------------------------
+// `fa0`, `fb0` are f(a) and f(b), which the caller has evaluated already
+// (the reference evaluates them again inside its brent; f is deterministic,
+// so the values are the same).
 template <class F>
-AXB_HD void brent_bracket(const F &f, double a, double b, int minbits,
-                          int maxiters, int &iters, double &lo, double &hi) {
+AXB_HD void brent_bracket(const F &f, double a, double b, double fa0, double fb0,
+                          int minbits, int maxiters, int &iters, double &lo, double &hi) {
   const double eps = ldexp(1.0, -minbits);
-  double fa = f(a);
-  double fb = f(b);
+  double fa = fa0;
+  double fb = fb0;
   iters = 0;
   if (fa == 0) {
     lo = hi = a;
@@ -658,7 +663,10 @@ AXB_HD double pal_froot(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
 // Palenzuela 1D (c2p_1DPalenzuela::solve, c2p_1DPalenzuela.hxx:306-556).
 // `xlo`/`xhi` > 0 narrow the initial bracket (learned initial guess); the
 // reference bracket is used when they are negative or do not bracket.
-template <class EOS>
+// FAST: the common path only -- every failure, and a bracket that did not
+// converge (which needs the conservative-variable check), returns REP_DEFER
+// before anything else, so the caller can hand the cell to the full cascade.
+template <class EOS, bool FAST = false>
 AXB_HD void palenzuela_solve(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
                              Prim &pv, Cons &cv, const sym3 &glo, Report &rep,
                              double xlo = -1.0, double xhi = -1.0) {
@@ -672,6 +680,10 @@ AXB_HD void palenzuela_solve(const EOS &eos, const C2PParams &cp, const Atmo &at
   const bool minor2 = glo.xx * glo.yy - glo.xy * glo.xy > 0.0;
   const bool minor3 = spatial_detg > 0.0;
   if (!(minor1 && minor2 && minor3)) {
+    if constexpr (FAST) {
+      rep.status = REP_DEFER;
+      return;
+    }
     rep.fail(REP_INVALID_DETG);
     pv.set_nan();
     cv.set_nan();
@@ -689,12 +701,20 @@ AXB_HD void palenzuela_solve(const EOS &eos, const C2PParams &cp, const Atmo &at
       cv.dBvec[0] * cv.mom[0] + cv.dBvec[1] * cv.mom[1] + cv.dBvec[2] * cv.mom[2];
   if (!isfinite(cv.dens) || !isfinite(Ssq) || !isfinite(Bsq) || !isfinite(BiSi) ||
       !isfinite(cv.DYe) || !isfinite(cv.DEnt)) {
+    if constexpr (FAST) {
+      rep.status = REP_DEFER;
+      return;
+    }
     rep.fail(REP_NANS_IN_CONS);
     pv.set_nan();
     cv.set_nan();
     return;
   }
   if (Bsq > cp.Bsq_lim) {
+    if constexpr (FAST) {
+      rep.status = REP_DEFER;
+      return;
+    }
     rep.fail(REP_B_LIMIT);
     pv.set_nan();
     cv.set_nan();
@@ -715,18 +735,34 @@ AXB_HD void palenzuela_solve(const EOS &eos, const C2PParams &cp, const Atmo &at
   double b = 2.0 + 2.0 * qP - sP;
   auto fn = [&](double x) { return pal_froot(eos, cp, atmo, k, x, cv); };
   bool narrowed = false;
+  double fa = 0.0, fb = 0.0;
   if (xlo > 0.0 && xhi > xlo) {
     const double flo = fn(xlo), fhi = fn(xhi);
     if (flo * fhi < 0) {
       a = xlo;
       b = xhi;
+      fa = flo;
+      fb = fhi;
       narrowed = true;
     }
   }
-  if (!narrowed && fn(a) * fn(b) > 0)
-    b = 3.0 + 3.0 * qP - 1.5 * sP;
+  if (!narrowed) {
+    fa = fn(a);
+    fb = fn(b);
+    if (fa * fb > 0) {
+      b = 3.0 + 3.0 * qP - 1.5 * sP;
+      fb = fn(b);
+    }
+  }
   double r0, r1;
-  brent_bracket(fn, a, b, cp.minbits, cp.maxIter, rep.iters, r0, r1);
+  brent_bracket(fn, a, b, fa, fb, cp.minbits, cp.maxIter, rep.iters, r0, r1);
+  const bool converged = !(fabs(r0 - r1) > cp.tolerance_0 * fmin(fabs(r0), fabs(r1)));
+  if constexpr (FAST) {
+    if (!converged) {
+      rep.status = REP_DEFER;
+      return;
+    }
+  }
   const double x_sol = 0.5 * (r0 + r1);
   // xPalenzuelaToPrim (c2p_1DPalenzuela.hxx:142-258); W = rsqrt(W^-2)
   // instead of pow, the divisions by W and W^2 as products with W^-1 and
@@ -756,6 +792,12 @@ AXB_HD void palenzuela_solve(const EOS &eos, const C2PParams &cp, const Atmo &at
       pv.Bvec[i] = cv.dBvec[i];
     set_E(pv, gup);
   }
+  if constexpr (FAST) {
+    if (!(pv.rho > 0.0) || !(pv.eps > 0.0)) {
+      rep.status = REP_DEFER;
+      return;
+    }
+  }
   if (pv.rho <= 0.0) {
     rep.fail(REP_RANGE_RHO);
     cv.scale(sqrt_detg);
@@ -766,7 +808,7 @@ AXB_HD void palenzuela_solve(const EOS &eos, const C2PParams &cp, const Atmo &at
     cv.scale(sqrt_detg);
     return;
   }
-  if (fabs(r0 - r1) > cp.tolerance_0 * fmin(fabs(r0), fabs(r1))) {
+  if (!FAST && !converged) {
     Cons ck;
     cons_from_prim(ck, pv, glo);
     ck.unscale(sqrt_detg);

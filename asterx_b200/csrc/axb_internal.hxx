@@ -35,7 +35,35 @@ struct axb_ctx {
   int ev_used = 0;
   cudaEvent_t *ev = nullptr; // 2 * AXB_EVENT_POOL
   int *ev_region = nullptr;
+  // stream-ordered pool of per-call scratch (the recovery's deferred-cell
+  // queue); keeps its memory between calls
+  cudaMemPool_t pool = nullptr;
 };
+
+// Stream-ordered scratch: from the context's pool, or (during a stream
+// capture) from the device's default pool, which captures as a graph
+// allocation node.  Release with cudaFreeAsync on the same stream.
+inline cudaError_t axb_scratch_alloc(axb_ctx *c, void **p, size_t bytes, cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess)
+    return cudaErrorUnknown;
+  if (cs != cudaStreamCaptureStatusNone)
+    return cudaMallocAsync(p, bytes, s);
+  if (!c->pool) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = c->device;
+    cudaError_t e = cudaMemPoolCreate(&c->pool, &props);
+    if (e != cudaSuccess) {
+      c->pool = nullptr;
+      return e;
+    }
+    unsigned long long keep = ~0ull;
+    cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  return cudaMallocFromPoolAsync(p, bytes, c->pool, s);
+}
 
 // Record the start / end event of one timed launch (no-ops unless timing).
 inline void axb_mark(axb_ctx *c, int region, cudaStream_t s, bool start) {

@@ -116,21 +116,22 @@ AXB_D void run_solver(int which, const EOS &eos, const C2PBoxArgs &a,
 #ifndef AXB_C2P_MINB
 #define AXB_C2P_MINB 4 // resident CTAs per SM the register budget must allow
 #endif
-template <class EOS>
-AXB_D void c2p_box_body(const C2PBoxArgs &a, const EOS &eos, const uint3 bid) {
-  __shared__ unsigned int s_hist[64];
+//
+// MODE C2P_FULL runs the whole cascade.  MODE C2P_FAST (Palenzuela as the
+// first solver) runs the common path only and returns true, having written
+// nothing, for a cell that needs anything else -- the excision / BH-interior
+// treatment, a Palenzuela failure (and so the second solver), or a bracket
+// that did not converge (and so the conservative-variable check); such a
+// cell is then recovered by the full cascade in a second launch, from the
+// same unmodified inputs, so every cell gets exactly the full cascade's
+// result.  The rare paths' code stays out of the fast kernel and no warp of
+// it waits on them.
+enum { C2P_FULL = 0, C2P_FAST = 1 };
+template <class EOS, int MODE>
+AXB_D bool c2p_cell(const C2PBoxArgs &a, const EOS &eos, const int i, const int j,
+                    const int k, int &iters_first, bool &failed) {
   const BoxDev &b = a.b;
-  if (a.want_hist) {
-    for (int q = threadIdx.x; q < 64; q += blockDim.x)
-      s_hist[q] = 0;
-    __syncthreads();
-  }
-  int i, j;
-  const int k = b.ng + bid.z;
-  const bool in_range = b.row_ij(b.ng, b.n[0], b.ng, b.n[1], bid, i, j);
-  int iters_first = -1;
-  bool failed = false;
-  if (in_range) {
+  {
     const long long I = b.at(i, j, k);
     double dB[3];
     dB[0] = 0.5 * (a.dBstag[0][I] + a.dBstag[0][I + 1]);
@@ -223,14 +224,27 @@ AXB_D void c2p_box_body(const C2PBoxArgs &a, const EOS &eos, const uint3 bid) {
     }
     if (alp_avg < a.cp.alp_thresh)
       mask_local = 0.0;
-    if (a.excise && mask_local != 1.0) {
+    if constexpr (MODE == C2P_FAST) {
+      if (mask_local != 1.0)
+        return true;
+    }
+    if (MODE == C2P_FULL && a.excise && mask_local != 1.0) {
       seeds.entropy = eos.kappa_from_valid_rho_eps_ye(seeds.rho, seeds.eps, seeds.Ye);
       bh_interior<false>(eos, a.cp, atmo, seeds, cv, glo);
       pv = seeds;
       call_c2p = false;
     }
     cons_floors(cv, glo);
-    if (call_c2p) {
+    if constexpr (MODE == C2P_FAST) {
+      if (call_c2p) {
+        Report r1;
+        code = AXB_C2P_PRIME;
+        palenzuela_solve<EOS, true>(eos, a.cp, atmo, pv, cv, glo, r1);
+        if (r1.failed())
+          return true; // REP_DEFER: every failure goes to the full cascade
+        iters_first = r1.iters;
+      }
+    } else if (call_c2p) {
       Report r1, r2;
       code = AXB_C2P_PRIME;
       run_solver(a.c2p_prime, eos, a, atmo, pv, seeds, cv, glo, r1);
@@ -291,6 +305,21 @@ AXB_D void c2p_box_body(const C2PBoxArgs &a, const EOS &eos, const uint3 bid) {
     a.saved_eps[I] = pv.eps;
     a.saved_Ye[I] = pv.Ye;
   }
+  return false;
+}
+
+// Warp and block epilogue of a recovery launch: failure count, and the
+// first solver's iteration histogram through shared memory (every thread of
+// the block must arrive).
+AXB_D void c2p_hist_init(const C2PBoxArgs &a, unsigned int *s_hist) {
+  if (a.want_hist) {
+    for (int q = threadIdx.x; q < 64; q += blockDim.x)
+      s_hist[q] = 0;
+    __syncthreads();
+  }
+}
+AXB_D void c2p_epilogue(const C2PBoxArgs &a, unsigned int *s_hist, int iters_first,
+                        bool failed) {
   const unsigned nfail = __popc(__ballot_sync(0xffffffffu, failed));
   if (nfail && (threadIdx.x % 32) == 0) {
     atomicAdd(&a.status->c2p_fail_count, nfail);
@@ -305,12 +334,127 @@ AXB_D void c2p_box_body(const C2PBoxArgs &a, const EOS &eos, const uint3 bid) {
         atomicAdd(&a.status->c2p_iter_hist[q], (unsigned long long)s_hist[q]);
   }
 }
+
+template <class EOS>
+AXB_D void c2p_box_body(const C2PBoxArgs &a, const EOS &eos, const uint3 bid) {
+  __shared__ unsigned int s_hist[64];
+  c2p_hist_init(a, s_hist);
+  int i, j;
+  const int k = a.b.ng + bid.z;
+  const bool in_range = a.b.row_ij(a.b.ng, a.b.n[0], a.b.ng, a.b.n[1], bid, i, j);
+  int iters_first = -1;
+  bool failed = false;
+  if (in_range)
+    c2p_cell<EOS, C2P_FULL>(a, eos, i, j, k, iters_first, failed);
+  c2p_epilogue(a, s_hist, iters_first, failed);
+}
 template <class EOS>
 __global__ void __launch_bounds__(128, AXB_C2P_MINB)
     k_c2p_box(const C2PBoxArgs a, const EOS eos) {
   c2p_box_body<EOS>(a, eos, blockIdx);
 }
 
+// Deferred cells of a fast pass: the count, then one entry per cell,
+// i | j << 15 | k << 30 | box << 45 (box 0 for a single box).
+struct C2PQueue {
+  unsigned long long *count;
+  unsigned long long *cell;
+};
+constexpr int C2P_QUEUE_MAX_EXTENT = 1 << 15; // per axis, ghosts included
+constexpr int C2P_QUEUE_MAX_BOXES = 1 << 19;
+
+// Fast pass over one tile: the common path, deferred cells appended to the
+// queue (warp-aggregated).
+template <class EOS>
+AXB_D void c2p_fast_body(const C2PBoxArgs &a, const EOS &eos, const uint3 bid, int box,
+                         const C2PQueue &q) {
+  __shared__ unsigned int s_hist[64];
+  c2p_hist_init(a, s_hist);
+  int i, j;
+  const int k = a.b.ng + bid.z;
+  const bool in_range = a.b.row_ij(a.b.ng, a.b.n[0], a.b.ng, a.b.n[1], bid, i, j);
+  int iters_first = -1;
+  bool failed = false;
+  bool defer = false;
+  if (in_range)
+    defer = c2p_cell<EOS, C2P_FAST>(a, eos, i, j, k, iters_first, failed);
+  const unsigned m = __ballot_sync(0xffffffffu, defer);
+  if (m) {
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == leader)
+      base = atomicAdd(q.count, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (defer)
+      q.cell[base + __popc(m & ((1u << lane) - 1u))] =
+          (unsigned long long)i | ((unsigned long long)j << 15) |
+          ((unsigned long long)k << 30) | ((unsigned long long)box << 45);
+  }
+  c2p_epilogue(a, s_hist, iters_first, failed);
+}
+
+// The full cascade over the queued cells; `args_of(box)` gives the box's
+// argument block.  Every thread runs the same number of rounds, so the
+// warp-level epilogue sees full warps.
+template <class EOS, class ArgsOf>
+AXB_D void c2p_deferred_body(const ArgsOf &args_of, const EOS &eos, const C2PQueue &q) {
+  __shared__ unsigned int s_hist[64];
+  const C2PBoxArgs &a0 = args_of(0);
+  const bool want_hist = a0.want_hist;
+  DevStatus *const status = a0.status;
+  if (want_hist) {
+    for (int t = threadIdx.x; t < 64; t += blockDim.x)
+      s_hist[t] = 0;
+    __syncthreads();
+  }
+  const unsigned long long n = *q.count;
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  const unsigned long long rounds = (n + stride - 1) / stride;
+  for (unsigned long long r = 0; r < rounds; ++r) {
+    const unsigned long long e = r * stride + blockIdx.x * blockDim.x + threadIdx.x;
+    int iters_first = -1;
+    bool failed = false;
+    if (e < n) {
+      const unsigned long long v = q.cell[e];
+      const int i = int(v & 0x7fff), j = int((v >> 15) & 0x7fff), k = int((v >> 30) & 0x7fff);
+      c2p_cell<EOS, C2P_FULL>(args_of(int(v >> 45)), eos, i, j, k, iters_first, failed);
+    }
+    const unsigned nfail = __popc(__ballot_sync(0xffffffffu, failed));
+    if (nfail && (threadIdx.x % 32) == 0) {
+      atomicAdd(&status->c2p_fail_count, nfail);
+      atomicOr(&status->error_word, AXB_EW_C2P_FAIL);
+    }
+    if (want_hist && iters_first >= 0)
+      atomicAdd(&s_hist[min(iters_first, 63)], 1u);
+  }
+  if (want_hist) {
+    __syncthreads();
+    for (int t = threadIdx.x; t < 64; t += blockDim.x)
+      if (s_hist[t])
+        atomicAdd(&status->c2p_iter_hist[t], (unsigned long long)s_hist[t]);
+  }
+}
+
+template <class EOS>
+__global__ void __launch_bounds__(128, AXB_C2P_MINB)
+    k_c2p_fast(const C2PBoxArgs a, const EOS eos, const C2PQueue q) {
+  c2p_fast_body<EOS>(a, eos, blockIdx, 0, q);
+}
+
+template <class EOS>
+__global__ void __launch_bounds__(128, AXB_C2P_MINB)
+    k_c2p_deferred(const C2PBoxArgs a, const EOS eos, const C2PQueue q) {
+  c2p_deferred_body([&](int) -> const C2PBoxArgs & { return a; }, eos, q);
+}
+
+// whether a box's extent fits the queue's packing
+inline bool c2p_queue_fits(const axb_box &b) {
+  for (int d = 0; d < 3; ++d)
+    if (b.n[d] + 2 * b.ng + 1 > C2P_QUEUE_MAX_EXTENT)
+      return false;
+  return true;
+}
 } // namespace axb
 
 // ---------------------------------------------------------------------------
@@ -523,6 +667,36 @@ __global__ void __launch_bounds__(128, AXB_C2P_MINB)
     c2p_box_body<EOS>(a, eos, bid);
   });
 }
+template <class EOS>
+__global__ void __launch_bounds__(128, AXB_C2P_MINB)
+    k_c2p_fast_batch(const C2PBoxArgs *args, const TileTable t, unsigned long long *ctr,
+                     const EOS eos, const C2PQueue q) {
+  batch_loop(args, t, ctr, [&](const C2PBoxArgs &a, const uint3 bid, int box) {
+    c2p_fast_body<EOS>(a, eos, bid, box, q);
+  });
+}
+template <class EOS>
+__global__ void __launch_bounds__(128, AXB_C2P_MINB)
+    k_c2p_deferred_batch(const C2PBoxArgs *args, const EOS eos, const C2PQueue q) {
+  c2p_deferred_body([&](int box) -> const C2PBoxArgs & { return args[box]; }, eos, q);
+}
+template <class EOS>
+int launch_c2p_batch_eos(const C2PBoxArgs *a, const TileTable &t, unsigned long long *ctr,
+                         const EOS &eos, int nblocks, unsigned long long *queue,
+                         int deferred_blocks, cudaStream_t s) {
+  if (!queue) {
+    k_c2p_box_batch<<<nblocks, 128, 0, s>>>(a, t, ctr, eos);
+  } else {
+    C2PQueue q;
+    q.count = queue;
+    q.cell = queue + 1;
+    if (cudaMemsetAsync(q.count, 0, sizeof(unsigned long long), s) != cudaSuccess)
+      return AXB_ERR_CUDA;
+    k_c2p_fast_batch<<<nblocks, 128, 0, s>>>(a, t, ctr, eos, q);
+    k_c2p_deferred_batch<<<deferred_blocks, 128, 0, s>>>(a, eos, q);
+  }
+  return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+}
 } // namespace
 
 namespace axb {
@@ -558,19 +732,35 @@ uint3 c2p_grid(int which, const axb_box &b) {
   return make_uint3(unsigned((plane + T - 1) / T), 1, b.n[2] + e);
 }
 
+// `queue` (count, then room for every interior cell of the batch) selects
+// the fast pass + deferred full cascade (Palenzuela first), else the full
+// cascade in one launch.
 int launch_c2p_batch(int which, const void *args, const TileTable &t,
                      unsigned long long *ctr, const axb_eos &eos, DevStatus *status,
-                     int nblocks, cudaStream_t s) {
+                     int nblocks, cudaStream_t s, unsigned long long *queue,
+                     int deferred_blocks) {
   if (t.total == 0)
     return AXB_OK;
   const C2PBoxArgs *a = static_cast<const C2PBoxArgs *>(args);
-  if (which == 0)
+  if (which == 0) {
     k_bstag_batch<<<nblocks, 128, 0, s>>>(a, t, ctr);
-  else if (eos.kind == 1)
-    k_c2p_box_batch<<<nblocks, 128, 0, s>>>(a, t, ctr, tab_for_launch(eos, status));
-  else
-    k_c2p_box_batch<<<nblocks, 128, 0, s>>>(a, t, ctr, eos.ideal);
-  return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+    return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+  }
+  if (eos.kind == 1)
+    return launch_c2p_batch_eos(a, t, ctr, tab_for_launch(eos, status), nblocks, queue,
+                                deferred_blocks, s);
+  return launch_c2p_batch_eos(a, t, ctr, eos.ideal, nblocks, queue, deferred_blocks, s);
+}
+
+// whether a batch can take the fast pass: Palenzuela first, boxes and
+// extents within the queue's packing
+bool c2p_batch_fast_ok(int nbox, const axb_box *boxes, const axb_params *p) {
+  if (p->c2p_prime != AXB_C2P_PALENZUELA || nbox > C2P_QUEUE_MAX_BOXES)
+    return false;
+  for (int b = 0; b < nbox; ++b)
+    if (!c2p_queue_fits(boxes[b]))
+      return false;
+  return true;
 }
 } // namespace axb
 
@@ -599,10 +789,34 @@ AXB_API int axb_con2prim_group(axb_ctx *c, const axb_box *box,
   {
     const dim3 grid((b.n[0] + T - 1) / T, b.n[1], b.n[2]);
     axb_mark(c, AXB_R_C2P, s, true);
-    if (eos->kind == 1)
+    if (a.c2p_prime == AXB_C2P_PALENZUELA && c2p_queue_fits(*box)) {
+      // fast pass + the full cascade on the deferred cells; the queue (all
+      // interior cells at most) comes from the stream-ordered allocator
+      const unsigned long long ncell = (unsigned long long)b.n[0] * b.n[1] * b.n[2];
+      void *buf = nullptr;
+      if (axb_scratch_alloc(c, &buf, (ncell + 1) * sizeof(unsigned long long), s) !=
+          cudaSuccess)
+        return AXB_ERR_CUDA;
+      C2PQueue q;
+      q.count = static_cast<unsigned long long *>(buf);
+      q.cell = q.count + 1;
+      cudaMemsetAsync(q.count, 0, sizeof(unsigned long long), s);
+      int sms = 148;
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+      if (eos->kind == 1) {
+        const EosTab t = tab_for_launch(*eos, a.status);
+        k_c2p_fast<<<grid, T, 0, s>>>(a, t, q);
+        k_c2p_deferred<<<4 * sms, T, 0, s>>>(a, t, q);
+      } else {
+        k_c2p_fast<<<grid, T, 0, s>>>(a, eos->ideal, q);
+        k_c2p_deferred<<<4 * sms, T, 0, s>>>(a, eos->ideal, q);
+      }
+      cudaFreeAsync(buf, s);
+    } else if (eos->kind == 1) {
       k_c2p_box<<<grid, T, 0, s>>>(a, tab_for_launch(*eos, a.status));
-    else
+    } else {
       k_c2p_box<<<grid, T, 0, s>>>(a, eos->ideal);
+    }
     axb_mark(c, AXB_R_C2P, s, false);
   }
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
