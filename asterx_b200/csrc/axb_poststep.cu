@@ -116,6 +116,9 @@ AXB_D void run_solver(int which, const EOS &eos, const C2PBoxArgs &a,
 #ifndef AXB_C2P_MINB
 #define AXB_C2P_MINB 4 // resident CTAs per SM the register budget must allow
 #endif
+#ifndef AXB_C2P_FAST_MINB
+#define AXB_C2P_FAST_MINB 7 // the fast pass: fewer live values, more warps
+#endif
 //
 // MODE C2P_FULL runs the whole cascade.  MODE C2P_FAST (Palenzuela as the
 // first solver) runs the common path only and returns true, having written
@@ -437,7 +440,7 @@ AXB_D void c2p_deferred_body(const ArgsOf &args_of, const EOS &eos, const C2PQue
 }
 
 template <class EOS>
-__global__ void __launch_bounds__(128, AXB_C2P_MINB)
+__global__ void __launch_bounds__(128, AXB_C2P_FAST_MINB)
     k_c2p_fast(const C2PBoxArgs a, const EOS eos, const C2PQueue q) {
   c2p_fast_body<EOS>(a, eos, blockIdx, 0, q);
 }
@@ -668,7 +671,7 @@ __global__ void __launch_bounds__(128, AXB_C2P_MINB)
   });
 }
 template <class EOS>
-__global__ void __launch_bounds__(128, AXB_C2P_MINB)
+__global__ void __launch_bounds__(128, AXB_C2P_FAST_MINB)
     k_c2p_fast_batch(const C2PBoxArgs *args, const TileTable t, unsigned long long *ctr,
                      const EOS eos, const C2PQueue q) {
   batch_loop(args, t, ctr, [&](const C2PBoxArgs &a, const uint3 bid, int box) {
