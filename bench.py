@@ -587,7 +587,10 @@ def amr_bench(args):
     """Batched AMR level: `boxes` boxes (512) with interior edges drawn
     log-uniformly from 16 to 64 per axis, 3 ghosts, the curved-metric physics
     of the 256^3 workload (WENO-Z + HLLE, Palenzuela with Noble backup,
-    Gamma 4/3), each box periodic on itself.  Times SSP-RK3 substeps done
+    Gamma 4/3) in a milder state that a 16-cell box still resolves (Lorentz
+    factor up to 2, magnetisation up to 0.1, no density jumps; the 256^3
+    workload's W <= 10, sigma <= 10 and jumps run away on boxes this small),
+    each box periodic on itself.  Times SSP-RK3 substeps done
     (a) as one axb_substep per box (each phase launched once per box, as the
     reference's driver does) and (b) as axb_batch_substep (one persistent
     launch per phase over all boxes, tuned by the autotuner) replayed from a
@@ -615,7 +618,8 @@ def amr_bench(args):
     skip = {"zvec_x", "zvec_y", "zvec_z", "svec_x", "svec_y", "svec_z", "dBx", "dBy", "dBz"}
     layouts, fields = [], []
     for b, n in enumerate(shapes):
-        L, f = W.curved_box(n=n, ng=3, seed=1000 + b, wmax=10.0, xp=xp)
+        L, f = W.curved_box(n=n, ng=3, seed=1000 + b, wmax=2.0, njumps=0,
+                            sigma=(1e-3, 0.1), xp=xp)
         W.cons_from_prims(L, f, xp=xp)
         W.saved_from_prims(f, xp=xp)
         for name in abi.GF_NAMES:
@@ -710,7 +714,8 @@ def amr_bench(args):
         "ms_per_step": ms_b / sub, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded boxes of the level)",
         "config": {"workload": f"{args.boxes} boxes, edges log-uniform in [16, 64] per axis, "
-                               f"3 ghosts, curved metric, {args.recon}+HLLE, Palenzuela c2p, "
+                               f"3 ghosts, curved metric, W <= 2, sigma <= 0.1, "
+                               f"{args.recon}+HLLE, Palenzuela c2p, "
                                "Gamma=4/3, SSP-RK3; batched persistent launches in a CUDA "
                                "graph vs one launch per box",
                    "boxes": args.boxes, "zones": zones, "recon": args.recon,
