@@ -85,8 +85,11 @@ AXB_D double avg_v2c(const double *__restrict__ f, long long I, long long sy,
 
 AXB_HD double sym_get(const sym3 &m, int p, int q) { return m(p, q); }
 
+#ifndef AXB_SOURCES_SMEM
+#define AXB_SOURCES_SMEM 1
+#endif
 #ifndef AXB_SOURCES_MINB
-#define AXB_SOURCES_MINB 1
+#define AXB_SOURCES_MINB 3
 #endif
 template <int FD>
 AXB_D void sources_body(const RhsArgs &a, const uint3 bid) {
@@ -97,8 +100,21 @@ AXB_D void sources_body(const RhsArgs &a, const uint3 bid) {
     return;
   const long long I = b.at(i, j, k);
   const long long sy = b.sy, sz = b.sz;
-  double d_alp[3], d_beta[3][3];
-  sym3 d_g[3];
+#if AXB_SOURCES_SMEM
+  // the 30 metric derivatives wait in shared memory (one column per thread)
+  // until the stress tensor is formed: in registers they pushed the kernel
+  // to 255 registers and 8 warps per SM
+  __shared__ double s_der[30][128];
+  const int tl = threadIdx.x;
+#define AXB_DALP(d) s_der[(d)][tl]
+#define AXB_DBETA(d, q) s_der[3 + 3 * (d) + (q)][tl]
+#define AXB_DG(d, q) s_der[12 + 6 * (d) + (q)][tl]
+#else
+  double d_alp_r[3], d_beta_r[3][3], d_g_r[3][6];
+#define AXB_DALP(d) d_alp_r[d]
+#define AXB_DBETA(d, q) d_beta_r[d][q]
+#define AXB_DG(d, q) d_g_r[d][q]
+#endif
   double alp, beta[3];
   sym3 g, K;
   {
@@ -106,7 +122,7 @@ AXB_D void sources_body(const RhsArgs &a, const uint3 bid) {
     alp = r.avg;
 #pragma unroll
     for (int d = 0; d < 3; ++d)
-      d_alp[d] = r.d[d];
+      AXB_DALP(d) = r.d[d];
   }
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
@@ -114,21 +130,18 @@ AXB_D void sources_body(const RhsArgs &a, const uint3 bid) {
     beta[q] = r.avg;
 #pragma unroll
     for (int d = 0; d < 3; ++d)
-      d_beta[d][q] = r.d[d];
+      AXB_DBETA(d, q) = r.d[d];
   }
-  double gv[6], dgv[6][3];
+  double gv[6];
 #pragma unroll
   for (int q = 0; q < 6; ++q) {
     const V2C r = v2c_field<FD>(a.g[q], I, b);
     gv[q] = r.avg;
 #pragma unroll
     for (int d = 0; d < 3; ++d)
-      dgv[q][d] = r.d[d];
+      AXB_DG(d, q) = r.d[d];
   }
   g = sym3{gv[0], gv[1], gv[2], gv[3], gv[4], gv[5]};
-#pragma unroll
-  for (int d = 0; d < 3; ++d)
-    d_g[d] = sym3{dgv[0][d], dgv[1][d], dgv[2][d], dgv[3][d], dgv[4][d], dgv[5][d]};
   K.xx = avg_v2c(a.K[0], I, sy, sz);
   K.xy = avg_v2c(a.K[1], I, sy, sz);
   K.xz = avg_v2c(a.K[2], I, sy, sz);
@@ -188,30 +201,37 @@ AXB_D void sources_body(const RhsArgs &a, const uint3 bid) {
   double X[3];
 #pragma unroll
   for (int q = 0; q < 3; ++q)
-    X[q] = -d_alp[q] + 2.0 * shiftk[q];
+    X[q] = -AXB_DALP(q) + 2.0 * shiftk[q];
   double Kt = 0.0;
 #pragma unroll
   for (int p = 0; p < 3; ++p)
 #pragma unroll
     for (int q = 0; q < 3; ++q)
       Kt += K(p, q) * t[p][q];
-  const double tau_source = t00 * (ssk - dot3(beta, d_alp)) + dot3(t0, X) + Kt;
+  const double d_alp3[3] = {AXB_DALP(0), AXB_DALP(1), AXB_DALP(2)};
+  const double tau_source = t00 * (ssk - dot3(beta, d_alp3)) + dot3(t0, X) + Kt;
   double ms[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
+    const sym3 dgd{AXB_DG(d, 0), AXB_DG(d, 1), AXB_DG(d, 2),
+                   AXB_DG(d, 3), AXB_DG(d, 4), AXB_DG(d, 5)};
     double nrm = 0.0, c1 = 0.0, c3 = 0.0;
 #pragma unroll
     for (int p = 0; p < 3; ++p)
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
-        const double dg = d_g[d](p, q);
+        const double dg = dgd(p, q);
         nrm += dg * beta[p] * beta[q];
         c1 += dg * t0[p] * beta[q];
         c3 += t[p][q] * dg;
       }
-    const double c2 = dot3(t0low, d_beta[d]);
-    ms[d] = t00 * (0.5 * nrm - alp * d_alp[d]) + c1 + c2 + 0.5 * c3;
+    const double dbd[3] = {AXB_DBETA(d, 0), AXB_DBETA(d, 1), AXB_DBETA(d, 2)};
+    const double c2 = dot3(t0low, dbd);
+    ms[d] = t00 * (0.5 * nrm - alp * AXB_DALP(d)) + c1 + c2 + 0.5 * c3;
   }
+#undef AXB_DALP
+#undef AXB_DBETA
+#undef AXB_DG
   const double as = alp * sqrt_detg;
   a.rhs[V_DENS][I] = 0.0;
   a.rhs[V_DENT][I] = 0.0;
