@@ -13,6 +13,10 @@ AXB_D void load_pencil(const double *__restrict__ f, long long I, long long s,
     q[m] = __ldg(f + I + (m - N / 2) * s);
 }
 
+AXB_D void prefetch_l2(const double *p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 AXB_D double warp_max(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1)
@@ -147,6 +151,18 @@ AXB_D void flux_status(const RhsArgs &a, double smax, bool bad) {
 #ifndef AXB_FLUX_SMEM_CARRY
 #define AXB_FLUX_SMEM_CARRY 1
 #endif
+#ifndef AXB_FLUX_PREFETCH
+#define AXB_FLUX_PREFETCH 1 // steps of L2 prefetch ahead of the march (0: none)
+#endif
+#ifndef AXB_FLUX_X_PREFETCH
+#define AXB_FLUX_X_PREFETCH 1
+#endif
+#ifndef AXB_FLUX_PF_RECON
+#define AXB_FLUX_PF_RECON 1
+#endif
+#ifndef AXB_FLUX_PF_ACC
+#define AXB_FLUX_PF_ACC 1
+#endif
 
 // ---------------------------------------------------------------------------
 // k_flux_pass (y and z): one thread marches one pencil segment along DIR.
@@ -214,6 +230,44 @@ AXB_D void flux_pass_body(const RhsArgs &a, const EOS &eos, const int &seglen, c
 #define AXB_FPREV(v) Fprev[v]
 #endif
     for (int c = f0 - 1; c <= flast; ++c, I += sd) {
+#if AXB_FLUX_PREFETCH > 0
+      // L2 prefetch of the rows the march first touches AXB_FLUX_PREFETCH
+      // steps ahead: the new stencil row of every reconstructed variable,
+      // the face metric's two vertex rows, the face's staggered B and the
+      // partial divergences (and RHS) it will accumulate into; all of them
+      // within the rows this segment reads anyway
+      if (c + AXB_FLUX_PREFETCH <= flast) {
+        const long long J = I + AXB_FLUX_PREFETCH * sd;
+#if AXB_FLUX_PF_RECON
+#pragma unroll
+        for (int v = 0; v < NREC; ++v)
+          prefetch_l2(fld[v] + J + 2 * sd);
+#endif
+        constexpr int D1 = (DIR + 1) % 3, D2 = (DIR + 2) % 3;
+        const long long so = (D1 == 0) ? b.stride(D2) : b.stride(D1);
+        prefetch_l2(a.alp + J);
+        prefetch_l2(a.alp + J + so);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          prefetch_l2(a.beta[q] + J);
+          prefetch_l2(a.beta[q] + J + so);
+        }
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          prefetch_l2(a.g[q] + J);
+          prefetch_l2(a.g[q] + J + so);
+        }
+        prefetch_l2(a.dBstag[DIR] + J);
+        if (AXB_FLUX_PF_ACC && trans_int) {
+#pragma unroll
+          for (int v = 0; v < NHYDRO; ++v) {
+            prefetch_l2(a.acc[v] + J - sd);
+            if (DIR == 2)
+              prefetch_l2(a.rhs[v] + J - sd);
+          }
+        }
+      }
+#endif
       double lo[NREC], up[NREC];
       recon_cell_all<DIR, RECON>(a, fld, I, sd, lo, up);
       if (c >= f0) {
@@ -287,6 +341,29 @@ AXB_D void flux_x_body(const RhsArgs &a, const EOS &eos, const uint3 bid) {
       const int c = c0 + lane;
       const bool has_cell = c <= clast;
       const long long I = row + c;
+#if AXB_FLUX_X_PREFETCH
+      // L2 prefetch of the next chunk's cells (the lanes cover it): stencil
+      // tops of the reconstructed variables, the four metric rows of the
+      // x faces, the staggered B
+      if (c + 30 <= clast) {
+        const long long J = I + 30;
+#pragma unroll
+        for (int v = 0; v < NREC; ++v)
+          prefetch_l2(fld[v] + J + 2);
+        const long long so[4] = {0, b.sy, b.sz, b.sy + b.sz};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          prefetch_l2(a.alp + J + so[q]);
+#pragma unroll
+          for (int d = 0; d < 3; ++d)
+            prefetch_l2(a.beta[d] + J + so[q]);
+#pragma unroll
+          for (int d = 0; d < 6; ++d)
+            prefetch_l2(a.g[d] + J + so[q]);
+        }
+        prefetch_l2(a.dBstag[0] + J);
+      }
+#endif
       double lo[NREC], up[NREC];
       if (has_cell) {
         recon_cell_all<0, RECON>(a, fld, I, 1, lo, up);
