@@ -522,7 +522,14 @@ namespace axb {
 int launch_rhs_misc(int which, const RhsArgs &a, cudaStream_t s) {
   const BoxDev &b = a.b;
   const int T = 128;
-  if (which <= 1) {
+  if (which <= 1 && AXB_SOURCES_SEG > 1) {
+    const int seg = AXB_SOURCES_SEG;
+    const dim3 grid((b.n[0] + T - 1) / T, b.n[1], (b.n[2] + seg - 1) / seg);
+    if (which == 0)
+      k_sources_column<2><<<grid, T, 0, s>>>(a, seg);
+    else
+      k_sources_column<4><<<grid, T, 0, s>>>(a, seg);
+  } else if (which <= 1) {
     const dim3 grid((b.n[0] + T - 1) / T, b.n[1], b.n[2]);
     if (which == 0)
       k_sources<2><<<grid, T, 0, s>>>(a);
@@ -546,7 +553,12 @@ namespace {
 template <int FD>
 __global__ void __launch_bounds__(128, AXB_SOURCES_MINB)
     k_sources_batch(const RhsArgs *args, const TileTable t, unsigned long long *ctr) {
-  batch_loop(args, t, ctr, [&](const RhsArgs &a, const uint3 bid) { sources_body<FD>(a, bid); });
+  batch_loop(args, t, ctr, [&](const RhsArgs &a, const uint3 bid) {
+    if (AXB_SOURCES_SEG > 1)
+      sources_column<FD>(a, bid, AXB_SOURCES_SEG);
+    else
+      sources_body<FD>(a, bid);
+  });
 }
 __global__ void __launch_bounds__(128) k_aux_batch(const RhsArgs *args, const TileTable t, unsigned long long *ctr) {
   batch_loop(args, t, ctr, [&](const RhsArgs &a, const uint3 bid) { aux_body(a, bid); });
@@ -588,6 +600,9 @@ uint3 rhs_misc_grid(int which, const axb_box &b) {
   const int T = 128;
   const int e = which <= 1 ? 0 : which == 2 ? 5 : 1;
   const long long plane = (long long)(b.n[0] + e) * (b.n[1] + e);
+  if (which <= 1 && AXB_SOURCES_SEG > 1) // z columns of the sources
+    return make_uint3(unsigned((plane + T - 1) / T), 1,
+                      (b.n[2] + AXB_SOURCES_SEG - 1) / AXB_SOURCES_SEG);
   return make_uint3(unsigned((plane + T - 1) / T), 1, b.n[2] + e);
 }
 

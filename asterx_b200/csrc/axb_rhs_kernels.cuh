@@ -154,9 +154,6 @@ AXB_D void flux_status(const RhsArgs &a, double smax, bool bad) {
 #ifndef AXB_FLUX_PREFETCH
 #define AXB_FLUX_PREFETCH 1 // steps of L2 prefetch ahead of the march (0: none)
 #endif
-#ifndef AXB_FLUX_X_PREFETCH
-#define AXB_FLUX_X_PREFETCH 1
-#endif
 #ifndef AXB_FLUX_PF_RECON
 #define AXB_FLUX_PF_RECON 1
 #endif
@@ -341,29 +338,6 @@ AXB_D void flux_x_body(const RhsArgs &a, const EOS &eos, const uint3 bid) {
       const int c = c0 + lane;
       const bool has_cell = c <= clast;
       const long long I = row + c;
-#if AXB_FLUX_X_PREFETCH
-      // L2 prefetch of the next chunk's cells (the lanes cover it): stencil
-      // tops of the reconstructed variables, the four metric rows of the
-      // x faces, the staggered B
-      if (c + 30 <= clast) {
-        const long long J = I + 30;
-#pragma unroll
-        for (int v = 0; v < NREC; ++v)
-          prefetch_l2(fld[v] + J + 2);
-        const long long so[4] = {0, b.sy, b.sz, b.sy + b.sz};
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          prefetch_l2(a.alp + J + so[q]);
-#pragma unroll
-          for (int d = 0; d < 3; ++d)
-            prefetch_l2(a.beta[d] + J + so[q]);
-#pragma unroll
-          for (int d = 0; d < 6; ++d)
-            prefetch_l2(a.g[d] + J + so[q]);
-        }
-        prefetch_l2(a.dBstag[0] + J);
-      }
-#endif
       double lo[NREC], up[NREC];
       if (has_cell) {
         recon_cell_all<0, RECON>(a, fld, I, 1, lo, up);

@@ -92,12 +92,8 @@ AXB_HD double sym_get(const sym3 &m, int p, int q) { return m(p, q); }
 #define AXB_SOURCES_MINB 3
 #endif
 template <int FD>
-AXB_D void sources_body(const RhsArgs &a, const uint3 bid) {
+AXB_D void sources_cell(const RhsArgs &a, const int i, const int j, const int k) {
   const BoxDev &b = a.b;
-  int i, j;
-  const int k = b.ng + bid.z;
-  if (!b.row_ij(b.ng, b.n[0], b.ng, b.n[1], bid, i, j))
-    return;
   const long long I = b.at(i, j, k);
   const long long sy = b.sy, sz = b.sz;
 #if AXB_SOURCES_SMEM
@@ -242,9 +238,70 @@ AXB_D void sources_body(const RhsArgs &a, const uint3 bid) {
   a.rhs[V_DYE][I] = 0.0;
 }
 template <int FD>
+AXB_D void sources_body(const RhsArgs &a, const uint3 bid) {
+  int i, j;
+  const int k = a.b.ng + bid.z;
+  if (!a.b.row_ij(a.b.ng, a.b.n[0], a.b.ng, a.b.n[1], bid, i, j))
+    return;
+  sources_cell<FD>(a, i, j, k);
+}
+
+// A thread walks `seg` cells up a z column (block z = segment), prefetching
+// into L2 the rows the next cell adds: the upper vertex plane of the 16
+// metric fields and the cell's primitives (its lower vertex plane is the
+// current cell's upper one).
+#ifndef AXB_SOURCES_SEG
+#define AXB_SOURCES_SEG 16 // cells per thread along z; 0 or 1: one cell
+#endif
+template <int FD>
+AXB_D void sources_column(const RhsArgs &a, const uint3 bid, const int seg) {
+  const BoxDev &b = a.b;
+  int i, j;
+  if (!b.row_ij(b.ng, b.n[0], b.ng, b.n[1], bid, i, j))
+    return;
+  const int k0 = b.ng + int(bid.z) * seg;
+  const int k1 = min(k0 + seg, b.ng + b.n[2]);
+  for (int k = k0; k < k1; ++k) {
+    if (k + 1 < k1) {
+      const long long J = b.at(i, j, k + 2); // upper vertex plane of cell k+1
+      const long long C = b.at(i, j, k + 1);
+      const long long sy = b.sy;
+      prefetch_l2(a.alp + J);
+      prefetch_l2(a.alp + J + sy);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        prefetch_l2(a.beta[q] + J);
+        prefetch_l2(a.beta[q] + J + sy);
+      }
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        prefetch_l2(a.g[q] + J);
+        prefetch_l2(a.g[q] + J + sy);
+        prefetch_l2(a.K[q] + J);
+        prefetch_l2(a.K[q] + J + sy);
+      }
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        prefetch_l2(a.vel[q] + C);
+        prefetch_l2(a.Bvec[q] + C);
+      }
+      prefetch_l2(a.rho + C);
+      prefetch_l2(a.eps + C);
+      prefetch_l2(a.press + C);
+    }
+    sources_cell<FD>(a, i, j, k);
+  }
+}
+
+template <int FD>
 __global__ void __launch_bounds__(128, AXB_SOURCES_MINB)
     k_sources(const RhsArgs a) {
   sources_body<FD>(a, blockIdx);
+}
+template <int FD>
+__global__ void __launch_bounds__(128, AXB_SOURCES_MINB)
+    k_sources_column(const RhsArgs a, const int seg) {
+  sources_column<FD>(a, blockIdx, seg);
 }
 
 // ---------------------------------------------------------------------------
