@@ -535,12 +535,18 @@ int launch_rhs_misc(int which, const RhsArgs &a, cudaStream_t s) {
       k_sources<2><<<grid, T, 0, s>>>(a);
     else
       k_sources<4><<<grid, T, 0, s>>>(a);
-  } else if (which == 2) {
-    const dim3 grid((b.n[0] + 5 + T - 1) / T, b.n[1] + 5, b.n[2] + 5);
-    k_aux<<<grid, T, 0, s>>>(a);
   } else {
-    const dim3 grid((b.n[0] + 1 + T - 1) / T, b.n[1] + 1, b.n[2] + 1);
-    k_ct_psi<<<grid, T, 0, s>>>(a);
+    // vertex and edge kernels: threads walk the (i, j) plane row after row,
+    // so rows of n+5 or n+1 points do not leave a block mostly idle
+    RhsArgs ap = a;
+    ap.b.packed = 1;
+    const int e = which == 2 ? 5 : 1;
+    const long long plane = (long long)(b.n[0] + e) * (b.n[1] + e);
+    const dim3 grid(unsigned((plane + T - 1) / T), 1, b.n[2] + e);
+    if (which == 2)
+      k_aux<<<grid, T, 0, s>>>(ap);
+    else
+      k_ct_psi<<<grid, T, 0, s>>>(ap);
   }
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
 }

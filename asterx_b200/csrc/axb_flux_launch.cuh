@@ -23,12 +23,17 @@ int launch_flux_pass_eos(int dir, const RhsArgs &a, const EOS &eos, int seglen,
   }
   const int T0 = 0, T1 = dir == 2 ? 1 : 2;
   const dim3 block(32, 4);
-  const dim3 grid((b.n[T0] + 2 + 31) / 32, (b.n[T1] + 2 + 3) / 4,
-                  (b.n[dir] + seglen - 1) / seglen);
+  // the threads walk the transverse plane [ng-1, ng+n]^2 row after row
+  // (as in the batched kernels), so the 2 extra columns of the plane do
+  // not leave most of a warp idle
+  RhsArgs ap = a;
+  ap.b.packed = 1;
+  const long long plane = (long long)(b.n[T0] + 2) * (b.n[T1] + 2);
+  const dim3 grid(unsigned((plane + 127) / 128), 1, (b.n[dir] + seglen - 1) / seglen);
   if (dir == 1)
-    k_flux_pass<1, RECON, EOS><<<grid, block, 0, s>>>(a, eos, seglen);
+    k_flux_pass<1, RECON, EOS><<<grid, block, 0, s>>>(ap, eos, seglen);
   else
-    k_flux_pass<2, RECON, EOS><<<grid, block, 0, s>>>(a, eos, seglen);
+    k_flux_pass<2, RECON, EOS><<<grid, block, 0, s>>>(ap, eos, seglen);
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
 }
 

@@ -784,9 +784,13 @@ AXB_API int axb_con2prim_group(axb_ctx *c, const axb_box *box,
   const BoxDev &b = a.b;
   const int T = 128;
   {
-    const dim3 grid((b.n[0] + 2 + T - 1) / T, b.n[1] + 2, b.n[2] + 2);
+    // the (i, j) plane walked row after row (rows of n+2 faces)
+    C2PBoxArgs ap = a;
+    ap.b.packed = 1;
+    const long long plane = (long long)(b.n[0] + 2) * (b.n[1] + 2);
+    const dim3 grid(unsigned((plane + T - 1) / T), 1, b.n[2] + 2);
     axb_mark(c, AXB_R_BSTAG, s, true);
-    k_bstag<<<grid, T, 0, s>>>(a);
+    k_bstag<<<grid, T, 0, s>>>(ap);
     axb_mark(c, AXB_R_BSTAG, s, false);
   }
   {
