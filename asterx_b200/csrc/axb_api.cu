@@ -491,7 +491,7 @@ AXB_API int axb_rhs_group(axb_ctx *c, const axb_box *box, const axb_fields *f,
     return AXB_ERR_UNSUPPORTED;
   cudaStream_t s = (cudaStream_t)stream;
 #ifndef AXB_FLUX_SEGLEN
-#define AXB_FLUX_SEGLEN 32 // cells per y/z pencil segment (one thread each)
+#define AXB_FLUX_SEGLEN 16 // cells per y/z pencil segment (one thread each)
 #endif
   const int seglen = AXB_FLUX_SEGLEN;
   axb_mark(c, AXB_R_SOURCES, s, true);
