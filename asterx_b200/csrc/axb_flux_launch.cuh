@@ -23,6 +23,21 @@ int launch_flux_pass_eos(int dir, const RhsArgs &a, const EOS &eos, int seglen,
   }
   const int T0 = 0, T1 = dir == 2 ? 1 : 2;
   const dim3 block(32, 4);
+  // Thread layout: 32 columns x 4 rows of the transverse plane per block,
+  // or the plane walked row after row (no lane idle on the n+2-wide rows).
+  // Measured at 256^3: the packed walk is 7-9 % faster for WENO-Z and PPM,
+  // while MP5 is 30 % faster on the 32 x 4 blocks (each block's four rows
+  // share the face metric's second vertex row in L1).
+  constexpr bool packed = RECON != AXB_RECON_MP5;
+  if (!packed) {
+    const dim3 grid((b.n[T0] + 2 + 31) / 32, (b.n[T1] + 2 + 3) / 4,
+                    (b.n[dir] + seglen - 1) / seglen);
+    if (dir == 1)
+      k_flux_pass<1, RECON, EOS><<<grid, block, 0, s>>>(a, eos, seglen);
+    else
+      k_flux_pass<2, RECON, EOS><<<grid, block, 0, s>>>(a, eos, seglen);
+    return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+  }
   // the threads walk the transverse plane [ng-1, ng+n]^2 row after row
   // (as in the batched kernels), so the 2 extra columns of the plane do
   // not leave most of a warp idle
