@@ -63,6 +63,10 @@ C2P = {"none": 0, "noble": 1, "palenzuela": 2, "entropy": 3}
 
 # c2p cell flags (AsterX/src/con2prim.cxx:27-35)
 C2P_INIT, C2P_PRIME, C2P_SECOND, C2P_ENTROPY, C2P_ATMO, C2P_AVG, C2P_FAIL = range(7)
+# outer-boundary rules (axb_bc)
+BC_PERIODIC, BC_NEUMANN, BC_LINEAR = 0, 1, 2
+# device error-word bits (AXB_EW_* in include/asterx_b200.h)
+EW_NAN_FLUX, EW_NAN_RHS, EW_C2P_FAIL, EW_ROOT_CAP, EW_QUEUE_TIMEOUT = 1, 2, 4, 8, 16
 
 
 class Box(C.Structure):

@@ -32,6 +32,19 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
 FILE_FLAGS = {"axb_poststep.cu": ["-fmad=false"]}
 
 
+def _includes(path, seen=None):
+    """The quoted #include files a source reaches, transitively."""
+    import re
+    seen = set() if seen is None else seen
+    with open(path) as fh:
+        for m in re.finditer(r'^\s*#\s*include\s+"([^"]+)"', fh.read(), re.M):
+            dep = os.path.normpath(os.path.join(os.path.dirname(path), m.group(1)))
+            if os.path.exists(dep) and dep not in seen:
+                seen.add(dep)
+                _includes(dep, seen)
+    return seen
+
+
 def _stale(target, deps):
     if not os.path.exists(target):
         return True
@@ -53,14 +66,12 @@ def build(force=False, verbose=False, extra=()):
     objdir = os.path.join(LIBDIR, "obj")
     os.makedirs(objdir, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
-    headers = (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.hxx"))
-               + [os.path.join(REPO, "include", "asterx_b200.h")])
     jobs = []
     objs = []
     for s in srcs:
         o = os.path.join(objdir, os.path.basename(s)[:-3] + ".o")
         objs.append(o)
-        if force or _stale(o, [s, *headers, os.path.abspath(__file__)]):
+        if force or _stale(o, [s, *_includes(s), os.path.abspath(__file__)]):
             jobs.append((s, o))
     if jobs:
         with cf.ThreadPoolExecutor(max_workers=min(8, len(jobs))) as ex:

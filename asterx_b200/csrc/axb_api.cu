@@ -372,17 +372,29 @@ int fill_rhs_args(axb_ctx *c, const axb_box *box, const axb_fields *f,
     return rc;
   if (!f || !p)
     return AXB_ERR_ARG;
-  if (p->recon_type != AXB_RECVAR_V || p->use_uct ||
+  if (p->recon_type < AXB_RECVAR_V || p->recon_type > AXB_RECVAR_S || p->use_uct ||
       p->reconstruction_method == AXB_RECON_EPPM ||
       !(p->local_spatial_order == 2 || p->local_spatial_order == 4))
     return AXB_ERR_UNSUPPORTED;
   if (p->local_spatial_order == 4 && box->ng < 3)
     return AXB_ERR_GHOSTS;
   a.b = make_box(*box);
+  // no fused stage unless the caller sets one up (axb_substep)
+  a.fuse_stage = 0;
+  a.st_alpha = a.st_beta = a.st_gdt = 0.0;
+  for (int v = 0; v < 11; ++v) {
+    a.st_un[v] = nullptr;
+    a.st_uk[v] = nullptr;
+  }
   a.rho = GFP(rho);
   a.vel[0] = GFP(velx);
   a.vel[1] = GFP(vely);
   a.vel[2] = GFP(velz);
+  a.recvar = p->recon_type;
+  for (int q = 0; q < 3; ++q)
+    a.recv[q] = p->recon_type == AXB_RECVAR_Z   ? f->gf[AXB_GF_zvec_x + q]
+                : p->recon_type == AXB_RECVAR_S ? f->gf[AXB_GF_svec_x + q]
+                                                : a.vel[q];
   a.eps = GFP(eps);
   a.press = GFP(press);
   a.temperature = GFP(temperature);
@@ -455,6 +467,9 @@ int fill_rhs_args(axb_ctx *c, const axb_box *box, const axb_fields *f,
   for (int q = 0; q < 7; ++q)
     if (!a.acc[q] || !a.rhs[q] || !a.aux[q])
       return AXB_ERR_ARG;
+  for (int q = 0; q < 3; ++q)
+    if (!a.recv[q])
+      return AXB_ERR_ARG;
   return AXB_OK;
 }
 } // namespace
@@ -471,19 +486,41 @@ int launch_flux_pass(int dir, int recon, const RhsArgs &a, const axb_eos &eos,
 }
 } // namespace axb
 
-// AsterX_RHSGroup (AsterX/schedule.ccl:169-228): AsterX_Fluxes
-// (fluxes.cxx:828-878), AsterX_SourceTerms (source.cxx:170-185) and
-// AsterX_RHS (rhs.cxx:18-253) on one box.  Writes densrhs..DEntrhs,
-// Avec_*_rhs and Psi_rhs on the interior; uses the scratch grid functions
-// acc_*, fxBy..fzBy and Fx..G.  Asynchronous on `stream`.
-AXB_API int axb_rhs_group(axb_ctx *c, const axb_box *box, const axb_fields *f,
-                          const axb_params *p, const axb_eos *eos, void *stream) {
+namespace {
+// The stage update a substep fuses into its RHS group.
+struct StageFuse {
+  const axb_fields *un;
+  double alpha, beta, gdt;
+};
+
+int rhs_group_run(axb_ctx *c, const axb_box *box, const axb_fields *f,
+                  const axb_params *p, const axb_eos *eos, void *stream,
+                  const StageFuse *fuse, const int *bc = nullptr) {
   if (!c || !eos)
     return AXB_ERR_ARG;
   RhsArgs a;
   int rc = fill_rhs_args(c, box, f, p, a);
   if (rc)
     return rc;
+  a.fuse_stage = 0;
+  if (fuse) {
+    static const int evolved[11] = {AXB_GF_dens,   AXB_GF_momx,   AXB_GF_momy,
+                                    AXB_GF_momz,   AXB_GF_tau,    AXB_GF_DYe,
+                                    AXB_GF_DEnt,   AXB_GF_Avec_x, AXB_GF_Avec_y,
+                                    AXB_GF_Avec_z, AXB_GF_Psi};
+    if (!fuse->un)
+      return AXB_ERR_ARG;
+    for (int v = 0; v < 11; ++v) {
+      a.st_un[v] = fuse->un->gf[evolved[v]];
+      a.st_uk[v] = f->gf[evolved[v]];
+      if (!a.st_un[v] || !a.st_uk[v])
+        return AXB_ERR_ARG;
+    }
+    a.fuse_stage = 1;
+    a.st_alpha = fuse->alpha;
+    a.st_beta = fuse->beta;
+    a.st_gdt = fuse->gdt;
+  }
   // the tabulated EOS has no eps(rho, press) (the reference asserts,
   // eos_3p_tabulated3d.hxx:259-269): its fluxes need the reconstructed
   // temperature
@@ -506,15 +543,48 @@ AXB_API int axb_rhs_group(axb_ctx *c, const axb_box *box, const axb_fields *f,
     if (rc)
       return rc;
   }
+  // physical outer boundaries: the face B fluxes of the ghost layers by the
+  // boundary rule, as the reference SYNCs its face fluxes
+  static const int bflux_ids[6] = {AXB_GF_fxBy, AXB_GF_fxBz, AXB_GF_fyBx,
+                                   AXB_GF_fyBz, AXB_GF_fzBx, AXB_GF_fzBy};
+  static const int aux_ids[7] = {AXB_GF_Fx, AXB_GF_Fy, AXB_GF_Fz, AXB_GF_Fbetax,
+                                 AXB_GF_Fbetay, AXB_GF_Fbetaz, AXB_GF_G};
+  if (bc && (rc = axb_fill_boundary(c, box, f, bflux_ids, 6, bc, stream)))
+    return rc;
   axb_mark(c, AXB_R_AUX, s, true);
   rc = launch_rhs_misc(2, a, s);
   axb_mark(c, AXB_R_AUX, s, false);
   if (rc)
     return rc;
+  if (bc && (rc = axb_fill_boundary(c, box, f, aux_ids, 7, bc, stream)))
+    return rc;
   axb_mark(c, AXB_R_CT, s, true);
   rc = launch_rhs_misc(3, a, s);
   axb_mark(c, AXB_R_CT, s, false);
   return rc;
+}
+} // namespace
+
+// AsterX_RHSGroup (AsterX/schedule.ccl:169-228): AsterX_Fluxes
+// (fluxes.cxx:828-878), AsterX_SourceTerms (source.cxx:170-185) and
+// AsterX_RHS (rhs.cxx:18-253) on one box.  Writes densrhs..DEntrhs,
+// Avec_*_rhs and Psi_rhs on the interior; uses the scratch grid functions
+// acc_*, fxBy..fzBy and Fx..G.  Asynchronous on `stream`.
+AXB_API int axb_rhs_group(axb_ctx *c, const axb_box *box, const axb_fields *f,
+                          const axb_params *p, const axb_eos *eos, void *stream) {
+  return rhs_group_run(c, box, f, p, eos, stream, nullptr);
+}
+
+// AsterX_RHSGroup on a box with physical outer boundaries: the face B
+// fluxes and the vertex auxiliaries of the ghost points come from the
+// boundary rule applied to their interior values (the reference computes
+// them on the interior and SYNCs them, AsterX/schedule.ccl:174-195).
+AXB_API int axb_rhs_group_bc(axb_ctx *c, const axb_box *box, const axb_fields *f,
+                             const axb_params *p, const axb_eos *eos, const int bc[6],
+                             void *stream) {
+  if (!bc)
+    return AXB_ERR_ARG;
+  return rhs_group_run(c, box, f, p, eos, stream, nullptr, bc);
 }
 
 namespace axb {
@@ -676,8 +746,9 @@ extern "C" int axb_rk_stage(axb_ctx *, const axb_box *, const axb_fields *,
 extern "C" int axb_sync_periodic(axb_ctx *, const axb_box *, const axb_fields *,
                                  const int *, int, void *);
 
-// One Runge-Kutta substep of one box: the RHS group, the stage update
-//   U_k <- alpha U_n + beta U_k + gamma dt RHS(U_k),
+// One Runge-Kutta substep of one box: the RHS group and the stage update
+//   U_k <- alpha U_n + beta U_k + gamma dt RHS(U_k)
+// (fused: the RHS grid functions are not written),
 // a periodic ghost fill of the evolved variables (when `periodic`), the
 // post-step group (curl A, dB, con2prim) and a periodic ghost fill of the
 // primitives.  `f` holds U_k (updated in place), the primitives and the
@@ -687,10 +758,13 @@ AXB_API int axb_substep(axb_ctx *c, const axb_box *box, const axb_fields *f,
                         const axb_fields *fn, const axb_params *p,
                         const axb_eos *eos, double alpha, double beta,
                         double gamma, double dt, int periodic, void *stream) {
-  int rc = axb_rhs_group(c, box, f, p, eos, stream);
+  // the RHS group with the stage update fused into its last kernels: the
+  // z flux pass updates the hydro variables, the CT kernel A and Psi, and
+  // no RHS grid function is stored (the same bits as axb_rhs_group followed
+  // by axb_rk_stage)
+  const StageFuse fuse{fn, alpha, beta, gamma * dt};
+  int rc = rhs_group_run(c, box, f, p, eos, stream, &fuse);
   if (rc)
-    return rc;
-  if ((rc = axb_rk_stage(c, box, f, fn, f, f, alpha, beta, gamma, dt, stream)))
     return rc;
   if (periodic) {
     static const int evolved[] = {AXB_GF_dens,   AXB_GF_momx,   AXB_GF_momy,
@@ -703,11 +777,19 @@ AXB_API int axb_substep(axb_ctx *c, const axb_box *box, const axb_fields *f,
   if ((rc = axb_con2prim_group(c, box, f, p, eos, stream)))
     return rc;
   if (periodic) {
-    static const int prims[] = {AXB_GF_rho,   AXB_GF_velx,    AXB_GF_vely,
-                                AXB_GF_velz,  AXB_GF_eps,     AXB_GF_press,
-                                AXB_GF_temperature, AXB_GF_Ye, AXB_GF_entropy,
-                                AXB_GF_Bvecx, AXB_GF_Bvecy,   AXB_GF_Bvecz};
-    if ((rc = axb_sync_periodic(c, box, f, prims, 12, stream)))
+    // the primitives, and the zvec or svec the fluxes reconstruct instead
+    // of the velocity when recon_type asks for one of them
+    int prims[15] = {AXB_GF_rho,   AXB_GF_velx,    AXB_GF_vely,
+                     AXB_GF_velz,  AXB_GF_eps,     AXB_GF_press,
+                     AXB_GF_temperature, AXB_GF_Ye, AXB_GF_entropy,
+                     AXB_GF_Bvecx, AXB_GF_Bvecy,   AXB_GF_Bvecz};
+    int nprims = 12;
+    if (p->recon_type == AXB_RECVAR_Z || p->recon_type == AXB_RECVAR_S) {
+      const int first = p->recon_type == AXB_RECVAR_Z ? AXB_GF_zvec_x : AXB_GF_svec_x;
+      for (int q = 0; q < 3; ++q)
+        prims[nprims++] = first + q;
+    }
+    if ((rc = axb_sync_periodic(c, box, f, prims, nprims, stream)))
       return rc;
   }
   return AXB_OK;

@@ -28,7 +28,7 @@ int batch_rhs_setup(axb_ctx *c, int nbox, const axb_box *boxes, const axb_fields
 int batch_c2p_setup(axb_ctx *c, int nbox, const axb_box *boxes, const axb_fields *f,
                     const axb_params *p, const axb_eos *eos, void **out);
 int batch_rk_setup(int nbox, const axb_box *boxes, const axb_fields *f, const axb_fields *fn,
-                   void **stage_args, void **sync_evolved, void **sync_prims);
+                   int recvar, void **stage_args, void **sync_evolved, void **sync_prims);
 uint3 rhs_misc_grid(int which, const axb_box &b);
 uint3 flux_grid(int dir, const axb_box &b, int seglen);
 uint3 stage_grid(const axb_box &b);
@@ -248,7 +248,8 @@ AXB_API int axb_batch_create(axb_ctx *c, int nbox, const axb_box *boxes,
   if (!rc)
     rc = batch_c2p_setup(c, nbox, boxes, fields, p, eos, &B->c2p_args);
   if (!rc)
-    rc = batch_rk_setup(nbox, boxes, fields, fields_n, &B->stage_args, &B->sync_e, &B->sync_p);
+    rc = batch_rk_setup(nbox, boxes, fields, fields_n, p->recon_type, &B->stage_args,
+                        &B->sync_e, &B->sync_p);
   if (!rc)
     rc = make_table(bx, g_sources, 0, B->tab[P_SOURCES]);
   if (!rc)

@@ -67,12 +67,21 @@ AXB_API int axb_rhs_group_noalloc(const axb_box *box, const axb_fields *fields,
                                   void *stream) {
   if (!box || !fields || !params || !eos)
     return AXB_ERR_ARG;
-  if (box->ng < 0 || box->n[2] < 0 || box->sz < 1)
+  // sizes are range-checked before any arithmetic on them (axb_rhs_group
+  // checks the box again in full)
+  constexpr int64_t kMaxExtent = int64_t(1) << 15;
+  for (int d = 0; d < 3; ++d)
+    if (box->n[d] < 1 || box->n[d] > kMaxExtent)
+      return AXB_ERR_ARG;
+  if (box->ng < 0 || box->ng > kMaxExtent || box->sy < 1 || box->sz < 1)
     return AXB_ERR_ARG;
+  if (box->sz > (int64_t)kScratchDoubles)
+    return AXB_ERR_TOO_LARGE;
   // one scratch grid function = the box's whole index space, rounded up to
   // 32 doubles so every slice starts on a 256-byte boundary
-  const size_t per = ((size_t)box->sz * (size_t)(box->n[2] + 2 * box->ng + 1) + 31) / 32 * 32;
-  if (per * kNScratch > kScratchDoubles)
+  const size_t planes = (size_t)box->n[2] + 2 * (size_t)box->ng + 1;
+  const size_t per = ((size_t)box->sz * planes + 31) / 32 * 32;
+  if (per > kScratchDoubles / kNScratch)
     return AXB_ERR_TOO_LARGE;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess)

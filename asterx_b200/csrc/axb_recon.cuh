@@ -34,9 +34,10 @@ struct ReconParams {
 AXB_HD int sgn_int(double v) { return (0.0 < v) - (v < 0.0); }
 
 AXB_HD double minmod2(double x, double y) {
-  if (signbit(x) != signbit(y))
-    return 0.0;
-  return fabs(x) < fabs(y) ? x : y;
+  // selects only (no branch): 0 for opposite signs, else the smaller
+  // magnitude (y on ties), as ReconX's minmod
+  const double m = fabs(x) < fabs(y) ? x : y;
+  return signbit(x) != signbit(y) ? 0.0 : m;
 }
 
 AXB_HD double monocentral2(double x, double y) {
@@ -183,16 +184,47 @@ AXB_HD CellLoUp recon_wenoz(const double q[5], double weno_eps) {
   return {var_m, var_p};
 }
 
+// Products and sums rounded one by one, never fused into a multiply-add
+// (the reference's CPU build rounds every operation as written): for the
+// values that feed a branch decision, so that both builds take the same
+// branch.
+AXB_HD double mul_rn(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dmul_rn(a, b);
+#else
+  return a * b;
+#endif
+}
+AXB_HD double add_rn(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dadd_rn(a, b);
+#else
+  return a + b;
+#endif
+}
+
+#ifndef AXB_MP5_SELECT
+#define AXB_MP5_SELECT 1
+#endif
+
 // MP5 interface value of the middle cell towards u_p1's side.
 AXB_HD double mp5_one(double gf_Imm, double gf_Im, double gf_I, double gf_Ip,
                       double gf_Ipp, double alpha) {
-  // (kept as the reference's division: ul feeds the early-accept test)
-  const double ul = (2 * gf_Imm - 13 * gf_Im + 47 * gf_I + 27 * gf_Ip - 3 * gf_Ipp) / 60.0;
+  // ul feeds the early-accept test: the reference's division, and its
+  // products and sums rounded one by one, left to right
+  const double ul =
+      add_rn(add_rn(add_rn(add_rn(mul_rn(2, gf_Imm), -mul_rn(13, gf_Im)), mul_rn(47, gf_I)),
+                    mul_rn(27, gf_Ip)),
+             -mul_rn(3, gf_Ipp)) /
+      60.0;
   const double deltam = gf_I - gf_Im;
   const double deltap = gf_Ip - gf_I;
   const double ump = gf_I + minmod2(deltap, alpha * deltam);
-  if ((ul - gf_I) * (ul - ump) <= 1.0e-10)
+  const bool accept = mul_rn(ul - gf_I, ul - ump) <= 1.0e-10;
+#if !AXB_MP5_SELECT
+  if (accept)
     return ul;
+#endif
   const double dm = gf_Imm + gf_I - 2 * gf_Im;
   const double d = gf_Im + gf_Ip - 2 * gf_I;
   const double dp = gf_I + gf_Ipp - 2 * gf_Ip;
@@ -205,7 +237,13 @@ AXB_HD double mp5_one(double gf_Imm, double gf_Im, double gf_I, double gf_Ip,
   const double umin = fmax(fmin(gf_I, fmin(gf_Ip, umd)), fmin(gf_I, fmin(uul, ulc)));
   const double umax = fmin(fmax(gf_I, fmax(gf_Ip, umd)), fmax(gf_I, fmax(uul, ulc)));
   // median(ul, umin, umax) = ul + minmod(umin - ul, umax - ul)
+#if AXB_MP5_SELECT
+  // both results computed, the early accept a select: no lane of a warp
+  // waits on another lane's limiter branch
+  return accept ? ul : ul + minmod2(umin - ul, umax - ul);
+#else
   return ul + minmod2(umin - ul, umax - ul);
+#endif
 }
 
 AXB_HD CellLoUp recon_mp5(const double q[5], double alpha) {

@@ -27,6 +27,11 @@ struct RhsArgs {
   // temperature when rec_temp, else pressure (fluxes.cxx:257-355)
   const double *temperature, *thermo;
   int rec_temp;
+  // the velocity-like variable reconstructed at the faces (recon_type,
+  // fluxes.cxx:396-505): vel^i (v_vec), zvec^i = W v^i (z_vec) or
+  // svec^i = rho h W^2 v^i (s_vec)
+  const double *recv[3];
+  int recvar;
   const double *dBstag[3];
   const double *alp, *beta[3], *g[6], *K[6];
   const double *Avec[3], *Psi;
@@ -35,11 +40,28 @@ struct RhsArgs {
   double *bflux[6]; // fxBy fxBz fyBx fyBz fzBx fzBy
   double *aux[7];   // Fx Fy Fz Fbetax Fbetay Fbetaz G
   double *Arhs[3], *Psi_rhs;
+  // The stage update fused into the group (axb_substep): with fuse_stage
+  // the z flux pass and the CT kernel write
+  //   U_k <- st_alpha U_n + st_beta U_k + st_gdt RHS
+  // for the 11 evolved variables (dens, mom, tau, DYe, DEnt, Avec, Psi; U_k
+  // updated in place) instead of storing the RHS grid functions
+  int fuse_stage;
+  double st_alpha, st_beta, st_gdt;
+  const double *st_un[11];
+  double *st_uk[11];
   ReconParams rp;
   int recon_lo, flux_type, gauge, fd_order, write_bflux;
   double lorenz_damp_fac;
   DevStatus *status;
 };
+
+// The stage combine U_k <- alpha U_n + beta U_k + gdt RHS with an explicit
+// rounding order, so that the fused and the separate stage update give the
+// same bits.
+AXB_D double stage_combine(double alpha, double un, double beta, double uk, double gdt,
+                           double rhs) {
+  return fma(gdt, rhs, fma(beta, uk, alpha * un));
+}
 
 // ---------------------------------------------------------------------------
 // face metric: v2f averages of the vertex metric (AsterUtils aster_interp.hxx
@@ -102,14 +124,16 @@ struct SideOut {
   double lam_p, lam_m; // the two distinct fast speeds of this side
 };
 
-// Per-side physics of CalcFlux (fluxes.cxx:357-654) for a v_vec state.
+// Per-side physics of CalcFlux (fluxes.cxx:357-654).
 // With rec_temp, r[R_PRESS] holds the reconstructed temperature and eps and
 // press come from (rho, T, Ye) (fluxes.cxx:297-304); otherwise eps comes
 // from (rho, press, Ye) (:346-353; the temperature computed there is unused
 // and only the tabulated EOS, which cannot take this route, would clamp eps).
+// r[R_VX..R_VZ] hold the reconstructed vel^i, zvec^i or svec^i (recvar):
+// W and v^i follow from them as in fluxes.cxx:396-505.
 template <int DIR, class EOS>
 AXB_D void side_physics(const FaceMetric &m, const double *r, double Bdir,
-                        const EOS &eos, int rec_temp, SideOut &o) {
+                        const EOS &eos, int rec_temp, int recvar, SideOut &o) {
   constexpr int D1 = (DIR + 1) % 3, D2 = (DIR + 2) % 3;
   const double rho = r[R_RHO], ent = r[R_ENT], ye = r[R_YE];
   double eps, press;
@@ -120,18 +144,48 @@ AXB_D void side_physics(const FaceMetric &m, const double *r, double Bdir,
     press = r[R_PRESS];
     eps = eos.eps_from_valid_rho_press_ye(rho, press, ye);
   }
-  const double vel[3] = {r[R_VX], r[R_VY], r[R_VZ]};
   double B[3];
   B[DIR] = Bdir;
   B[D1] = r[R_B1];
   B[D2] = r[R_B2];
-  double vlow[3];
-  lower3(m.g, vel, vlow);
-  // W = rsqrt(1 - v^2) and 1/W = (1 - v^2) W, used in four places as a
-  // product (last-ulp differences from the reference's divisions by W)
-  const double omv2 = 1 - dot3(vlow, vel);
-  const double W = rsqrt(omv2);
-  const double iW = omv2 * W;
+  double vel[3], vlow[3], W, iW;
+  if (recvar == AXB_RECVAR_V) {
+    vel[0] = r[R_VX];
+    vel[1] = r[R_VY];
+    vel[2] = r[R_VZ];
+    lower3(m.g, vel, vlow);
+    // W = rsqrt(1 - v^2) and 1/W = (1 - v^2) W, used in four places as a
+    // product (last-ulp differences from the reference's divisions by W)
+    const double omv2 = 1 - dot3(vlow, vel);
+    W = rsqrt(omv2);
+    iW = omv2 * W;
+  } else {
+    // z_vec: W = sqrt(1 + z_i z^i), v^i = z^i / W (fluxes.cxx:453-463);
+    // s_vec: W^2 = 1/2 + sqrt(1/4 + s_i s^i / (rho h)^2),
+    // v^i = s^i / (W^2 rho h) (:492-504).  The divisions by W (and rho h)
+    // are products with one reciprocal here, and for z_vec 1/W is one rsqrt
+    // with W = (1 + z^2) / W (last-ulp differences).
+    const double q[3] = {r[R_VX], r[R_VY], r[R_VZ]};
+    double qlow[3];
+    lower3(m.g, q, qlow);
+    const double qq = dot3(qlow, q);
+    double f;
+    if (recvar == AXB_RECVAR_Z) {
+      const double opz2 = 1 + qq;
+      iW = rsqrt(opz2);
+      W = opz2 * iW;
+      f = iW;
+    } else {
+      const double rhoh = rho + rho * eps + press;
+      W = sqrt(0.5 + sqrt(0.25 + qq / rhoh / rhoh));
+      iW = 1 / W;
+      f = iW * iW / rhoh;
+    }
+    for (int i = 0; i < 3; ++i) {
+      vel[i] = q[i] * f;
+      vlow[i] = qlow[i] * f;
+    }
+  }
   double vt[3];
   for (int i = 0; i < 3; ++i)
     vt[i] = m.alp * vel[i] - m.beta[i];

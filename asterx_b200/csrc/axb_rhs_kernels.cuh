@@ -42,7 +42,7 @@ AXB_D void recon_cell_all(const RhsArgs &a, const double *const (&fld)[NREC],
     if (v == R_PRESS && !a.rec_temp) {
 #pragma unroll
       for (int m = 0; m < 5; ++m) q[m] = pr[m];
-    } else if (v == R_VX + DIR) {
+    } else if (v == R_VX + DIR && a.recvar == AXB_RECVAR_V) {
 #pragma unroll
       for (int m = 0; m < 5; ++m) q[m] = vd[m];
     } else {
@@ -87,8 +87,8 @@ AXB_D void face_fluxes(const RhsArgs &a, const EOS &eos,
   const FaceMetric m = face_metric<DIR>(a, I);
   const double Bdir = __ldg(a.dBstag[DIR] + I) * m.isqrtg;
   SideOut sL, sR;
-  side_physics<DIR>(m, L, Bdir, eos, a.rec_temp, sL);
-  side_physics<DIR>(m, R, Bdir, eos, a.rec_temp, sR);
+  side_physics<DIR>(m, L, Bdir, eos, a.rec_temp, a.recvar, sL);
+  side_physics<DIR>(m, R, Bdir, eos, a.rec_temp, a.recvar, sR);
   const double cmax = fmax(0.0, fmax(fmax(sL.lam_p, sL.lam_m), fmax(sR.lam_p, sR.lam_m)));
   const double cmin = fmin(0.0, fmin(fmin(sL.lam_p, sL.lam_m), fmin(sR.lam_p, sR.lam_m)));
   smax = fmax(smax, fmax(cmax, -cmin));
@@ -117,29 +117,43 @@ AXB_D void face_fluxes(const RhsArgs &a, const EOS &eos,
 
 // Fold F(face c+1) - F(face c) into the partial divergence of cell c (at I),
 // in the reference's summation order (rhs.cxx:188-207): x writes, y adds,
-// z adds and forms the RHS.
+// z adds and forms the RHS.  Returns true when the z pass formed a
+// non-finite hydro RHS (the reference asserts there, rhs.cxx:199-206).
 template <int DIR>
-AXB_D void fold_divergence(const RhsArgs &a, long long I, double idxd,
+AXB_D bool fold_divergence(const RhsArgs &a, long long I, double idxd,
                            const double (&Fhi)[NHYDRO], const double (&Flo)[NHYDRO]) {
+  bool bad = false;
 #pragma unroll
   for (int v = 0; v < NHYDRO; ++v) {
     const double dF = Fhi[v] - Flo[v];
-    if (DIR == 0)
+    if (DIR == 0) {
       a.acc[v][I] = idxd * dF;
-    else if (DIR == 1)
+    } else if (DIR == 1) {
       a.acc[v][I] = a.acc[v][I] + idxd * dF;
-    else
-      a.rhs[v][I] = a.rhs[v][I] + (-(a.acc[v][I] + idxd * dF));
+    } else {
+      const double r = a.rhs[v][I] + (-(a.acc[v][I] + idxd * dF));
+      if (a.fuse_stage)
+        a.st_uk[v][I] = stage_combine(a.st_alpha, a.st_un[v][I], a.st_beta,
+                                      a.st_uk[v][I], a.st_gdt, r);
+      else
+        a.rhs[v][I] = r;
+      bad |= !isfinite(r);
+    }
   }
+  return bad;
 }
 
-AXB_D void flux_status(const RhsArgs &a, double smax, bool bad) {
+AXB_D void flux_status(const RhsArgs &a, double smax, bool bad, bool bad_rhs = false) {
   // characteristic-speed maximum: warp shuffle, one atomic per warp
   smax = warp_max(smax);
-  if ((threadIdx.x + threadIdx.y * blockDim.x) % 32 == 0)
+  const bool lead = (threadIdx.x + threadIdx.y * blockDim.x) % 32 == 0;
+  if (lead)
     atomic_max_nonneg(&a.status->max_speed_bits, smax);
-  if (__any_sync(0xffffffffu, bad) && (threadIdx.x + threadIdx.y * blockDim.x) % 32 == 0)
-    atomicOr(&a.status->error_word, AXB_EW_NAN_FLUX);
+  const bool any_bad = __any_sync(0xffffffffu, bad);
+  const bool any_rhs = __any_sync(0xffffffffu, bad_rhs);
+  if (lead && (any_bad || any_rhs))
+    atomicOr(&a.status->error_word,
+             (any_bad ? AXB_EW_NAN_FLUX : 0u) | (any_rhs ? AXB_EW_NAN_RHS : 0u));
 }
 
 #ifndef AXB_FLUX_MINB
@@ -195,7 +209,7 @@ AXB_D void flux_pass_body(const RhsArgs &a, const EOS &eos, const int &seglen, c
     active = (t0 <= ng + b.n[T0]) && (t1 <= ng + b.n[T1]);
   }
   double smax = 0.0;
-  bool bad = false;
+  bool bad = false, bad_rhs = false;
   if (active) {
     const bool trans_int = (t0 >= ng) && (t0 < ng + b.n[T0]) && (t1 >= ng) &&
                            (t1 < ng + b.n[T1]);
@@ -207,8 +221,8 @@ AXB_D void flux_pass_body(const RhsArgs &a, const EOS &eos, const int &seglen, c
     ijk[T1] = t1;
     ijk[DIR] = f0 - 1;
     long long I = b.at(ijk[0], ijk[1], ijk[2]);
-    const double *const fld[NREC] = {a.rho,    a.entropy, a.Ye,       a.thermo,
-                                     a.vel[0], a.vel[1],  a.vel[2],   a.Bvec[D1],
+    const double *const fld[NREC] = {a.rho,     a.entropy, a.Ye,       a.thermo,
+                                     a.recv[0], a.recv[1], a.recv[2], a.Bvec[D1],
                                      a.Bvec[D2]};
     const double idxd = b.idx[DIR];
 #if AXB_FLUX_SMEM_CARRY
@@ -283,7 +297,7 @@ AXB_D void flux_pass_body(const RhsArgs &a, const EOS &eos, const int &seglen, c
             Fc[v] = F[v];
             Fp[v] = AXB_FPREV(v);
           }
-          fold_divergence<DIR>(a, I - sd, idxd, Fc, Fp);
+          bad_rhs |= fold_divergence<DIR>(a, I - sd, idxd, Fc, Fp);
         }
 #pragma unroll
         for (int v = 0; v < NHYDRO; ++v)
@@ -296,7 +310,7 @@ AXB_D void flux_pass_body(const RhsArgs &a, const EOS &eos, const int &seglen, c
 #undef AXB_UPL
 #undef AXB_FPREV
   }
-  flux_status(a, smax, bad);
+  flux_status(a, smax, bad, bad_rhs);
 }
 template <int DIR, int RECON, class EOS>
 __global__ void __launch_bounds__(128, AXB_FLUX_MINB)
@@ -329,8 +343,8 @@ AXB_D void flux_x_body(const RhsArgs &a, const EOS &eos, const uint3 bid) {
     const int j = ng - 1 + warp % ny;
     const int k = ng - 1 + warp / ny;
     const bool trans_int = (j >= ng) && (j < ng + b.n[1]) && (k >= ng) && (k < ng + b.n[2]);
-    const double *const fld[NREC] = {a.rho,    a.entropy, a.Ye,     a.thermo, a.vel[0],
-                                     a.vel[1], a.vel[2],  a.Bvec[1], a.Bvec[2]};
+    const double *const fld[NREC] = {a.rho,     a.entropy, a.Ye,      a.thermo, a.recv[0],
+                                     a.recv[1], a.recv[2], a.Bvec[1], a.Bvec[2]};
     const double idxd = b.idx[0];
     const long long row = b.at(0, j, k);
     const int clast = ng + b.n[0]; // last cell needed (right state of the last face)

@@ -382,7 +382,11 @@ AXB_D void ct_psi_body(const RhsArgs &a, const uint3 bid) {
     double r = -E;
     if (gl)
       r = -E - (G[I + b.stride(e)] - G[I]) / b.dx[e];
-    a.Arhs[e][I] = r;
+    if (a.fuse_stage)
+      a.st_uk[7 + e][I] = stage_combine(a.st_alpha, a.st_un[7 + e][I], a.st_beta,
+                                        a.st_uk[7 + e][I], a.st_gdt, r);
+    else
+      a.Arhs[e][I] = r;
   }
   if (gl) {
     double dF = 0.0;
@@ -396,9 +400,18 @@ AXB_D void ct_psi_body(const RhsArgs &a, const uint3 bid) {
           (0.5 / b.dx[d]);
       dF += c2c - one;
     }
-    a.Psi_rhs[I] = -dF - a.lorenz_damp_fac * a.alp[I] * a.Psi[I];
+    const double r = -dF - a.lorenz_damp_fac * a.alp[I] * a.Psi[I];
+    if (a.fuse_stage) // Psi is read above at this vertex only
+      a.st_uk[10][I] = stage_combine(a.st_alpha, a.st_un[10][I], a.st_beta,
+                                     a.st_uk[10][I], a.st_gdt, r);
+    else
+      a.Psi_rhs[I] = r;
   } else {
-    a.Psi_rhs[I] = 0.0;
+    if (a.fuse_stage)
+      a.st_uk[10][I] = stage_combine(a.st_alpha, a.st_un[10][I], a.st_beta,
+                                     a.st_uk[10][I], a.st_gdt, 0.0);
+    else
+      a.Psi_rhs[I] = 0.0;
   }
 }
 __global__ void __launch_bounds__(128)

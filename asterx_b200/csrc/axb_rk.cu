@@ -49,8 +49,10 @@ AXB_D void rk_stage_body(const StageArgs &a, double alpha, double beta, double g
 #pragma unroll
     for (int d = 0; d < 3; ++d)
       in &= ijk[d] < b.ng + b.n[d] + (a.cent[v][d] ? 0 : 1);
+    // explicit rounding order, the same as the stage update fused into the
+    // z flux pass and the CT kernel (stage_combine)
     if (in)
-      a.out[v][I] = alpha * a.un[v][I] + beta * a.uk[v][I] + gdt * a.rhs[v][I];
+      a.out[v][I] = fma(gdt, a.rhs[v][I], fma(beta, a.uk[v][I], alpha * a.un[v][I]));
   }
 }
 __global__ void __launch_bounds__(128)
@@ -266,10 +268,18 @@ namespace axb {
 
 // Per-box stage and ghost-fill argument blocks of a batch, in device memory.
 int batch_rk_setup(int nbox, const axb_box *boxes, const axb_fields *f, const axb_fields *fn,
-                   void **stage_args, void **sync_evolved, void **sync_prims) {
-  static const int prims[12] = {AXB_GF_rho,   AXB_GF_velx, AXB_GF_vely,        AXB_GF_velz,
-                                AXB_GF_eps,   AXB_GF_press, AXB_GF_temperature, AXB_GF_Ye,
-                                AXB_GF_entropy, AXB_GF_Bvecx, AXB_GF_Bvecy,     AXB_GF_Bvecz};
+                   int recvar, void **stage_args, void **sync_evolved, void **sync_prims) {
+  // the 12 cell-centred primitives, plus the reconstructed zvec or svec
+  // when the fluxes reconstruct one of those instead of the velocity
+  int prims[15] = {AXB_GF_rho,   AXB_GF_velx, AXB_GF_vely,        AXB_GF_velz,
+                   AXB_GF_eps,   AXB_GF_press, AXB_GF_temperature, AXB_GF_Ye,
+                   AXB_GF_entropy, AXB_GF_Bvecx, AXB_GF_Bvecy,     AXB_GF_Bvecz};
+  int nprims = 12;
+  if (recvar == AXB_RECVAR_Z || recvar == AXB_RECVAR_S) {
+    const int first = recvar == AXB_RECVAR_Z ? AXB_GF_zvec_x : AXB_GF_svec_x;
+    for (int q = 0; q < 3; ++q)
+      prims[nprims++] = first + q;
+  }
   std::vector<StageArgs> st(nbox);
   std::vector<SyncArgs> se(nbox), sp(nbox);
   for (int b = 0; b < nbox; ++b) {
@@ -297,7 +307,7 @@ int batch_rk_setup(int nbox, const axb_box *boxes, const axb_fields *f, const ax
       SyncArgs &y = pass ? sp[b] : se[b];
       std::memset(&y, 0, sizeof y);
       y.b = make_box(box);
-      const int nf = pass ? 12 : NEVOLVED;
+      const int nf = pass ? nprims : NEVOLVED;
       y.nf = nf;
       for (int q = 0; q < nf; ++q) {
         const int id = pass ? prims[q] : kEvolved[q];
@@ -355,4 +365,10 @@ int launch_sync_batch(const void *args, const TileTable &t, unsigned long long *
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
 }
 
+} // namespace axb
+
+namespace axb {
+// The centring of a grid function (1 = cell-centred along x, y, z), for the
+// other translation units of the library.
+int gf_centring(int gf, int c[3]) { return centring_of(gf, c); }
 } // namespace axb

@@ -91,6 +91,18 @@ class SlabHalo:
         recv_high = t[(ng + nz + v) * p:(2 * ng + nz + v) * p]
         return send_up, send_down, recv_low, recv_high
 
+    def _buffers(self, like, nfields):
+        """Persistent send and receive buffers for `nfields` fields (ng
+        planes each, per neighbour), kept between exchanges."""
+        import torch
+        n = nfields * self.L.ng * self.plane
+        key = (nfields, like.device, like.dtype)
+        if getattr(self, "_key", None) != key:
+            mk = lambda: torch.empty(n, dtype=like.dtype, device=like.device)
+            self._bufs = (mk(), mk(), mk(), mk())  # send up, send down, recv low, recv high
+            self._key = key
+        return self._bufs
+
     def exchange(self, tensors: Dict[str, "object"], names: Iterable[str]) -> None:
         names = list(names)
         if self.world == 1:
@@ -99,23 +111,43 @@ class SlabHalo:
                 rl.copy_(su)
                 rh.copy_(sd)
             return
+        import torch
         import torch.distributed as dist
-        ops, bufs = [], []
-        for n in names:
-            su, sd, rl, rh = self._slices(tensors[n], n)
-            # receive into separate buffers: a view being received into
-            # must not overlap a view being sent
-            bl, bh = rl.clone(), rh.clone()
-            bufs.append((rl, bl, rh, bh))
-            ops += [dist.P2POp(dist.isend, su.contiguous(), self.up, self.group),
-                    dist.P2POp(dist.isend, sd.contiguous(), self.down, self.group),
-                    dist.P2POp(dist.irecv, bl, self.down, self.group),
-                    dist.P2POp(dist.irecv, bh, self.up, self.group)]
+        sl = [self._slices(tensors[n], n) for n in names]
+        b_up, b_down, b_low, b_high = self._buffers(tensors[names[0]], len(names))
+        # the ghost planes of all fields travel as one message per neighbour
+        # and direction: pack, 4 point-to-point operations, unpack
+        torch.cat([q[0] for q in sl], out=b_up)
+        torch.cat([q[1] for q in sl], out=b_down)
+        ops = [dist.P2POp(dist.isend, b_up, self.up, self.group),
+               dist.P2POp(dist.isend, b_down, self.down, self.group),
+               dist.P2POp(dist.irecv, b_low, self.down, self.group),
+               dist.P2POp(dist.irecv, b_high, self.up, self.group)]
         for req in dist.batch_isend_irecv(ops):
             req.wait()
-        for rl, bl, rh, bh in bufs:
-            rl.copy_(bl)
-            rh.copy_(bh)
+        seg = self.L.ng * self.plane
+        for q, (_, _, rl, rh) in enumerate(sl):
+            rl.copy_(b_low[q * seg:(q + 1) * seg])
+            rh.copy_(b_high[q * seg:(q + 1) * seg])
+
+
+def allreduce_max(value: float, group=None, device=None) -> float:
+    """The largest `value` over the ranks of `group` (one all-reduce of a
+    double; the identity without an initialised process group)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return float(t.item())
+
+
+def cfl_dt(max_speed: float, dx: Sequence[float], dtfac: float, cfl: float = 0.9) -> float:
+    """Time step of the next substep: dtfac * dx[0] (the driver's fixed
+    dtfac), capped so that dt * max_speed * sum(1/dx) <= cfl."""
+    cap = cfl / (max(float(max_speed), 1e-300) * sum(1.0 / d for d in dx))
+    return min(dtfac * dx[0], cap)
 
 
 def slab_layout(n_global: Tuple[int, int, int], ng: int, rank: int, world: int
@@ -128,15 +160,34 @@ def slab_layout(n_global: Tuple[int, int, int], ng: int, rank: int, world: int
     return L, k0
 
 
-def slab_substep(eng, L, f, fn, params, eos, alpha, beta, gamma, dt, halo: SlabHalo):
+def prims_to_sync(params) -> List[str]:
+    """The cell-centred primitives a substep fills and exchanges, plus zvec
+    or svec when the fluxes reconstruct one of them (recon_type)."""
+    extra = {1: ["zvec_x", "zvec_y", "zvec_z"], 2: ["svec_x", "svec_y", "svec_z"]}
+    return PRIMS + extra.get(int(getattr(params, "recon_type", 0)), [])
+
+
+def slab_substep(eng, L, f, fn, params, eos, alpha, beta, gamma, dt, halo: SlabHalo,
+                 cfl: bool = False):
     """One RK substep of a rank's slab (axb_substep's sequence with the
     neighbours' ghost planes): RHS group, stage update, local periodic fill
     and halo exchange of the evolved variables, post-step group, local fill
-    and exchange of the primitives."""
+    and exchange of the primitives.  With `cfl`, returns the maximum
+    characteristic speed of this substep's faces over all ranks (one
+    all-reduce of a double after the RHS group; the engine's status is
+    reset first), the input of the next substep's cfl_dt."""
+    if cfl:
+        eng.status_reset()
     eng.rhs_group(L, f, params, eos)
+    smax = None
+    if cfl:
+        smax = allreduce_max(eng.status()["max_speed"], halo.group,
+                             device=f["rho"].device)
     eng.rk_stage(L, f, fn, f, f, alpha, beta, gamma, dt)
     eng.sync_periodic(L, f, EVOLVED)
     halo.exchange(f, EVOLVED)
     eng.con2prim_group(L, f, params, eos)
-    eng.sync_periodic(L, f, PRIMS)
-    halo.exchange(f, PRIMS)
+    prims = prims_to_sync(params)
+    eng.sync_periodic(L, f, prims)
+    halo.exchange(f, prims)
+    return smax

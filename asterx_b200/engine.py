@@ -83,6 +83,18 @@ def load_library(path=LIB_PATH):
     lib.axb_batch_substep.argtypes = [_vp, _vp, C.c_double, C.c_double, C.c_double,
                                       C.c_double, C.c_int, _vp]
     lib.axb_batch_autotune.argtypes = [_vp, _vp, C.POINTER(C.c_int), _vp]
+    lib.axb_fill_boundary.argtypes = [_vp, C.POINTER(Box), C.POINTER(Fields),
+                                      C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int), _vp]
+    lib.axb_fill_boundary.restype = C.c_int
+    lib.axb_rhs_group_bc.argtypes = [_vp, C.POINTER(Box), C.POINTER(Fields),
+                                     C.POINTER(Params), _vp, C.POINTER(C.c_int), _vp]
+    lib.axb_rhs_group_bc.restype = C.c_int
+    lib.axb_rk_lincomb.argtypes = [_vp, C.POINTER(Box), C.POINTER(Fields), C.c_int,
+                                   _dp, C.POINTER(C.POINTER(Fields)), C.c_double,
+                                   C.POINTER(Fields), _vp]
+    lib.axb_rk_lincomb.restype = C.c_int
+    lib.axb_probe_fp64.argtypes = [_dp]
+    lib.axb_probe_fp64.restype = C.c_int
     lib.axb_timing_begin.argtypes = [_vp]
     lib.axb_timing_end.argtypes = [_vp, C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_int]
     for name in ("axb_con2prim_group", "axb_substep", "axb_rk_stage",
@@ -190,6 +202,40 @@ class Engine:
                                                 self.stream_ptr(stream)),
                     "axb_con2prim_group")
 
+    def fill_boundary(self, layout, tensors, names, bc, stream=None):
+        """axb_fill_boundary: the ghost layers of `names` by the face rules
+        bc = (x-lower, x-upper, y-lower, y-upper, z-lower, z-upper), each an
+        abi.BC_* code."""
+        box = layout.box()
+        f = self.fields_struct(tensors)
+        ids = (C.c_int * len(names))(*[GF[n] for n in names])
+        b = (C.c_int * 6)(*bc)
+        self._check(self.lib.axb_fill_boundary(self.ctx, C.byref(box), C.byref(f), ids,
+                                               len(names), b, self.stream_ptr(stream)),
+                    "axb_fill_boundary")
+
+    def rhs_group_bc(self, layout, tensors, params, eos, bc, stream=None):
+        """axb_rhs_group_bc: the RHS group with physical outer boundaries."""
+        box = layout.box()
+        f = self.fields_struct(tensors)
+        b = (C.c_int * 6)(*bc)
+        self._check(self.lib.axb_rhs_group_bc(self.ctx, C.byref(box), C.byref(f),
+                                              C.byref(params), eos, b,
+                                              self.stream_ptr(stream)), "axb_rhs_group_bc")
+
+    def rk_lincomb(self, layout, out, states, coef, gdt, rhs, stream=None):
+        """axb_rk_lincomb: out = sum coef[q] * states[q] + gdt * RHS (rhs: a
+        dict with the RHS grid functions' names)."""
+        box = layout.box()
+        fo = self.fields_struct(out)
+        fs = [self.fields_struct(t) for t in states]
+        fr = self.fields_struct(rhs)
+        arr = (C.POINTER(Fields) * len(fs))(*[C.pointer(x) for x in fs])
+        cf = (C.c_double * len(coef))(*coef)
+        self._check(self.lib.axb_rk_lincomb(self.ctx, C.byref(box), C.byref(fo), len(fs),
+                                            cf, arr, gdt, C.byref(fr),
+                                            self.stream_ptr(stream)), "axb_rk_lincomb")
+
     def rk_stage(self, layout, out, un, uk, rhs, alpha, beta, gamma, dt, stream=None):
         box = layout.box()
         fs = [self.fields_struct(t) for t in (out, un, uk, rhs)]
@@ -214,6 +260,14 @@ class Engine:
                                          C.byref(params), eos, alpha, beta, gamma, dt,
                                          int(periodic), self.stream_ptr(stream)),
                     "axb_substep")
+
+    def probe_fp64(self):
+        """FP64 rates of this device: FMA TFLOP/s, divisions, square roots and
+        reciprocal square roots in G/s (axb_probe_fp64)."""
+        out = (C.c_double * 4)()
+        self._check(self.lib.axb_probe_fp64(out), "axb_probe_fp64")
+        return dict(fma_tflops=out[0], div_gops=out[1], sqrt_gops=out[2],
+                    rsqrt_gops=out[3])
 
     def timing_begin(self):
         self._check(self.lib.axb_timing_begin(self.ctx), "axb_timing_begin")

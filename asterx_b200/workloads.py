@@ -485,7 +485,8 @@ def c2p_cells(ncells, seed=4, gamma=5.0 / 3.0, rho_range=(1e-12, 1e-2),
 def cons_from_prims(L: Layout, f: dict, xp=None):
     """Densitised conserved variables of every cell from its primitives and
     the vertex-to-cell metric (the Valencia prim->cons map of
-    AsterX/src/prim2con.hxx:38-83), written into f."""
+    AsterX/src/prim2con.hxx:38-83), written into f, together with
+    zvec^i = W v^i and svec^i = rho h W^2 v^i."""
     xp = xp or _NP
     sq, g = _sqrt_detg_cell(L, f, xp)
     gd = [[g[0], g[1], g[2]], [g[1], g[3], g[4]], [g[2], g[4], g[5]]]
@@ -512,6 +513,12 @@ def cons_from_prims(L: Layout, f: dict, xp=None):
     f["tau"] = sq * (hW2 - (press + 0.5 * bs2) - bst * bst) - f["dens"]
     f["DYe"] = f["dens"] * f["Ye"]
     f["DEnt"] = f["dens"] * f["entropy"]
+    # the velocity-like variables the fluxes reconstruct with recon_type
+    # z_vec / s_vec, as the recovery writes them back (con2prim.cxx:432-441)
+    rhoh = rho + rho * eps + press
+    for i, ax in enumerate("xyz"):
+        f["zvec_" + ax] = W * v[i]
+        f["svec_" + ax] = rhoh * W * W * v[i]
 
 
 def perturbed_saved(f: dict, seed=7, amp=1e-2):

@@ -33,6 +33,10 @@ METRIC = "Zone-updates/s per RK3 substep"
 UNIT = "zone-updates/s"
 SSPRK3 = [(0.0, 1.0, 1.0), (0.75, 0.25, 0.25), (1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0)]
 GAMMA = 4.0 / 3.0
+CFL_MAX = 0.9
+# the survey's algorithmic figure for one substep: 112 FP64 values per zone
+# (RHS reads 34, stage 33, post-step reads 23 and writes 22)
+SUBSTEP_BYTES = 112 * 8
 EOS_KW = dict(rho=(1e-40, 1e10), eps=(0.0, 1e10))
 REGIONS = ["sources", "flux_x", "flux_y", "flux_z", "aux", "ct_psi", "rk_stage",
            "sync", "bstag", "c2p", "c2p_cells", "mlp"]
@@ -42,9 +46,13 @@ ALG_DOUBLES = {
     "sources": 9 + 16 + 7,           # prims + vertex metric & curvature, 7 RHS
     "flux_x": 9 + 1 + 10 + 7 + 2,    # recon fields, dB_stag, metric; acc, B fluxes
     "flux_y": 9 + 1 + 10 + 14 + 2,   # + acc read-modify-write
-    "flux_z": 9 + 1 + 10 + 7 + 14 + 2,  # + acc read, RHS read-modify-write
+    # z pass with the stage update fused (axb_substep): acc and the sources'
+    # RHS read, U_n and U_k read, U_k written
+    "flux_z": 9 + 1 + 10 + 7 + 7 + 14 + 7 + 2,
     "aux": 3 + 1 + 10 + 7,
-    "ct_psi": 6 + 7 + 4 + 4,
+    # CT + Psi with the fused stage: B fluxes, auxiliaries, lapse and shift,
+    # U_n and U_k of A and Psi read, U_k written
+    "ct_psi": 6 + 7 + 4 + 8 + 4,
     "rk_stage": 11 * 4,
     "bstag": 3 + 3,
     # ghost fill: the ghost shell of 11 + 12 fields, read and written, per
@@ -62,6 +70,14 @@ def parse_args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256, help="interior cells per axis")
     ap.add_argument("--recon", default="wenoz", choices=["wenoz", "mp5", "ppm"])
+    ap.add_argument("--recvar", default="z", choices=["v", "z", "s"],
+                    help="velocity variable the fluxes reconstruct (AsterX recon_type): "
+                         "v = vel (v_vec), z = W vel (z_vec, default: the 256^3 state's "
+                         "Lorentz factors up to 10 push a reconstructed v_vec past the "
+                         "speed of light at some faces), s = rho h W^2 vel (s_vec)")
+    ap.add_argument("--dtfac", type=float, default=0.25,
+                    help="dt = dtfac * dx, capped by the CFL limit of the engine's "
+                         "characteristic-speed maximum")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
@@ -177,12 +193,12 @@ class _StdoutToStderr:
         return False
 
 
-def reference_substep_rate(seconds, recon, seed=2, start_n=24):
+def reference_substep_rate(seconds, recon, seed=2, start_n=24, recvar="z"):
     with _StdoutToStderr():
-        return _reference_substep_rate(seconds, recon, seed, start_n)
+        return _reference_substep_rate(seconds, recon, seed, start_n, recvar)
 
 
-def _reference_substep_rate(seconds, recon, seed=2, start_n=24):
+def _reference_substep_rate(seconds, recon, seed=2, start_n=24, recvar="z"):
     """Time the reference's scheduled routines (AsterX_Fluxes,
     AsterX_SourceTerms, AsterX_RHS, the stage update, AsterX_ComputedBstagFromA,
     AsterX_ComputedBFromdBstag, AsterX_Con2Prim) on one box of the workload,
@@ -204,7 +220,8 @@ def _reference_substep_rate(seconds, recon, seed=2, start_n=24):
         for name in abi.GF_NAMES:
             f.setdefault(name, L.zeros())
         p = abi.default_params(reconstruction_method=recon, flux_type="hlle",
-                               c2p_prime="palenzuela", c2p_second="noble")
+                               c2p_prime="palenzuela", c2p_second="noble",
+                               recon_type={"v": 0, "z": 1, "s": 2}[recvar])
         host = {k: v.copy() for k, v in f.items()}
         ref.setup(L, p, host)
         ref.eos_idealgas(GAMMA, **EOS_KW)
@@ -243,9 +260,9 @@ def reference_arm(args):
     sample = None
     threads = None
     for _ in range(args.warmup):
-        reference_substep_rate(2.0, args.recon)
+        reference_substep_rate(2.0, args.recon, recvar=args.recvar)
     for _ in range(args.steps):
-        rate, sample, threads, _t = reference_substep_rate(6.0, args.recon)
+        rate, sample, threads, _t = reference_substep_rate(6.0, args.recon, recvar=args.recvar)
         res_rate.append(rate)
     value = statistics.median(res_rate)
     line = {
@@ -254,7 +271,8 @@ def reference_arm(args):
         "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"{args.n}^3 curved-metric patch (bounded CPU sample), "
-                               f"{args.recon}+HLLE, Palenzuela c2p, flux-CT",
+                               f"{args.recon}+HLLE on {args.recvar}_vec, Palenzuela c2p, "
+                               "flux-CT",
                    "parallelism": "OpenMP host threads"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
                          "kind": "reference", "sample": sample},
@@ -296,6 +314,13 @@ def ours(args):
     L, f = W.curved_box(n=args.n, ng=3, seed=2 + rank, wmax=10.0, xp=xp)
     W.cons_from_prims(L, f, xp=xp)
     W.saved_from_prims(f, xp=xp)
+    # keep only the reconstructed velocity variable the fluxes use (the
+    # recovery writes zvec / svec back only when they are given)
+    for ax in "xyz":
+        if args.recvar != "z":
+            f.pop("zvec_" + ax, None)
+        if args.recvar != "s":
+            f.pop("svec_" + ax, None)
     skip = {"zvec_x", "zvec_y", "zvec_z", "svec_x", "svec_y", "svec_z", "dBx",
             "dBy", "dBz"}
     for name in abi.GF_NAMES:
@@ -304,11 +329,24 @@ def ours(args):
     evolved = abi.CONS + ["Avec_x", "Avec_y", "Avec_z", "Psi"]
     fn = {k: f[k].clone() for k in evolved}
     params = abi.default_params(reconstruction_method=args.recon, flux_type="hlle",
-                                c2p_prime="palenzuela", c2p_second="noble")
+                                c2p_prime="palenzuela", c2p_second="noble",
+                                recon_type={"v": 0, "z": 1, "s": 2}[args.recvar])
     eos = eng.eos_idealgas(GAMMA, **EOS_KW)
-    dt = 0.25 * L.dx[0]
     zones = args.n ** 3
     stream = torch.cuda.current_stream(dev)
+
+    # time step: dtfac * dx, capped by the CFL limit of the characteristic
+    # speeds of the initial state (the engine's max |lambda| over all faces
+    # of one RHS evaluation): dt * smax * (1/dx + 1/dy + 1/dz) <= CFL_MAX
+    eng.status_reset()
+    eng.rhs_group(L, f, params, eos)
+    smax0 = eng.status()["max_speed"]
+    if world > 1:
+        t = torch.tensor([smax0], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        smax0 = float(t.item())
+    from asterx_b200.distribute import cfl_dt
+    dt = cfl_dt(smax0, L.dx, args.dtfac, CFL_MAX)
 
     halo = None
     if world > 1 and args.decomp == "slab":
@@ -326,8 +364,18 @@ def ours(args):
             from asterx_b200.distribute import slab_substep
             slab_substep(eng, L, f, fn, params, eos, a_, b_, g_, dt, halo)
 
+    # the FP64 peaks that bound the instruction-bound kernels
+    fp64 = eng.probe_fp64()
+
+    # warm-up, with the recovery failures and error word of every substep
+    warm_fail = []
+    warm_ew = 0
     for s in range(args.warmup):
+        eng.status_reset()
         substep(s)
+        st = eng.status()
+        warm_fail.append(st["c2p_fail"])
+        warm_ew |= st["error_word"]
     torch.cuda.synchronize()
     eng.status_reset()
     sampler = ClockSampler(local)
@@ -355,6 +403,10 @@ def ours(args):
         ms = float(t.item())
     value = world * zones * args.steps / (ms / 1e3)
     launches = int(sum(region_n))
+    healthy = (st["error_word"] & (abi.EW_NAN_FLUX | abi.EW_NAN_RHS)) == 0
+    if not healthy:
+        print(f"bench: the timed substeps raised error word {st['error_word']:#x} "
+              "(non-finite face fluxes or RHS)", file=sys.stderr)
 
     # dominant kernel and its roofline
     shares = {REGIONS[i]: region_ms[i] for i in range(len(REGIONS))
@@ -366,6 +418,7 @@ def ours(args):
     achieved = alg_bytes / avg_launch_s / 1e9
     peak, peak_kind = peak_hbm()
     traffic = traffic_table().get(f"{dom}:{args.recon}:{args.n}")
+    substep_gbs = SUBSTEP_BYTES * zones / (ms / args.steps / 1e3) / 1e9
 
     # end to end through the C ABI from pinned host memory: every step copies
     # the state the substep reads in and the state it writes back out
@@ -377,7 +430,8 @@ def ours(args):
               and not k.startswith("acc_")]
     outputs = [k for k in ["rho", "velx", "vely", "velz", "eps", "press",
                            "temperature", "Ye", "entropy", "Bvecx", "Bvecy", "Bvecz",
-                           "con2prim_flag"] + evolved + abi.SAVED if k in f]
+                           "con2prim_flag", "zvec_x", "zvec_y", "zvec_z", "svec_x",
+                           "svec_y", "svec_z"] + evolved + abi.SAVED if k in f]
     host = {k: torch.empty(L.size, dtype=torch.float64, pin_memory=True) for k in
             set(inputs) | set(outputs)}
     for k in host:
@@ -408,11 +462,14 @@ def ours(args):
     e2e_value = world * zones * ne / (ms_e2e / 1e3)
 
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            rate, sample, threads, _t = reference_substep_rate(args.cpu_seconds, args.recon)
+            rate, sample, threads, _t = reference_substep_rate(args.cpu_seconds, args.recon,
+                                                               recvar=args.recvar)
             cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
                    "sample": sample}
+            parity = reference_parity(eng, L, f, params, eos, dt)
         except Exception as exc:  # the checker library may be absent
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
                    "sample": f"unavailable: {exc}"}
@@ -424,9 +481,13 @@ def ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded fields of the configuration)",
             "config": {"workload": f"{args.n}^3 periodic patch, 3 ghosts, curved static "
-                                   f"metric, {args.recon}+HLLE, flux-CT, Palenzuela c2p "
-                                   f"(Noble backup), ideal gas Gamma=4/3, SSP-RK3 substeps",
+                                   f"metric, W <= 10, b^2/rho <= 10, 3 planar jumps, "
+                                   f"{args.recon}+HLLE on {args.recvar}_vec, flux-CT, "
+                                   f"Palenzuela c2p (Noble backup), ideal gas Gamma=4/3, "
+                                   f"SSP-RK3 substeps",
                        "box": [args.n] * 3, "ghosts": 3, "recon": args.recon,
+                       "recon_type": f"{args.recvar}_vec", "dt_over_dx": dt / L.dx[0],
+                       "cfl": dt * smax0 * sum(1.0 / d for d in L.dx),
                        "parallelism": (f"one box per GPU x{world}" if halo is None else
                                        f"z-slabs of one patch, halo exchange x{world}"),
                        "l2": "inputs larger than L2 (146 MB per field)"},
@@ -434,17 +495,26 @@ def ours(args):
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "alg_bytes_per_launch": alg_bytes,
-                         "avg_launch_ms": avg_launch_s * 1e3},
+                         "avg_launch_ms": avg_launch_s * 1e3,
+                         "substep": {"alg_bytes_per_zone": SUBSTEP_BYTES,
+                                     "achieved": substep_gbs, "frac": substep_gbs / peak}},
             "kernels_ms_per_step": {REGIONS[i]: region_ms[i] / args.steps
                                     for i in range(len(REGIONS)) if region_n[i]},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": ne},
             "cpu_baseline": cpu,
+            "parity": parity,
             "gpu_launches": launches,
             "clocks": clocks,
-            "error_word": st["error_word"], "c2p_fail_cells": st["c2p_fail"],
+            "health": {"nan_free": healthy, "error_word": st["error_word"],
+                       "c2p_fail_cells_timed": st["c2p_fail"],
+                       "c2p_fail_per_substep_timed": st["c2p_fail"] / args.steps,
+                       "c2p_fail_per_substep_warmup": warm_fail,
+                       "warmup_error_word": warm_ew},
             "max_char_speed": st["max_speed"],
             "c2p_mean_iters": _mean_iters(st["iter_hist"]),
+            "c2p_iter_hist": {int(i): int(v) for i, v in enumerate(st["iter_hist"]) if v},
+            "fp64_probe": fp64,
         }
         print(json.dumps(line), flush=True)
     eng.close()
@@ -452,6 +522,101 @@ def ours(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def reference_parity(eng, L, f, params, eos, dt, m=40, off=8, ng_ref=5):
+    """The checker half of the CPU-baseline leg: one substep (RHS group,
+    stage U + dt RHS, post-step group; no ghost fill in between) of a
+    m^3 sub-box cut from the timed state, on the engine (3 ghost zones) and
+    on the reference build (ng_ref ghost zones, the same cells), with the
+    maximum and L2 relative errors of the RHS and of the recovered
+    primitives and conserved variables."""
+    import numpy as np
+    import torch
+
+    from asterx_b200 import abi
+    from asterx_b200.abi import Layout
+    from oracle.oracle import reference
+    ref = reference()
+    if ref is None:
+        return None
+    o = L.ng + off
+    lo = o - ng_ref
+    L5 = Layout((m, m, m), ng_ref, L.dx,
+                tuple(L.xmin[d] + (o - L.ng) * L.dx[d] for d in range(3)))
+    L3 = Layout((m, m, m), 3, L5.dx, L5.xmin)
+    npt = L5.npts[0]
+    sub5 = {}
+    for k, t in f.items():
+        v = t.view(L.npts[2], L.npts[1], L.sy)[lo:lo + npt, lo:lo + npt, lo:lo + npt]
+        a = L5.zeros()
+        L5.view(a)[:, :, :npt] = v.cpu().numpy()
+        sub5[k] = a
+    d = ng_ref - 3
+    n3 = L3.npts[0]
+
+    def crop(a):
+        out = L3.zeros()
+        L3.view(out)[:, :, :n3] = L5.view(a)[d:d + n3, d:d + n3, d:d + n3]
+        return out
+
+    evolved = abi.CONS + ["Avec_x", "Avec_y", "Avec_z", "Psi"]
+    rhs = abi.HYDRO_RHS + abi.AVEC_RHS
+    cent = {"Avec_x": (1, 0, 0), "Avec_y": (0, 1, 0), "Avec_z": (0, 0, 1), "Psi": (0, 0, 0),
+            "Avec_x_rhs": (1, 0, 0), "Avec_y_rhs": (0, 1, 0), "Avec_z_rhs": (0, 0, 1),
+            "Psi_rhs": (0, 0, 0)}
+    # engine
+    dev = {k: torch.from_numpy(crop(a)).to(f["rho"].device) for k, a in sub5.items()}
+    eng.rhs_group(L3, dev, params, eos)
+    got_rhs = {k: dev[k].cpu().numpy() for k in rhs}
+    eng.rk_stage(L3, dev, dev, dev, dev, 0.0, 1.0, 1.0, dt)
+    eng.con2prim_group(L3, dev, params, eos)
+    got = {k: dev[k].cpu().numpy() for k in dev}
+    # reference build
+    host = {k: a.copy() for k, a in sub5.items()}
+    for name in abi.GF_NAMES:
+        host.setdefault(name, L5.zeros())
+    with _StdoutToStderr():
+        ref.setup(L5, params, host)
+        ref.eos_idealgas(GAMMA, **EOS_KW)
+        ref.rhs_group()
+        want_rhs = {k: host[k].copy() for k in rhs}
+        for u, r in zip(evolved, rhs):
+            sl = L5.interior(cent.get(u, (1, 1, 1)))
+            L5.view(host[u])[sl] = L5.view(host[u])[sl] + dt * L5.view(host[r])[sl]
+        ref.con2prim_group()
+
+    def errs(names, g, w):
+        emax = el2 = ept = 0.0
+        for k in names:
+            c = cent.get(k, (1, 1, 1))
+            gg = L3.view(g[k])[L3.interior(c)]
+            ww = L3.view(crop(w[k]))[L3.interior(c)]
+            scale = float(np.abs(ww).max()) or 1.0
+            diff = np.abs(gg - ww)
+            emax = max(emax, float(diff.max()) / scale)
+            el2 = max(el2, float(np.linalg.norm(gg - ww) / (np.linalg.norm(ww) or 1.0)))
+            ept = max(ept, float((diff / np.maximum(np.abs(ww), 1e-6 * scale)).max()))
+        return {"max_rel": emax, "l2_rel": el2, "max_point_rel_floor_1e-6": ept}
+
+    prims = ["rho", "eps", "press", "velx", "vely", "velz", "Bvecx", "Bvecy", "Bvecz"]
+    fl_g = L3.view(got["con2prim_flag"])[L3.interior()]
+    fl_w = L3.view(crop(host["con2prim_flag"]))[L3.interior()]
+    diff = fl_g != fl_w
+    ps = [abi.C2P_PRIME, abi.C2P_SECOND]
+    # cells whose Palenzuela bracket ends within a few ulps of the iteration
+    # cap may be recovered by the first scheme in one build and the second in
+    # the other (both within the tolerance): counted apart from other
+    # mismatches, and their primitives compared like every other cell's
+    swaps = diff & np.isin(fl_g, ps) & np.isin(fl_w, ps)
+    return {"sub_box": f"{m}^3 cells of the timed state (offset {off} from the interior "
+                       f"corner), engine with 3 ghosts, reference build with {ng_ref}",
+            "substep": "RHS group, U + dt RHS, post-step group",
+            "rhs": errs(rhs, got_rhs, want_rhs),
+            "prims_cons": errs(prims + abi.CONS, got, host),
+            "flag_prime_second_swaps": int(swaps.sum()),
+            "flag_other_mismatches": int((diff & ~swaps).sum()), "cells": int(diff.size),
+            "c2p_fail_cells_reference": int((fl_w == abi.C2P_FAIL).sum())}
 
 
 def c2p_bench(args):

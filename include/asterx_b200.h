@@ -294,10 +294,59 @@ AXB_API int axb_sync_periodic(axb_ctx *ctx, const axb_box *box,
                               const axb_fields *fields, const int *ids, int nids,
                               void *stream);
 
-/* One RK substep of one box: axb_rhs_group, axb_rk_stage (U_k updated in
- * place in `fields`, U_n read from `fields_n`), periodic fill of the evolved
+/* ------------------------------------------------------------------------ */
+/* physical outer boundaries and general Runge-Kutta methods                 */
+/* ------------------------------------------------------------------------ */
+
+/* Outer-boundary rules of CarpetX's boundary_x .. boundary_upper_z
+ * parameters that the reference's tests use (AsterX/test/*.par). */
+typedef enum axb_bc {
+  AXB_BC_PERIODIC = 0, /* ghost = periodic image                          */
+  AXB_BC_NEUMANN = 1,  /* "neumann": ghost = outermost interior point      */
+  AXB_BC_LINEAR = 2    /* "linear extrapolation" from the two outermost
+                          interior points                                   */
+} axb_bc;
+
+/* Fill the ghost layers of the grid functions ids[0..nids), each with its
+ * own centring, by the rule of each face: bc[0..5] = x-lower, x-upper,
+ * y-lower, y-upper, z-lower, z-upper; the x ghosts first (over all y, z
+ * points), then y, then z, so edges and corners take each direction's rule
+ * in turn.  The boundary point of a face is the outermost interior point of
+ * the centring (the boundary vertex itself for a vertex-centred direction).
+ * The driver applies this on every SYNC of a grid function with a physical
+ * boundary (AsterX/schedule.ccl's SYNC lists); no counterpart in the
+ * reference sources. */
+AXB_API int axb_fill_boundary(axb_ctx *ctx, const axb_box *box, const axb_fields *fields,
+                              const int *ids, int nids, const int bc[6], void *stream);
+
+/* axb_rhs_group for a box with the outer-boundary rules bc[6]: the face B
+ * fluxes (fxBy .. fzBy) and the vertex auxiliaries (Fx .. G) are computed on
+ * the interior and then filled on the ghost points by axb_fill_boundary, as
+ * the reference's AsterX_Fluxes writes them on the interior and SYNCs them
+ * (AsterX/schedule.ccl:174-195); axb_rhs_group instead computes them from
+ * the ghost data, which equals this when every face is periodic. */
+AXB_API int axb_rhs_group_bc(axb_ctx *ctx, const axb_box *box, const axb_fields *fields,
+                             const axb_params *params, const axb_eos *eos,
+                             const int bc[6], void *stream);
+
+/* The general stage combination of an explicit Runge-Kutta method on the
+ * interiors of the 11 evolved variables:
+ *   out = sum_{q < nstates} coef[q] * states[q] + gdt * RHS,   nstates <= 4,
+ * as CarpetX's ODESolvers forms its stages (RK2, RK3, RK4 with their
+ * stored stages).  `out` may be one of the states; `rhs` holds the RHS grid
+ * functions (densrhs .. Psi_rhs).  No counterpart in the reference
+ * sources. */
+AXB_API int axb_rk_lincomb(axb_ctx *ctx, const axb_box *box, const axb_fields *out,
+                           int nstates, const double *coef,
+                           const axb_fields *const *states, double gdt,
+                           const axb_fields *rhs, void *stream);
+
+/* One RK substep of one box: axb_rhs_group with axb_rk_stage fused into its
+ * last kernels (U_k updated in place in `fields`, U_n read from `fields_n`;
+ * the RHS grid functions are not written), periodic fill of the evolved
  * variables (if `periodic`), axb_con2prim_group, periodic fill of the
- * primitives (if `periodic`).  Stream-ordered, allocation-free. */
+ * primitives and of zvec / svec when recon_type reconstructs them (if
+ * `periodic`).  Stream-ordered, allocation-free. */
 AXB_API int axb_substep(axb_ctx *ctx, const axb_box *box,
                         const axb_fields *fields, const axb_fields *fields_n,
                         const axb_params *params, const axb_eos *eos,
@@ -439,11 +488,17 @@ AXB_API int axb_c2p_cells(axb_ctx *ctx, const axb_cells *cells,
  * axb_rhs_group; the 20 scratch grid functions (acc_*, fxBy..fzBy, Fx..G) are
  * ignored if given and taken instead from a 16 MiB array that this library
  * holds in static device memory on every GPU it is loaded on, until exit.
- * Limit: 20 * sz * (n[2] + 2*ng + 1) doubles (each rounded up to 32) must fit
- * in 2^21 doubles -- e.g. a 32^3 box with 3 ghosts; larger boxes get
- * AXB_ERR_TOO_LARGE.  Calls no cudaMalloc, cudaFree or allocating library
- * routine and needs no axb_ctx (the error word and CFL maximum are kept in
- * the static block, not reported).  The first call on a device looks up the
+ * Limit: 20 * sz * (n[2] + 2*ng + 1) doubles (each of the 20 rounded up to
+ * 32) must fit in 2^21 doubles; the limit is that formula, so it depends on
+ * the caller's row and plane padding (sy, sz) -- for example a 32^3 box with
+ * 3 ghosts and rows padded to 4 doubles fits, a 48^3 box does not.  Larger
+ * boxes get AXB_ERR_TOO_LARGE, and n[d] or ng outside [1, 2^15] (ng >= 3 is
+ * required as for axb_rhs_group) AXB_ERR_ARG, before anything runs.  Calls
+ * no cudaMalloc, cudaFree or allocating library routine and needs no
+ * axb_ctx.  The device error word and the CFL maximum go to a static status
+ * block that this entry point clears on every call and that is not
+ * reported: a caller that needs them (for instance the root-cap flag of a
+ * tabulated EOS) uses axb_rhs_group.  The first call on a device looks up the
  * arrays' device addresses with that device current; make it before any
  * stream capture.  All calls share the arrays: calls that overlap on the GPU
  * (other streams, other threads) race; order them on one stream. */
@@ -459,5 +514,13 @@ AXB_API int axb_rhs_group_noalloc(const axb_box *box, const axb_fields *fields,
  * counts.  Not part of the reference; a measurement aid. */
 AXB_API int axb_timing_begin(axb_ctx *ctx);
 AXB_API int axb_timing_end(axb_ctx *ctx, double *ms, int *count, int nregions);
+
+/* FP64 rates of the current device, the peaks of the engine's
+ * instruction-bound kernels: out[0] = FMA TFLOP/s (2 FLOP per FMA), out[1] =
+ * IEEE divisions G/s, out[2] = square roots G/s, out[3] = reciprocal square
+ * roots G/s, each from independent dependency chains over a grid of 8 CTAs
+ * per SM.  Synchronous; allocates a small buffer for the call.  Not part of
+ * the reference; a measurement aid. */
+AXB_API int axb_probe_fp64(double out[4]);
 
 #endif /* ASTERX_B200_H */

@@ -21,7 +21,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
-REF_ROOT = os.environ.get("AXB_REFERENCE_ROOT", "/root/reference")
+# The reference checkout is named by the caller (argument or the
+# AXB_REFERENCE_ROOT environment variable); there is no built-in default.
+REF_ROOT = os.environ.get("AXB_REFERENCE_ROOT", "")
 REF_TUS = ["fluxes", "source", "rhs", "computeBfromA", "con2prim"]
 # -DNDEBUG: the reference's device asserts (NaN checks in fluxes.cxx:769,
 # rhs.cxx:206) compile out, as in an optimised build, instead of aborting
@@ -41,12 +43,14 @@ def _stale(target, sources):
     return any(os.path.getmtime(s) > t for s in sources if os.path.exists(s))
 
 
-def build_ref(force=False):
+def build_ref(force=False, ref_root=None):
     """Compile the reference hot path through the shim; returns the .so path
-    or None when the reference checkout is not available."""
+    or None when the reference checkout is not available.  `ref_root` (or
+    AXB_REFERENCE_ROOT) names the checkout."""
     out_dir = os.path.join(HERE, "_ref")
     so = os.path.join(out_dir, "libaxref.so")
-    if not os.path.isdir(os.path.join(REF_ROOT, "AsterX", "src")):
+    REF_ROOT = ref_root or globals()["REF_ROOT"]
+    if not REF_ROOT or not os.path.isdir(os.path.join(REF_ROOT, "AsterX", "src")):
         return so if os.path.exists(so) else None
     os.makedirs(out_dir, exist_ok=True)
     shim = os.path.join(HERE, "refshim")
@@ -86,8 +90,8 @@ def build_restatement(force=False):
     return so
 
 
-def build(force=False):
-    return build_restatement(force), build_ref(force)
+def build(force=False, ref_root=None):
+    return build_restatement(force), build_ref(force, ref_root)
 
 
 if __name__ == "__main__":

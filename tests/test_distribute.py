@@ -89,3 +89,36 @@ def test_slab_halo_matches_global_periodic_fill(world):
     import torch.multiprocessing as mp
     mp.start_processes(_rank_main, args=(world, _free_port()), nprocs=world,
                        start_method="spawn", join=True)
+
+
+def test_cfl_dt():
+    dx = (1 / 64, 1 / 32, 1 / 16)
+    # the fixed dtfac governs while the characteristic speeds allow it
+    assert D.cfl_dt(0.1, dx, 0.25) == 0.25 / 64
+    # otherwise dt * smax * sum(1/dx) equals the CFL number
+    dt = D.cfl_dt(4.0, dx, 0.25, cfl=0.9)
+    assert dt < 0.25 / 64
+    assert abs(dt * 4.0 * (64 + 32 + 16) - 0.9) < 1e-12
+
+
+def _cfl_main(rank, world, port):
+    import torch.distributed as dist
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank,
+                            world_size=world)
+    try:
+        # each rank's faces saw a different maximum speed; every rank must
+        # take the same (largest) one and so the same time step
+        smax = D.allreduce_max(1.0 + 0.5 * rank)
+        assert smax == 1.0 + 0.5 * (world - 1)
+        dts = [None] * world
+        dist.all_gather_object(dts, D.cfl_dt(smax, (1 / 8,) * 3, 0.25))
+        assert len(set(dts)) == 1
+    finally:
+        dist.destroy_process_group()
+
+
+def test_allreduce_max_speed_two_ranks():
+    import torch.multiprocessing as mp
+    assert D.allreduce_max(3.5) == 3.5  # no process group: the identity
+    mp.start_processes(_cfl_main, args=(2, _free_port()), nprocs=2, start_method="spawn",
+                       join=True)

@@ -39,6 +39,23 @@ def test_rhs_group_noalloc_matches_rhs_group():
         torch.cuda.synchronize()
         want = {n: dev[n].cpu().numpy() for n in OUT}
 
+        # first a call on a box of another size, seed and layout, so that the
+        # static array holds values the 16^3 calls below do not write: a
+        # kernel that read a scratch entry its group never writes would see
+        # them
+        L2, f2 = W.curved_box(n=20, ng=3, seed=23, wmax=2.0, sigma=(1e-3, 0.3),
+                              theta=(0.1, 1.0))
+        f2 = full_fields(L2, f2)
+        dev2 = eng.upload(L2, f2)
+        io2 = {n: t for n, t in dev2.items() if n not in SCRATCH}
+        box2 = L2.box()
+        fields2 = eng.fields_struct(io2)
+        rc = lib.axb_rhs_group_noalloc(C.byref(box2), C.byref(fields2), C.byref(p),
+                                       eos, eng.stream_ptr())
+        assert rc == 0
+        torch.cuda.synchronize()
+        del dev2, io2
+
         # inputs and outputs only: no scratch pointers at all
         io = {n: t for n, t in dev.items() if n not in SCRATCH}
         box = L.box()
@@ -61,5 +78,11 @@ def test_rhs_group_noalloc_matches_rhs_group():
         rc = lib.axb_rhs_group_noalloc(C.byref(bigbox), C.byref(fields), C.byref(p),
                                        eos, eng.stream_ptr())
         assert rc == 5  # AXB_ERR_TOO_LARGE
+        # sizes out of range are refused before any arithmetic on them
+        huge = L.box()
+        huge.ng = 1 << 30
+        rc = lib.axb_rhs_group_noalloc(C.byref(huge), C.byref(fields), C.byref(p),
+                                       eos, eng.stream_ptr())
+        assert rc == 1  # AXB_ERR_ARG
     finally:
         eng.close()
