@@ -233,7 +233,9 @@ AXB_HD double mp5_one(double gf_Imm, double gf_Im, double gf_I, double gf_Ip,
   const double uul = gf_I + alpha * deltam;
   const double uav = (gf_I + gf_Ip) / 2.0;
   const double umd = uav - dmp / 2.0;
-  const double ulc = gf_I + deltam / 2.0 + 4.0 / 3.0 * dmm;
+  // (4/3) dmm is the one product here that is not exact: rounded on its
+  // own, so no kernel that inlines this contracts it differently
+  const double ulc = add_rn(gf_I + deltam / 2.0, mul_rn(4.0 / 3.0, dmm));
   const double umin = fmax(fmin(gf_I, fmin(gf_Ip, umd)), fmin(gf_I, fmin(uul, ulc)));
   const double umax = fmin(fmax(gf_I, fmax(gf_Ip, umd)), fmax(gf_I, fmax(uul, ulc)));
   // median(ul, umin, umax) = ul + minmod(umin - ul, umax - ul)

@@ -150,9 +150,9 @@ int centring_of(int gf, int c[3]) {
   case AXB_GF_Avec_x: case AXB_GF_Avec_x_rhs: c[1] = c[2] = 0; break;
   case AXB_GF_Avec_y: case AXB_GF_Avec_y_rhs: c[0] = c[2] = 0; break;
   case AXB_GF_Avec_z: case AXB_GF_Avec_z_rhs: c[0] = c[1] = 0; break;
-  case AXB_GF_dBx_stag: c[0] = 0; break;
-  case AXB_GF_dBy_stag: c[1] = 0; break;
-  case AXB_GF_dBz_stag: c[2] = 0; break;
+  case AXB_GF_dBx_stag: case AXB_GF_fxBy: case AXB_GF_fxBz: c[0] = 0; break;
+  case AXB_GF_dBy_stag: case AXB_GF_fyBx: case AXB_GF_fyBz: c[1] = 0; break;
+  case AXB_GF_dBz_stag: case AXB_GF_fzBx: case AXB_GF_fzBy: c[2] = 0; break;
   default:
     if ((gf >= AXB_GF_gxx && gf <= AXB_GF_kzz) || gf == AXB_GF_Psi ||
         gf == AXB_GF_Psi_rhs || (gf >= AXB_GF_Fx && gf <= AXB_GF_G))
