@@ -79,6 +79,12 @@ class Fields(C.Structure):
     _fields_ = [("gf", C.c_void_p * NUM_GF)]
 
 
+class FieldsStrided(C.Structure):
+    """axb_fields_strided: one pointer and its own (sy, sz) per grid function."""
+    _fields_ = [("gf", C.c_void_p * NUM_GF), ("sy", C.c_int64 * NUM_GF),
+                ("sz", C.c_int64 * NUM_GF)]
+
+
 # independent cells for axb_c2p_cells / axb_mlp_features (axb_cells)
 CELL_INPUTS = ["dens", "momx", "momy", "momz", "tau", "DYe", "DEnt", "dBx", "dBy", "dBz",
                "gxx", "gxy", "gxz", "gyy", "gyz", "gzz"]
@@ -97,7 +103,8 @@ class Cells(C.Structure):
                 ("rho", C.c_void_p), ("eps", C.c_void_p), ("press", C.c_void_p),
                 ("vel", C.c_void_p * 3), ("w_lorentz", C.c_void_p), ("Ye", C.c_void_p),
                 ("temperature", C.c_void_p), ("entropy", C.c_void_p),
-                ("iters", C.c_void_p), ("flag", C.c_void_p), ("guess", C.c_void_p)]
+                ("iters", C.c_void_p), ("flag", C.c_void_p), ("guess", C.c_void_p),
+                ("fallback", C.c_void_p)]
 
 
 def cells_struct(n, arrays: dict):
@@ -116,7 +123,7 @@ def cells_struct(n, arrays: dict):
         c.g[q] = get(nm)
     for nm in ("seed_rho", "seed_eps", "seed_Ye", "seed_temperature", "rho", "eps",
                "press", "w_lorentz", "Ye", "temperature", "entropy", "iters", "flag",
-               "guess"):
+               "guess", "fallback"):
         setattr(c, nm, get(nm))
     return c
 

@@ -134,6 +134,79 @@ __global__ void __launch_bounds__(128) k_lincomb(const LincombArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// grid functions between the caller's per-field layouts and the engine's
+// ---------------------------------------------------------------------------
+struct CopyArgs {
+  BoxDev b;
+  double *dst[AXB_NUM_GF];
+  const double *src[AXB_NUM_GF];
+  long long ssy[AXB_NUM_GF], ssz[AXB_NUM_GF]; // strides of the strided side
+  int cent[AXB_NUM_GF][3];
+  int to_engine; // 1: strided -> engine layout, 0: engine -> strided
+};
+
+// One thread per point of the field's centring extent (ghosts included).
+__global__ void __launch_bounds__(128) k_copy_layout(const CopyArgs a) {
+  const int v = blockIdx.y;
+  const BoxDev &b = a.b;
+  const int *c = a.cent[v];
+  const int N0 = b.n[0] + 2 * b.ng + (c[0] ? 0 : 1);
+  const int N1 = b.n[1] + 2 * b.ng + (c[1] ? 0 : 1);
+  const int N2 = b.n[2] + 2 * b.ng + (c[2] ? 0 : 1);
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (long long)N0 * N1 * N2)
+    return;
+  const int i = int(g % N0);
+  const int j = int((g / N0) % N1);
+  const int k = int(g / ((long long)N0 * N1));
+  const long long E = b.at(i, j, k);
+  const long long S = (long long)i + a.ssy[v] * j + a.ssz[v] * k;
+  if (a.to_engine)
+    a.dst[v][E] = a.src[v][S];
+  else
+    a.dst[v][S] = a.src[v][E];
+}
+
+int copy_layout(axb_ctx *c, const axb_box *box, const axb_fields *eng,
+                const axb_fields_strided *str, const int *ids, int nids, int to_engine,
+                cudaStream_t s) {
+  if (!c || !box || !eng || !str || !ids || nids < 1 || nids > AXB_NUM_GF || box->ng < 0)
+    return AXB_ERR_ARG;
+  for (int d = 0; d < 3; ++d)
+    if (box->n[d] < 1)
+      return AXB_ERR_ARG;
+  CopyArgs a;
+  a.b = make_box(*box);
+  a.to_engine = to_engine;
+  long long gmax = 0;
+  for (int q = 0; q < nids; ++q) {
+    const int id = ids[q];
+    if (id < 0 || id >= AXB_NUM_GF || !eng->gf[id] || !str->gf[id])
+      return AXB_ERR_ARG;
+    gf_centring(id, a.cent[q]);
+    const long long N0 = box->n[0] + 2LL * box->ng + (a.cent[q][0] ? 0 : 1);
+    const long long N1 = box->n[1] + 2LL * box->ng + (a.cent[q][1] ? 0 : 1);
+    const long long N2 = box->n[2] + 2LL * box->ng + (a.cent[q][2] ? 0 : 1);
+    // the strided side must hold its centring's points without overlap
+    if (str->sy[id] < N0 || str->sz[id] < str->sy[id] * N1)
+      return AXB_ERR_ARG;
+    a.ssy[q] = str->sy[id];
+    a.ssz[q] = str->sz[id];
+    if (to_engine) {
+      a.src[q] = str->gf[id];
+      a.dst[q] = eng->gf[id];
+    } else {
+      a.src[q] = eng->gf[id];
+      a.dst[q] = str->gf[id];
+    }
+    gmax = std::max(gmax, N0 * N1 * N2);
+  }
+  const dim3 grid(unsigned((gmax + 127) / 128), nids);
+  k_copy_layout<<<grid, 128, 0, s>>>(a);
+  return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+}
+
 bool bc_valid(int t) {
   return t == AXB_BC_PERIODIC || t == AXB_BC_NEUMANN || t == AXB_BC_LINEAR;
 }
@@ -226,4 +299,16 @@ AXB_API int axb_rk_lincomb(axb_ctx *c, const axb_box *box, const axb_fields *out
   k_lincomb<<<grid, T, 0, s>>>(a);
   axb_mark(c, AXB_R_STAGE, s, false);
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+}
+
+// Grid functions whose centrings have their own extents and strides (as
+// CarpetX allocates them) into the engine's one-layout box, and back.
+AXB_API int axb_import_fields(axb_ctx *c, const axb_box *box, const axb_fields_strided *src,
+                              const int *ids, int nids, const axb_fields *dst, void *stream) {
+  return copy_layout(c, box, dst, src, ids, nids, 1, (cudaStream_t)stream);
+}
+AXB_API int axb_export_fields(axb_ctx *c, const axb_box *box, const axb_fields *src,
+                              const int *ids, int nids, const axb_fields_strided *dst,
+                              void *stream) {
+  return copy_layout(c, box, src, dst, ids, nids, 0, (cudaStream_t)stream);
 }

@@ -42,6 +42,7 @@ struct Offsets {
 
 struct axb_mlp {
   int nf;
+  int act; // hidden activation (MLP_ACT_SILU / MLP_ACT_RELU)
   int device;
   int64_t P;
   float *params; // FP32 master parameters
@@ -57,6 +58,7 @@ struct axb_mlp {
   MlpDev dev() const {
     MlpDev m;
     m.nf = nf;
+    m.act = act;
     m.w1 = wt;
     m.w2 = wt + MLP_H * MLP_K1;
     m.w3 = m.w2 + MLP_H * MLP_H;
@@ -131,6 +133,11 @@ AXB_D float dsilu(float z) {
   const float sg = sigm(z);
   return sg * (1.0f + z * (1.0f - sg));
 }
+// the hidden activation and its derivative (ReLU' = 1 for z > 0, else 0)
+AXB_D float act_f(float z, int act) { return act == MLP_ACT_RELU ? fmaxf(z, 0.0f) : z * sigm(z); }
+AXB_D float dact(float z, int act) {
+  return act == MLP_ACT_RELU ? (z > 0.0f ? 1.0f : 0.0f) : dsilu(z);
+}
 
 // ---------------------------------------------------------------------------
 // features of independent cells
@@ -149,7 +156,8 @@ __global__ void k_mlp_features(const axb_cells c, int nf, float *out) {
     out[i * nf + k] = f[k];
 }
 
-// tensor-core forward on given features (the code path of k_mlp_guess)
+// tensor-core forward on given features (the code path of the recovery's
+// learned guess, mlp_cell_guess)
 __global__ void __launch_bounds__(256) k_mlp_forward(const MlpDev m, const float *feat,
                                                      long long n, float *out) {
   __shared__ MlpSmem w;
@@ -166,48 +174,6 @@ __global__ void __launch_bounds__(256) k_mlp_forward(const MlpDev m, const float
   if (i < n) {
     out[2 * i] = y0;
     out[2 * i + 1] = y1;
-  }
-}
-
-// Learned guess of independent cells: features from the conserved
-// variables and metric, the network, and the decoded guess (x = h W, W) per
-// cell.  A persistent grid: each CTA stages the weights once and its warps
-// walk chunks of 32 cells.
-__global__ void __launch_bounds__(256) k_mlp_guess(const axb_cells c, const MlpDev m,
-                                                   float2 *guess) {
-  __shared__ MlpSmem w;
-  __shared__ uint32_t stage[8][32 * 8];
-  mlp_stage_weights(m, w);
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  const long long nchunks = (c.n + 31) / 32;
-  for (long long ch = warp0; ch < nchunks; ch += nwarps) { // warp-uniform
-    const long long i = ch * 32 + lane;
-    const bool valid = i < c.n;
-    float f[MLP_K1];
-#pragma unroll
-    for (int k = 0; k < MLP_K1; ++k)
-      f[k] = 0.0f;
-    CellInvariants inv{1.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    if (valid) {
-      const sym3 glo{c.g[0][i], c.g[1][i], c.g[2][i], c.g[3][i], c.g[4][i], c.g[5][i]};
-      const double mom[3] = {c.mom[0][i], c.mom[1][i], c.mom[2][i]};
-      const double dB[3] = {c.dB[0][i], c.dB[1][i], c.dB[2][i]};
-      inv = cell_invariants(c.dens[i], mom, c.tau[i], c.DYe[i], dB, glo);
-      mlp_features(inv, m.nf, f);
-    }
-    float y0, y1;
-    mlp_forward_warp(w, f, stage[threadIdx.x >> 5], y0, y1);
-    if (valid) {
-      // y0 places x = h W in the Palenzuela scheme's initial bracket
-      // (c2p_1DPalenzuela.hxx:395-398)
-      const double lo = fmax(1e-10, 1.0 + inv.q - inv.s), hi = 2.0 + 2.0 * inv.q - inv.s;
-      const double x = lo + double(y0) * (hi - lo);
-      const double W = fmax(exp(double(y1)), 1.0);
-      guess[i] = make_float2(float(x), float(W));
-    }
   }
 }
 
@@ -244,17 +210,18 @@ __device__ void dense64(const float *in, int ldin, int K, const float *W, const 
     out[(s0 + s) * LD + n] = acc[s];
 }
 
-// H = bf16(silu(Z)) for the 64 x 64 buffer
-__device__ void act64(const float *Z, float *H) {
+// H = bf16(act(Z)) for the 64 x 64 buffer
+__device__ void act64(const float *Z, float *H, int act) {
   for (int e = threadIdx.x; e < TB * MLP_H; e += TT) {
     const int s = e / MLP_H, k = e % MLP_H;
     const float z = Z[s * LD + k];
-    H[s * LD + k] = bf16r(z * sigm(z));
+    H[s * LD + k] = bf16r(act_f(z, act));
   }
 }
 
-// dZprev[s][k] = (sum_n dZ[s][n] W[k][n]) * silu'(Zprev[s][k])
-__device__ void back64(const float *dZ, const float *W, const float *Zprev, float *dZprev) {
+// dZprev[s][k] = (sum_n dZ[s][n] W[k][n]) * act'(Zprev[s][k])
+__device__ void back64(const float *dZ, const float *W, const float *Zprev, float *dZprev,
+                       int act) {
   const int k = threadIdx.x & 63, s0 = (threadIdx.x >> 6) * 32;
   float acc[32];
 #pragma unroll
@@ -268,7 +235,7 @@ __device__ void back64(const float *dZ, const float *W, const float *Zprev, floa
   }
 #pragma unroll
   for (int s = 0; s < 32; ++s)
-    dZprev[(s0 + s) * LD + k] = acc[s] * dsilu(Zprev[(s0 + s) * LD + k]);
+    dZprev[(s0 + s) * LD + k] = acc[s] * dact(Zprev[(s0 + s) * LD + k], act);
 }
 
 // gW[k][n] = sum_s H[s][k] dZ[s][n] (K x 64), gb[n] = sum_s dZ[s][n]
@@ -288,7 +255,7 @@ __device__ void grad64(const float *H, int ldh, int K, const float *dZ, float *g
   }
 }
 
-__global__ void __launch_bounds__(TT) k_mlp_train(const float *__restrict__ p, int nf,
+__global__ void __launch_bounds__(TT) k_mlp_train(const float *__restrict__ p, int nf, int act,
                                                   const float *__restrict__ feat,
                                                   const float *__restrict__ tgt,
                                                   long long n, float *partial,
@@ -326,15 +293,15 @@ __global__ void __launch_bounds__(TT) k_mlp_train(const float *__restrict__ p, i
   // forward
   dense64(S.X, MLP_K1, MLP_K1, S.W1, S.b1, S.Z1);
   __syncthreads();
-  act64(S.Z1, S.B0);
+  act64(S.Z1, S.B0, act);
   __syncthreads();
   dense64(S.B0, LD, MLP_H, S.W2, S.b2, S.Z2);
   __syncthreads();
-  act64(S.Z2, S.B0);
+  act64(S.Z2, S.B0, act);
   __syncthreads();
   dense64(S.B0, LD, MLP_H, S.W3, S.b3, S.Z3);
   __syncthreads();
-  act64(S.Z3, S.B0); // H3
+  act64(S.Z3, S.B0, act); // H3
   __syncthreads();
   float l = 0.0f;
   {
@@ -368,22 +335,22 @@ __global__ void __launch_bounds__(TT) k_mlp_train(const float *__restrict__ p, i
       gp[o.b4 + threadIdx.x] = b;
     }
   }
-  // dZ3 = (dY W4^T) * silu'(Z3)
+  // dZ3 = (dY W4^T) * act'(Z3)
   for (int e = threadIdx.x; e < TB * MLP_H; e += TT) {
     const int s = e / MLP_H, k = e % MLP_H;
     const float dh = S.dY[s * 2] * S.W4[k * 2] + S.dY[s * 2 + 1] * S.W4[k * 2 + 1];
-    S.B1[s * LD + k] = dh * dsilu(S.Z3[s * LD + k]);
+    S.B1[s * LD + k] = dh * dact(S.Z3[s * LD + k], act);
   }
   __syncthreads();
-  act64(S.Z2, S.B0); // H2
+  act64(S.Z2, S.B0, act); // H2
   __syncthreads();
   grad64(S.B0, LD, MLP_H, S.B1, gp + o.w3, gp + o.b3);
-  back64(S.B1, S.W3, S.Z2, S.B2); // dZ2
+  back64(S.B1, S.W3, S.Z2, S.B2, act); // dZ2
   __syncthreads();
-  act64(S.Z1, S.B0); // H1
+  act64(S.Z1, S.B0, act); // H1
   __syncthreads();
   grad64(S.B0, LD, MLP_H, S.B2, gp + o.w2, gp + o.b2);
-  back64(S.B2, S.W2, S.Z1, S.B1); // dZ1
+  back64(S.B2, S.W2, S.Z1, S.B1, act); // dZ1
   __syncthreads();
   grad64(S.X, MLP_K1, nf, S.B1, gp + o.w1, gp + o.b1);
   // loss partial (fixed-order tree)
@@ -439,7 +406,13 @@ AXB_API int64_t axb_mlp_param_count(int nf) {
 
 AXB_API int axb_mlp_create(int nf, const float *params, uint64_t seed, double bracket,
                            axb_mlp **out) {
-  if (!out || nf < 1 || nf > MLP_K1 || !(bracket > 0 && bracket < 1))
+  return axb_mlp_create_act(nf, AXB_MLP_SILU, params, seed, bracket, out);
+}
+
+AXB_API int axb_mlp_create_act(int nf, int activation, const float *params, uint64_t seed,
+                               double bracket, axb_mlp **out) {
+  if (!out || nf < 1 || nf > MLP_K1 || !(bracket > 0 && bracket < 1) ||
+      !(activation == AXB_MLP_SILU || activation == AXB_MLP_RELU))
     return AXB_ERR_ARG;
   *out = nullptr;
   const Offsets o(nf);
@@ -470,6 +443,7 @@ AXB_API int axb_mlp_create(int nf, const float *params, uint64_t seed, double br
     return AXB_ERR_ARG;
   }
   m->nf = nf;
+  m->act = activation == AXB_MLP_RELU ? MLP_ACT_RELU : MLP_ACT_SILU;
   m->P = o.P;
   m->bracket = bracket;
   cudaGetDevice(&m->device);
@@ -546,21 +520,6 @@ AXB_API int axb_mlp_forward(axb_ctx *c, const axb_mlp *m, const float *features,
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
 }
 
-namespace axb {
-int launch_mlp_guess(const axb_cells &c, const axb_mlp *m, float2 *guess, cudaStream_t s) {
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const long long chunks = (c.n + 31) / 32;
-  long long blocks = (chunks + 7) / 8;
-  if (blocks > 4LL * sms) // persistent: a few CTAs per SM amortise the weight copy
-    blocks = 4LL * sms;
-  if (blocks < 1)
-    return AXB_OK;
-  k_mlp_guess<<<(unsigned)blocks, 256, 0, s>>>(c, m->dev(), guess);
-  return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
-}
-} // namespace axb
 
 AXB_API int axb_mlp_train_step(axb_ctx *c, axb_mlp *m, const float *features,
                                const float *targets, int64_t n, float lr, float beta1,
@@ -585,7 +544,7 @@ AXB_API int axb_mlp_train_step(axb_ctx *c, axb_mlp *m, const float *features,
   const size_t smem = sizeof(TrainSmem);
   AXB_CUDA_TRY(cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)smem));
-  k_mlp_train<<<(unsigned)nblocks, TT, smem, s>>>(m->params, m->nf, features, targets, n,
+  k_mlp_train<<<(unsigned)nblocks, TT, smem, s>>>(m->params, m->nf, m->act, features, targets, n,
                                                   m->partial, m->loss_partial);
   float *g = grad ? grad : m->grad;
   k_mlp_reduce<<<(unsigned)((m->P + 255) / 256), 256, 0, s>>>(m->partial, nblocks,

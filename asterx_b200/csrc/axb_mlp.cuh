@@ -1,7 +1,7 @@
 // Learned initial guess for the primitive recovery: input features and the
 // warp-level MLP forward pass on the tensor cores.
 //
-// Network: nf -> 64 -> 64 -> 64 -> 2, SiLU on the hidden layers, BF16
+// Network: nf -> 64 -> 64 -> 64 -> 2, SiLU or ReLU on the hidden layers, BF16
 // weights and activations, FP32 accumulation and biases.  A CTA stages the
 // ~20 KB of weights in shared memory once (rows padded so that the B
 // fragments load without bank conflicts) and each warp evaluates 32 cells
@@ -25,8 +25,11 @@ constexpr int MLP_N4 = 8;             // padded output width
 // Inference parameters on the device.  Weights are stored transposed,
 // n-major (wT[n][k]), so that the two consecutive k of a B fragment are one
 // 32-bit word.
+enum { MLP_ACT_SILU = 0, MLP_ACT_RELU = 1 };
+
 struct MlpDev {
   int nf;
+  int act; // MLP_ACT_SILU or MLP_ACT_RELU
   const __nv_bfloat16 *w1; // [64][16]
   const __nv_bfloat16 *w2; // [64][64]
   const __nv_bfloat16 *w3; // [64][64]
@@ -115,6 +118,9 @@ AXB_D float silu(float z) {
   const float hz = 0.5f * z;
   return fmaf(hz, tanh_approx(hz), hz);
 }
+// The hidden activation: SiLU, or ReLU (one FP32 max, no special-function
+// instruction).  `act` is uniform over the warp.
+AXB_D float mlp_act(float z, int act) { return act == MLP_ACT_RELU ? fmaxf(z, 0.0f) : silu(z); }
 
 // Weights in shared memory, n-major with padded rows (K + 8 bf16): the
 // eight rows a B-fragment load touches then fall in distinct banks.
@@ -126,6 +132,7 @@ struct MlpSmem {
   __nv_bfloat16 w3[MLP_H * MLP_LDH];
   __nv_bfloat16 w4[MLP_N4 * MLP_LDH];
   float b1[MLP_H], b2[MLP_H], b3[MLP_H], b4[MLP_N4];
+  int act;
 };
 
 // Cooperative copy of the device weights into shared memory (all threads
@@ -146,6 +153,8 @@ AXB_D void mlp_stage_weights(const MlpDev &m, MlpSmem &w) {
   }
   if (threadIdx.x < MLP_N4)
     w.b4[threadIdx.x] = m.b4[threadIdx.x];
+  if (threadIdx.x == 0)
+    w.act = m.act;
 }
 
 // B fragment words for n-tile nt, k-block kb of a weight stored wT[n][ld].
@@ -160,7 +169,7 @@ AXB_D void load_b(const __nv_bfloat16 *wT, int ld, int nt, int kb, int lane, uin
 
 // Hidden layer: A (4 k-blocks of 16) x W [64 x 64] -> 8 n-tiles, bias, SiLU,
 // repacked as the next layer's A (4 k-blocks).
-AXB_D void mlp_hidden64(const __nv_bfloat16 *wT, const float *bias, int lane,
+AXB_D void mlp_hidden64(const __nv_bfloat16 *wT, const float *bias, int act, int lane,
                         const uint32_t (&ain)[4][4], uint32_t (&aout)[4][4]) {
   const int t2 = (lane & 3) * 2;
 #pragma unroll
@@ -181,10 +190,10 @@ AXB_D void mlp_hidden64(const __nv_bfloat16 *wT, const float *bias, int lane,
         mma_bf16_16816(c[h], ain[kk], b0, b1);
       }
     }
-    aout[kb][0] = pack_bf16x2(silu(c[0][0]), silu(c[0][1]));
-    aout[kb][1] = pack_bf16x2(silu(c[0][2]), silu(c[0][3]));
-    aout[kb][2] = pack_bf16x2(silu(c[1][0]), silu(c[1][1]));
-    aout[kb][3] = pack_bf16x2(silu(c[1][2]), silu(c[1][3]));
+    aout[kb][0] = pack_bf16x2(mlp_act(c[0][0], act), mlp_act(c[0][1], act));
+    aout[kb][1] = pack_bf16x2(mlp_act(c[0][2], act), mlp_act(c[0][3], act));
+    aout[kb][2] = pack_bf16x2(mlp_act(c[1][0], act), mlp_act(c[1][1], act));
+    aout[kb][3] = pack_bf16x2(mlp_act(c[1][2], act), mlp_act(c[1][3], act));
   }
 }
 
@@ -213,14 +222,14 @@ AXB_D void mlp_tile(const MlpSmem &w, const uint32_t *stage, int mt, int lane,
       load_b(w.w1, MLP_LD1, nt, 0, lane, b0, b1);
       mma_bf16_16816(cc[h], a1, b0, b1);
     }
-    h1[kb][0] = pack_bf16x2(silu(cc[0][0]), silu(cc[0][1]));
-    h1[kb][1] = pack_bf16x2(silu(cc[0][2]), silu(cc[0][3]));
-    h1[kb][2] = pack_bf16x2(silu(cc[1][0]), silu(cc[1][1]));
-    h1[kb][3] = pack_bf16x2(silu(cc[1][2]), silu(cc[1][3]));
+    h1[kb][0] = pack_bf16x2(mlp_act(cc[0][0], w.act), mlp_act(cc[0][1], w.act));
+    h1[kb][1] = pack_bf16x2(mlp_act(cc[0][2], w.act), mlp_act(cc[0][3], w.act));
+    h1[kb][2] = pack_bf16x2(mlp_act(cc[1][0], w.act), mlp_act(cc[1][1], w.act));
+    h1[kb][3] = pack_bf16x2(mlp_act(cc[1][2], w.act), mlp_act(cc[1][3], w.act));
   }
   uint32_t h2[4][4], h3[4][4];
-  mlp_hidden64(w.w2, w.b2, lane, h1, h2);
-  mlp_hidden64(w.w3, w.b3, lane, h2, h3);
+  mlp_hidden64(w.w2, w.b2, w.act, lane, h1, h2);
+  mlp_hidden64(w.w3, w.b3, w.act, lane, h2, h3);
   // layer 4: [16 x 64] x [64 x 8]
   const float bl = w.b4[t2], bh = w.b4[t2 + 1];
   c[0] = bl;
@@ -238,7 +247,7 @@ AXB_D void mlp_tile(const MlpSmem &w, const uint32_t *stage, int mt, int lane,
 // Hidden layer for both 16-row tiles at once: the two accumulator chains
 // are independent, which doubles the MMAs in flight per warp and reuses
 // each B fragment for both tiles.
-AXB_D void mlp_hidden64x2(const __nv_bfloat16 *wT, const float *bias, int lane,
+AXB_D void mlp_hidden64x2(const __nv_bfloat16 *wT, const float *bias, int act, int lane,
                           const uint32_t (&ain0)[4][4], const uint32_t (&ain1)[4][4],
                           uint32_t (&aout0)[4][4], uint32_t (&aout1)[4][4]) {
   const int t2 = (lane & 3) * 2;
@@ -261,14 +270,14 @@ AXB_D void mlp_hidden64x2(const __nv_bfloat16 *wT, const float *bias, int lane,
         mma_bf16_16816(c1[h], ain1[kk], b0, b1);
       }
     }
-    aout0[kb][0] = pack_bf16x2(silu(c0[0][0]), silu(c0[0][1]));
-    aout0[kb][1] = pack_bf16x2(silu(c0[0][2]), silu(c0[0][3]));
-    aout0[kb][2] = pack_bf16x2(silu(c0[1][0]), silu(c0[1][1]));
-    aout0[kb][3] = pack_bf16x2(silu(c0[1][2]), silu(c0[1][3]));
-    aout1[kb][0] = pack_bf16x2(silu(c1[0][0]), silu(c1[0][1]));
-    aout1[kb][1] = pack_bf16x2(silu(c1[0][2]), silu(c1[0][3]));
-    aout1[kb][2] = pack_bf16x2(silu(c1[1][0]), silu(c1[1][1]));
-    aout1[kb][3] = pack_bf16x2(silu(c1[1][2]), silu(c1[1][3]));
+    aout0[kb][0] = pack_bf16x2(mlp_act(c0[0][0], act), mlp_act(c0[0][1], act));
+    aout0[kb][1] = pack_bf16x2(mlp_act(c0[0][2], act), mlp_act(c0[0][3], act));
+    aout0[kb][2] = pack_bf16x2(mlp_act(c0[1][0], act), mlp_act(c0[1][1], act));
+    aout0[kb][3] = pack_bf16x2(mlp_act(c0[1][2], act), mlp_act(c0[1][3], act));
+    aout1[kb][0] = pack_bf16x2(mlp_act(c1[0][0], act), mlp_act(c1[0][1], act));
+    aout1[kb][1] = pack_bf16x2(mlp_act(c1[0][2], act), mlp_act(c1[0][3], act));
+    aout1[kb][2] = pack_bf16x2(mlp_act(c1[1][0], act), mlp_act(c1[1][1], act));
+    aout1[kb][3] = pack_bf16x2(mlp_act(c1[1][2], act), mlp_act(c1[1][3], act));
   }
 }
 
@@ -291,10 +300,10 @@ AXB_D void mlp_layer1(const MlpSmem &w, const uint32_t (&a1)[4], int lane,
       load_b(w.w1, MLP_LD1, nt, 0, lane, b0, b1);
       mma_bf16_16816(cc[h], a1, b0, b1);
     }
-    h1[kb][0] = pack_bf16x2(silu(cc[0][0]), silu(cc[0][1]));
-    h1[kb][1] = pack_bf16x2(silu(cc[0][2]), silu(cc[0][3]));
-    h1[kb][2] = pack_bf16x2(silu(cc[1][0]), silu(cc[1][1]));
-    h1[kb][3] = pack_bf16x2(silu(cc[1][2]), silu(cc[1][3]));
+    h1[kb][0] = pack_bf16x2(mlp_act(cc[0][0], w.act), mlp_act(cc[0][1], w.act));
+    h1[kb][1] = pack_bf16x2(mlp_act(cc[0][2], w.act), mlp_act(cc[0][3], w.act));
+    h1[kb][2] = pack_bf16x2(mlp_act(cc[1][0], w.act), mlp_act(cc[1][1], w.act));
+    h1[kb][3] = pack_bf16x2(mlp_act(cc[1][2], w.act), mlp_act(cc[1][3], w.act));
   }
 }
 
@@ -310,8 +319,8 @@ AXB_D void mlp_tile2(const MlpSmem &w, const uint32_t *stage, int lane, float (&
   uint32_t p0[4][4], p1[4][4], q0[4][4], q1[4][4];
   mlp_layer1(w, x0, lane, p0);
   mlp_layer1(w, x1, lane, p1);
-  mlp_hidden64x2(w.w2, w.b2, lane, p0, p1, q0, q1);
-  mlp_hidden64x2(w.w3, w.b3, lane, q0, q1, p0, p1);
+  mlp_hidden64x2(w.w2, w.b2, w.act, lane, p0, p1, q0, q1);
+  mlp_hidden64x2(w.w3, w.b3, w.act, lane, q0, q1, p0, p1);
   const float bl = w.b4[t2], bh = w.b4[t2 + 1];
   o0[0] = o1[0] = bl;
   o0[1] = o1[1] = bh;
@@ -358,6 +367,34 @@ AXB_D void mlp_forward_warp(const MlpSmem &w, const float (&f)[MLP_K1], uint32_t
     y0 = r < 8 ? v10 : v12;
     y1 = r < 8 ? v11 : v13;
   }
+}
+
+// The learned guess of cell i of `c` (all 32 lanes of the warp call this;
+// lanes with valid == false take part with zero features): features from
+// the conserved variables and metric, the network, and the decoded guess
+// x = h W (y0 places x in the Palenzuela scheme's initial bracket
+// [max(1e-10, 1 + q - s), 2 + 2 q - s], c2p_1DPalenzuela.hxx:395-398) and
+// W = max(exp(y1), 1).
+template <class Cells>
+AXB_D void mlp_cell_guess(const Cells &c, long long i, bool valid, int nf, const MlpSmem &w,
+                          uint32_t *stage, double &x, double &W) {
+  float f[MLP_K1];
+#pragma unroll
+  for (int k = 0; k < MLP_K1; ++k)
+    f[k] = 0.0f;
+  CellInvariants inv{1.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  if (valid) {
+    const sym3 glo{c.g[0][i], c.g[1][i], c.g[2][i], c.g[3][i], c.g[4][i], c.g[5][i]};
+    const double mom[3] = {c.mom[0][i], c.mom[1][i], c.mom[2][i]};
+    const double dB[3] = {c.dB[0][i], c.dB[1][i], c.dB[2][i]};
+    inv = cell_invariants(c.dens[i], mom, c.tau[i], c.DYe[i], dB, glo);
+    mlp_features(inv, nf, f);
+  }
+  float y0, y1;
+  mlp_forward_warp(w, f, stage, y0, y1);
+  const double lo = fmax(1e-10, 1.0 + inv.q - inv.s), hi = 2.0 + 2.0 * inv.q - inv.s;
+  x = lo + double(y0) * (hi - lo);
+  W = fmax(exp(double(y1)), 1.0);
 }
 
 } // namespace axb

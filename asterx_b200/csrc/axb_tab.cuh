@@ -37,14 +37,20 @@ struct EosTab {
 
   static constexpr bool kTabulated = true;
 
+  // The cell of the uniform axis d holding xin, clamped to [0, n - 2]
+  // (eos_linear_interp_ND.hxx:50-65).  The clamps act on the floating-point
+  // position before it becomes an integer, so a NaN query (the logarithm of
+  // a non-positive temperature that press_from_valid_rho_temp_ye takes
+  // before clamping) and an infinite one map to an end cell instead of an
+  // undefined conversion; finite queries are unchanged.
   AXB_HD int find(int d, double xin) const {
     const double xL = xin - x0[d];
-    if (xL <= 0)
+    if (!(xL > 0))
       return 0;
-    const int index = static_cast<int>(xL * idx[d]);
-    if (index > n[d] - 2)
+    const double t = xL * idx[d];
+    if (!(t < double(n[d] - 2)))
       return n[d] - 2;
-    return index;
+    return static_cast<int>(t);
   }
   AXB_HD static double lin(double A, double B, double xA, double xB, double xv) {
     const double lam = (xv - xA) / (xB - xA);

@@ -69,6 +69,9 @@ def load_library(path=LIB_PATH):
     lib.axb_mlp_param_count.argtypes = [C.c_int]
     lib.axb_mlp_param_count.restype = C.c_int64
     lib.axb_mlp_create.argtypes = [C.c_int, _vp, C.c_uint64, C.c_double, C.POINTER(_vp)]
+    lib.axb_mlp_create_act.argtypes = [C.c_int, C.c_int, _vp, C.c_uint64, C.c_double,
+                                       C.POINTER(_vp)]
+    lib.axb_mlp_create_act.restype = C.c_int
     lib.axb_mlp_destroy.argtypes = [_vp]
     lib.axb_mlp_get_params.argtypes = [_vp, _vp]
     lib.axb_mlp_features.argtypes = [_vp, C.POINTER(abi.Cells), C.c_int, _vp, _vp]
@@ -83,6 +86,13 @@ def load_library(path=LIB_PATH):
     lib.axb_batch_substep.argtypes = [_vp, _vp, C.c_double, C.c_double, C.c_double,
                                       C.c_double, C.c_int, _vp]
     lib.axb_batch_autotune.argtypes = [_vp, _vp, C.POINTER(C.c_int), _vp]
+    lib.axb_import_fields.argtypes = [_vp, C.POINTER(Box), C.POINTER(abi.FieldsStrided),
+                                      C.POINTER(C.c_int), C.c_int, C.POINTER(Fields), _vp]
+    lib.axb_import_fields.restype = C.c_int
+    lib.axb_export_fields.argtypes = [_vp, C.POINTER(Box), C.POINTER(Fields),
+                                      C.POINTER(C.c_int), C.c_int,
+                                      C.POINTER(abi.FieldsStrided), _vp]
+    lib.axb_export_fields.restype = C.c_int
     lib.axb_fill_boundary.argtypes = [_vp, C.POINTER(Box), C.POINTER(Fields),
                                       C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_int), _vp]
     lib.axb_fill_boundary.restype = C.c_int
@@ -202,6 +212,36 @@ class Engine:
                                                 self.stream_ptr(stream)),
                     "axb_con2prim_group")
 
+    @staticmethod
+    def strided_struct(arrays: dict):
+        """axb_fields_strided from {name: (tensor, sy, sz)}."""
+        fs = abi.FieldsStrided()
+        for n, (t, sy, sz) in arrays.items():
+            fs.gf[GF[n]] = t.data_ptr()
+            fs.sy[GF[n]] = int(sy)
+            fs.sz[GF[n]] = int(sz)
+        return fs
+
+    def import_fields(self, layout, strided, names, tensors, stream=None):
+        """axb_import_fields: `strided` {name: (tensor, sy, sz)} into the
+        engine-layout `tensors`."""
+        box = layout.box()
+        fs = self.strided_struct(strided)
+        f = self.fields_struct(tensors)
+        ids = (C.c_int * len(names))(*[GF[n] for n in names])
+        self._check(self.lib.axb_import_fields(self.ctx, C.byref(box), C.byref(fs), ids,
+                                               len(names), C.byref(f), self.stream_ptr(stream)),
+                    "axb_import_fields")
+
+    def export_fields(self, layout, tensors, names, strided, stream=None):
+        box = layout.box()
+        fs = self.strided_struct(strided)
+        f = self.fields_struct(tensors)
+        ids = (C.c_int * len(names))(*[GF[n] for n in names])
+        self._check(self.lib.axb_export_fields(self.ctx, C.byref(box), C.byref(f), ids,
+                                               len(names), C.byref(fs), self.stream_ptr(stream)),
+                    "axb_export_fields")
+
     def fill_boundary(self, layout, tensors, names, bc, stream=None):
         """axb_fill_boundary: the ghost layers of `names` by the face rules
         bc = (x-lower, x-upper, y-lower, y-upper, z-lower, z-upper), each an
@@ -306,25 +346,19 @@ class Engine:
         return abi.cells_struct(n, ptrs)
 
     def c2p_cells(self, cells, params: Params, eos, mlp=None, stream=None):
-        if mlp is not None and not cells.guess:
-            # scratch for the learned guess, kept for later calls of this size
-            n = int(cells.n)
-            buf = getattr(self, "_guess_buf", None)
-            if buf is None or buf.numel() < 2 * n:
-                buf = self.torch.empty(2 * n, dtype=self.torch.float32, device=self.device)
-                self._guess_buf = buf
-            cells.guess = buf.data_ptr()
         self._check(self.lib.axb_c2p_cells(self.ctx, C.byref(cells), C.byref(params), eos,
                                            mlp, self.stream_ptr(stream)), "axb_c2p_cells")
 
-    def mlp_create(self, nf=8, params=None, seed=1, bracket=0.05):
+    def mlp_create(self, nf=8, params=None, seed=1, bracket=0.05, act="silu"):
         h = _vp()
         arr = None
         if params is not None:
             arr = np.ascontiguousarray(params, dtype=np.float32)
             assert arr.size == self.lib.axb_mlp_param_count(nf)
-        self._check(self.lib.axb_mlp_create(nf, None if arr is None else arr.ctypes.data,
-                                            seed, bracket, C.byref(h)), "axb_mlp_create")
+        a = {"silu": 0, "relu": 1}[act]
+        self._check(self.lib.axb_mlp_create_act(nf, a, None if arr is None else arr.ctypes.data,
+                                                seed, bracket, C.byref(h)),
+                    "axb_mlp_create_act")
         self._mlp.append(h)
         return h
 

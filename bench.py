@@ -34,6 +34,9 @@ UNIT = "zone-updates/s"
 SSPRK3 = [(0.0, 1.0, 1.0), (0.75, 0.25, 0.25), (1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0)]
 GAMMA = 4.0 / 3.0
 CFL_MAX = 0.9
+# the tabulated-EOS substep: temperature reconstructed (the tabulated EOS has
+# no eps(rho, p)), atmosphere temperature inside the table
+TAB_PARAMS = dict(reconstruct_with_temperature=1, t_atmo=0.011)
 # the survey's algorithmic figure for one substep: 112 FP64 values per zone
 # (RHS reads 34, stage 33, post-step reads 23 and writes 22)
 SUBSTEP_BYTES = 112 * 8
@@ -82,12 +85,18 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the reference baseline sample")
-    ap.add_argument("--workload", default="substep", choices=["substep", "c2p", "amr"],
+    ap.add_argument("--workload", default="substep", choices=["substep", "tab", "c2p", "amr"],
                     help="substep: the RK3 substep of one box (the headline); "
+                         "tab: the same substep with the synthetic tabulated EOS at "
+                         "192^3, MP5 (the tabulated-EOS configuration); "
                          "c2p: the independent-cell recovery microbenchmark, "
                          "plain seeds vs the learned guess; amr: a level of boxes of "
                          "uneven sizes, batched + CUDA graph vs one launch per box")
     ap.add_argument("--boxes", type=int, default=512, help="boxes of the amr workload")
+    ap.add_argument("--amr-physics", default="config2", choices=["config2", "mild"],
+                    help="amr workload state: config2 = the 256^3 workload's physics "
+                         "(W <= 10, b^2/rho <= 10, 3 jumps) on every box; mild = W <= 2, "
+                         "b^2/rho <= 0.1, no jumps")
     ap.add_argument("--decomp", default="boxes", choices=["boxes", "slab"],
                     help="with several GPUs: boxes = one independent periodic box per rank "
                          "(no data-path collective); slab = the ranks' boxes are z-slabs of "
@@ -97,6 +106,8 @@ def parse_args():
                     help="cells of the recovery microbenchmark")
     ap.add_argument("--train-pairs", type=int, default=1 << 24)
     ap.add_argument("--train-epochs", type=float, default=4.0)
+    ap.add_argument("--mlp-act", default="relu", choices=["relu", "silu"],
+                    help="hidden activation of the learned guess's network")
     return ap.parse_args()
 
 
@@ -193,12 +204,12 @@ class _StdoutToStderr:
         return False
 
 
-def reference_substep_rate(seconds, recon, seed=2, start_n=24, recvar="z"):
+def reference_substep_rate(seconds, recon, seed=2, start_n=24, recvar="z", tab=False):
     with _StdoutToStderr():
-        return _reference_substep_rate(seconds, recon, seed, start_n, recvar)
+        return _reference_substep_rate(seconds, recon, seed, start_n, recvar, tab)
 
 
-def _reference_substep_rate(seconds, recon, seed=2, start_n=24, recvar="z"):
+def _reference_substep_rate(seconds, recon, seed=2, start_n=24, recvar="z", tab=False):
     """Time the reference's scheduled routines (AsterX_Fluxes,
     AsterX_SourceTerms, AsterX_RHS, the stage update, AsterX_ComputedBstagFromA,
     AsterX_ComputedBFromdBstag, AsterX_Con2Prim) on one box of the workload,
@@ -213,18 +224,27 @@ def _reference_substep_rate(seconds, recon, seed=2, start_n=24, recvar="z"):
         raise RuntimeError("oracle/_ref/libaxref.so is not built")
     threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
 
+    table = W.synthetic_table() if tab else None
+
     def one(n, nsub):
-        L, f = W.curved_box(n=n, ng=3, seed=seed, wmax=10.0)
+        if tab:
+            L, f = W.tabulated_box(n=n, ng=3, seed=seed + 3)
+        else:
+            L, f = W.curved_box(n=n, ng=3, seed=seed, wmax=10.0)
         W.cons_from_prims(L, f)
         W.saved_from_prims(f)
         for name in abi.GF_NAMES:
             f.setdefault(name, L.zeros())
         p = abi.default_params(reconstruction_method=recon, flux_type="hlle",
                                c2p_prime="palenzuela", c2p_second="noble",
-                               recon_type={"v": 0, "z": 1, "s": 2}[recvar])
+                               recon_type={"v": 0, "z": 1, "s": 2}[recvar],
+                               **(TAB_PARAMS if tab else {}))
         host = {k: v.copy() for k, v in f.items()}
         ref.setup(L, p, host)
-        ref.eos_idealgas(GAMMA, **EOS_KW)
+        if tab:
+            ref.eos_tabulated(*table)
+        else:
+            ref.eos_idealgas(GAMMA, **EOS_KW)
         dt = 0.25 * L.dx[0]
         evolved = abi.CONS + ["Avec_x", "Avec_y", "Avec_z", "Psi"]
         rhs = abi.HYDRO_RHS + abi.AVEC_RHS
@@ -311,7 +331,11 @@ def ours(args):
                                 device_id=dev)
     eng = Engine(local)
     xp = W._XP(torch, dev)
-    L, f = W.curved_box(n=args.n, ng=3, seed=2 + rank, wmax=10.0, xp=xp)
+    tab = args.workload == "tab"
+    if tab:
+        L, f = W.tabulated_box(n=args.n, ng=3, seed=5 + rank, xp=xp)
+    else:
+        L, f = W.curved_box(n=args.n, ng=3, seed=2 + rank, wmax=10.0, xp=xp)
     W.cons_from_prims(L, f, xp=xp)
     W.saved_from_prims(f, xp=xp)
     # keep only the reconstructed velocity variable the fluxes use (the
@@ -330,8 +354,9 @@ def ours(args):
     fn = {k: f[k].clone() for k in evolved}
     params = abi.default_params(reconstruction_method=args.recon, flux_type="hlle",
                                 c2p_prime="palenzuela", c2p_second="noble",
-                                recon_type={"v": 0, "z": 1, "s": 2}[args.recvar])
-    eos = eng.eos_idealgas(GAMMA, **EOS_KW)
+                                recon_type={"v": 0, "z": 1, "s": 2}[args.recvar],
+                                **(TAB_PARAMS if tab else {}))
+    eos = eng.eos_tabulated(*W.synthetic_table()) if tab else eng.eos_idealgas(GAMMA, **EOS_KW)
     zones = args.n ** 3
     stream = torch.cuda.current_stream(dev)
 
@@ -466,10 +491,10 @@ def ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             rate, sample, threads, _t = reference_substep_rate(args.cpu_seconds, args.recon,
-                                                               recvar=args.recvar)
+                                                               recvar=args.recvar, tab=tab)
             cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
                    "sample": sample}
-            parity = reference_parity(eng, L, f, params, eos, dt)
+            parity = reference_parity(eng, L, f, params, eos, dt, tab=tab)
         except Exception as exc:  # the checker library may be absent
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
                    "sample": f"unavailable: {exc}"}
@@ -483,8 +508,12 @@ def ours(args):
             "config": {"workload": f"{args.n}^3 periodic patch, 3 ghosts, curved static "
                                    f"metric, W <= 10, b^2/rho <= 10, 3 planar jumps, "
                                    f"{args.recon}+HLLE on {args.recvar}_vec, flux-CT, "
-                                   f"Palenzuela c2p (Noble backup), ideal gas Gamma=4/3, "
-                                   f"SSP-RK3 substeps",
+                                   f"Palenzuela c2p (Noble backup), " +
+                                   ("synthetic tabulated EOS 200x100x60 (P = rho T (1+Ye) "
+                                    "+ T^4/3 + 100 rho^2), Ye in [0.05, 0.5], temperature "
+                                    "reconstructed" if tab else "ideal gas Gamma=4/3") +
+                                   ", SSP-RK3 substeps",
+                       "eos": "tabulated3d" if tab else "idealgas",
                        "box": [args.n] * 3, "ghosts": 3, "recon": args.recon,
                        "recon_type": f"{args.recvar}_vec", "dt_over_dx": dt / L.dx[0],
                        "cfl": dt * smax0 * sum(1.0 / d for d in L.dx),
@@ -524,7 +553,7 @@ def ours(args):
     return 0
 
 
-def reference_parity(eng, L, f, params, eos, dt, m=40, off=8, ng_ref=5):
+def reference_parity(eng, L, f, params, eos, dt, m=40, off=8, ng_ref=5, tab=False):
     """The checker half of the CPU-baseline leg: one substep (RHS group,
     stage U + dt RHS, post-step group; no ghost fill in between) of a
     m^3 sub-box cut from the timed state, on the engine (3 ghost zones) and
@@ -535,6 +564,7 @@ def reference_parity(eng, L, f, params, eos, dt, m=40, off=8, ng_ref=5):
     import torch
 
     from asterx_b200 import abi
+    from asterx_b200 import workloads as W
     from asterx_b200.abi import Layout
     from oracle.oracle import reference
     ref = reference()
@@ -578,7 +608,10 @@ def reference_parity(eng, L, f, params, eos, dt, m=40, off=8, ng_ref=5):
         host.setdefault(name, L5.zeros())
     with _StdoutToStderr():
         ref.setup(L5, params, host)
-        ref.eos_idealgas(GAMMA, **EOS_KW)
+        if tab:
+            ref.eos_tabulated(*W.synthetic_table())
+        else:
+            ref.eos_idealgas(GAMMA, **EOS_KW)
         ref.rhs_group()
         want_rhs = {k: host[k].copy() for k in rhs}
         for u, r in zip(evolved, rhs):
@@ -654,7 +687,7 @@ def c2p_bench(args):
     eng.mlp_features(eng.cells(nt, {k: tr[k] for k in abi.CELL_INPUTS}), 8, feats)
     tgt = torch.stack([tr["t_u"], tr["t_lnw"]], dim=1).float().contiguous()
     del tr
-    mlp = eng.mlp_create(8, seed=7, bracket=0.02)
+    mlp = eng.mlp_create(8, seed=7, bracket=0.02, act=args.mlp_act)
     loss = torch.zeros(1, dtype=torch.float32, device=dev)
     bs = 65536
     nsteps = max(1, int(args.train_epochs * nt / bs))
@@ -673,12 +706,10 @@ def c2p_bench(args):
     cells = W.c2p_cells(n, seed=2002, gamma=gamma, device=dev)
     truth = {k: cells[k] for k in ("rho", "eps", "press", "W")}
     t = {k: cells[k] for k in abi.CELL_INPUTS}
-    outs = ["rho", "eps", "press", "w_lorentz", "iters", "flag"]
+    outs = ["rho", "eps", "press", "w_lorentz", "iters", "flag", "fallback"]
     for k in outs:
         t[k] = torch.empty(n, dtype=torch.float64, device=dev)
-    guess = torch.empty(2 * n, dtype=torch.float32, device=dev)
     cstruct = eng.cells(n, t)
-    cstruct.guess = guess.data_ptr()
     stream = torch.cuda.current_stream(dev)
     res = {}
     for name, m in (("plain", None), ("learned", mlp)):
@@ -712,11 +743,15 @@ def c2p_bench(args):
             "cells_per_s": n / (ms / 1e3), "ms": ms,
             "mean_iters": float((hist * it).sum() / max(1, hist.sum())),
             "iter_hist": {int(i): int(v) for i, v in enumerate(hist) if v},
-            "fallback_rate": float((~ok).double().mean().item()),
+            # cells whose guessed first attempt failed and went to the plain
+            # cold-start cascade (0 without a guess), and cells not recovered
+            # by the first scheme
+            "fallback_rate": float(t["fallback"].mean().item()),
+            "second_scheme_or_worse_rate": float((~ok).double().mean().item()),
             "fail_rate": float((flag == abi.C2P_FAIL).double().mean().item()),
             "max_rel_err": errs,
             "recovery_kernel_ms": region_ms[REGIONS.index("c2p_cells")] / max(1, args.steps),
-            "mlp_kernel_ms": region_ms[REGIONS.index("mlp")] / max(1, args.steps),
+            # (the network runs inside the recovery kernel: no separate launch)
             "gpu_launches": int(sum(region_n)),
         }
     alg = 8 * (16 + 8)  # bytes per cell: 16 inputs read, 8 outputs written
@@ -731,7 +766,8 @@ def c2p_bench(args):
         "data": "synthetic (seeded cells of the configuration)",
         "config": {"workload": f"{n} independent cells, Noble (Palenzuela backup), "
                                "ideal gas Gamma=5/3, c2p_tol 1e-10, MLP 8-64-64-64-2 "
-                               f"trained on {nt} pairs",
+                               f"({args.mlp_act}) trained on {nt} pairs, evaluated "
+                               "inside the recovery kernel",
                    "cells": n, "l2": "inputs larger than L2"},
         "plain": res["plain"], "learned": res["learned"],
         "speedup_learned_vs_plain": lr_["cells_per_s"] / res["plain"]["cells_per_s"],
@@ -783,10 +819,18 @@ def amr_bench(args):
     skip = {"zvec_x", "zvec_y", "zvec_z", "svec_x", "svec_y", "svec_z", "dBx", "dBy", "dBz"}
     layouts, fields = [], []
     for b, n in enumerate(shapes):
-        L, f = W.curved_box(n=n, ng=3, seed=1000 + b, wmax=2.0, njumps=0,
-                            sigma=(1e-3, 0.1), xp=xp)
+        if args.amr_physics == "config2":
+            L, f = W.curved_box(n=n, ng=3, seed=1000 + b, wmax=10.0, xp=xp)
+        else:
+            L, f = W.curved_box(n=n, ng=3, seed=1000 + b, wmax=2.0, njumps=0,
+                                sigma=(1e-3, 0.1), xp=xp)
         W.cons_from_prims(L, f, xp=xp)
         W.saved_from_prims(f, xp=xp)
+        for ax in "xyz":
+            if args.recvar != "z":
+                f.pop("zvec_" + ax, None)
+            if args.recvar != "s":
+                f.pop("svec_" + ax, None)
         for name in abi.GF_NAMES:
             if name not in f and name not in skip:
                 f[name] = torch.zeros(L.size, dtype=torch.float64, device=dev)
@@ -810,9 +854,19 @@ def amr_bench(args):
         fields_n.append(fn)
     zones = sum(n[0] * n[1] * n[2] for n in shapes)
     params = abi.default_params(reconstruction_method=args.recon, flux_type="hlle",
-                                c2p_prime="palenzuela", c2p_second="noble")
+                                c2p_prime="palenzuela", c2p_second="noble",
+                                recon_type={"v": 0, "z": 1, "s": 2}[args.recvar])
     eos = eng.eos_idealgas(GAMMA, **EOS_KW)
-    dt = 0.25 / 64
+    # one time step for the level: dtfac times the finest spacing, capped by
+    # the CFL limit of the largest characteristic speed over all boxes
+    from asterx_b200.distribute import cfl_dt
+    eng.status_reset()
+    smax = 0.0
+    dxmin = min(min(L.dx) for L in layouts)
+    for L, f in zip(layouts, fields):
+        eng.rhs_group(L, f, params, eos)
+    smax = eng.status()["max_speed"]
+    dt = cfl_dt(smax, (dxmin,) * 3, args.dtfac, CFL_MAX)
     stream = torch.cuda.current_stream(dev)
     # keep a pristine copy so both modes start from the same state
     pristine = arena.clone()
@@ -879,11 +933,14 @@ def amr_bench(args):
         "ms_per_step": ms_b / sub, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded boxes of the level)",
         "config": {"workload": f"{args.boxes} boxes, edges log-uniform in [16, 64] per axis, "
-                               f"3 ghosts, curved metric, W <= 2, sigma <= 0.1, "
-                               f"{args.recon}+HLLE, Palenzuela c2p, "
+                               f"3 ghosts, curved metric, " +
+                               ("W <= 10, sigma <= 10, 3 jumps, " if args.amr_physics ==
+                                "config2" else "W <= 2, sigma <= 0.1, no jumps, ") +
+                               f"{args.recon}+HLLE on {args.recvar}_vec, Palenzuela c2p, "
                                "Gamma=4/3, SSP-RK3; batched persistent launches in a CUDA "
                                "graph vs one launch per box",
                    "boxes": args.boxes, "zones": zones, "recon": args.recon,
+                   "dt": dt, "max_char_speed_initial": smax,
                    "l2": "level data far larger than L2"},
         "per_box_launch": {"value": v_a, "ms_per_step": ms_a / sub,
                            "host_wall_s": wall_a, "launches_per_substep": 11 * args.boxes},
@@ -911,6 +968,10 @@ def main():
         return c2p_bench(args)
     if args.workload == "amr":
         return amr_bench(args)
+    if args.workload == "tab" and "--n" not in sys.argv:
+        args.n = 192
+    if args.workload == "tab" and "--recon" not in sys.argv:
+        args.recon = "mp5"
     return ours(args)
 
 

@@ -295,6 +295,34 @@ AXB_API int axb_sync_periodic(axb_ctx *ctx, const axb_box *box,
                               void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* grid functions in the caller's own per-centring layouts                   */
+/* ------------------------------------------------------------------------ */
+
+/* A set of grid functions each with its own j and k strides: gf[id] points at
+ * the field's point (0, 0, 0) (the first ghost point of the box in every
+ * direction) and holds its centring's n[d] + 2*ng (cell) or n[d] + 2*ng + 1
+ * (vertex) points per direction at f[i + sy[id]*j + sz[id]*k] -- the layout
+ * CarpetX gives each centring of a box (a cell-centred field one point
+ * shorter per cell direction than a vertex-centred one).  No counterpart in
+ * the reference, whose GF3D2 views carry these strides per field. */
+typedef struct axb_fields_strided {
+  double *gf[AXB_NUM_GF];
+  int64_t sy[AXB_NUM_GF], sz[AXB_NUM_GF];
+} axb_fields_strided;
+
+/* Copy the grid functions ids[0..nids) of `src` (per-field strides) into
+ * the engine's layout of `box` (`dst`, strides box->sy, box->sz), every
+ * point of each field's centring, ghosts included; axb_export_fields copies
+ * back.  A caller whose fields are laid out per centring wraps the engine's
+ * groups with these copies (one read and one write per point). */
+AXB_API int axb_import_fields(axb_ctx *ctx, const axb_box *box,
+                              const axb_fields_strided *src, const int *ids, int nids,
+                              const axb_fields *dst, void *stream);
+AXB_API int axb_export_fields(axb_ctx *ctx, const axb_box *box, const axb_fields *src,
+                              const int *ids, int nids, const axb_fields_strided *dst,
+                              void *stream);
+
+/* ------------------------------------------------------------------------ */
 /* physical outer boundaries and general Runge-Kutta methods                 */
 /* ------------------------------------------------------------------------ */
 
@@ -399,8 +427,11 @@ AXB_API int axb_batch_autotune(axb_ctx *ctx, axb_batch *batch, int *out, void *s
  * Seeds (saved primitives: rho, eps, Ye, vel^i, temperature) may all be NULL
  * for a cold start: v = 0, eps = the atmosphere's eps, Ye = DYe/dens.
  * Outputs (any may be NULL): rho, eps, press, vel^i, w_lorentz, Ye,
- * temperature, entropy, the iteration count of the first solver (double),
- * and the con2prim flag (AXB_C2P_* code, as double). */
+ * temperature, entropy, the iteration count of the first solver (double;
+ * with a learned guess that failed, its attempt and the cold-start retry
+ * together), the con2prim flag (AXB_C2P_* code, as double), and with a
+ * learned guess `fallback` (1 where the guessed first attempt failed and the
+ * plain cascade recovered or failed the cell, else 0). */
 typedef struct axb_cells {
   int64_t n;
   const double *dens, *mom[3], *tau, *DYe, *DEnt, *dB[3];
@@ -408,7 +439,8 @@ typedef struct axb_cells {
   const double *seed_rho, *seed_eps, *seed_Ye, *seed_vel[3], *seed_temperature;
   double *rho, *eps, *press, *vel[3], *w_lorentz, *Ye, *temperature, *entropy;
   double *iters, *flag;
-  float *guess; /* scratch, 2 floats per cell; required with a learned guess */
+  float *guess;     /* unused (the guess stays in registers); may be NULL */
+  double *fallback; /* output, may be NULL */
 } axb_cells;
 
 /* Learned initial guess: an MLP nf -> 64 -> 64 -> 64 -> 2 (SiLU hidden
@@ -421,9 +453,12 @@ typedef struct axb_cells {
  * (c2p_2DNoble.hxx:374-393), the Palenzuela scheme brackets x by
  * [x (1 - bracket), x (1 + bracket)] when that interval brackets the root
  * and otherwise keeps its own bracket (c2p_1DPalenzuela.hxx:395-401).
- * The network runs in its own kernel before the recovery (a persistent
- * grid whose CTAs stage the weights in shared memory once) and leaves
- * (x, W) per cell in the caller's `guess` scratch.
+ * The network runs inside the recovery kernel: each CTA stages the weights
+ * in shared memory, each warp evaluates its 32 cells on the tensor cores and
+ * the guess stays in registers.  A cell whose guessed first attempt fails is
+ * retried from the plain cold-start seeds of c2p_2DNoble.hxx:374-393 (and
+ * the plain bracket) before the second scheme, so the cascade after a
+ * failed guess is exactly the plain one.
  * No counterpart in the reference. */
 typedef struct axb_mlp axb_mlp;
 
@@ -440,6 +475,15 @@ AXB_API int64_t axb_mlp_param_count(int nf);
  * NULL.  `bracket` is the relative half-width of the Palenzuela bracket. */
 AXB_API int axb_mlp_create(int nf, const float *params, uint64_t seed,
                            double bracket, axb_mlp **out);
+
+/* Hidden activations of the network. */
+#define AXB_MLP_SILU 0 /* z sigmoid(z) (axb_mlp_create's choice)           */
+#define AXB_MLP_RELU 1 /* max(z, 0): no special-function instruction       */
+
+/* axb_mlp_create with the hidden activation chosen (AXB_MLP_SILU or
+ * AXB_MLP_RELU); training and inference use it alike. */
+AXB_API int axb_mlp_create_act(int nf, int activation, const float *params,
+                               uint64_t seed, double bracket, axb_mlp **out);
 AXB_API int axb_mlp_destroy(axb_mlp *mlp);
 /* Copy the FP32 master parameters to host memory (param_count floats). */
 AXB_API int axb_mlp_get_params(const axb_mlp *mlp, float *params);

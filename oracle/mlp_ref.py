@@ -9,7 +9,7 @@ and the input features against an independent implementation:
                        variables and gamma_ij, built on the Palenzuela
                        invariants q, r, s, t (Con2PrimFactory/src/
                        c2p_1DPalenzuela.hxx:150-153,267-270);
-* ``forward``       -- nf -> 64 -> 64 -> 64 -> 2 with SiLU, BF16 rounding
+* ``forward``       -- nf -> 64 -> 64 -> 64 -> 2 with SiLU or ReLU, BF16 rounding
                        of inputs, weights and hidden activations
                        (round-to-nearest-even), wide accumulation;
 * ``loss_and_grad`` -- mean squared error and its gradient by backward
@@ -58,12 +58,25 @@ def dsilu(z):
     return s * (1.0 + z * (1.0 - s))
 
 
+def relu(z):
+    return np.maximum(z, 0.0)
+
+
+def drelu(z):
+    return (z > 0.0).astype(np.float64)
+
+
+ACTS = {"silu": (silu, dsilu), "relu": (relu, drelu)}
+
+
 def _r(x, rounding):
     return bf16r(x).astype(np.float64) if rounding else np.asarray(x, dtype=np.float64)
 
 
-def forward(params, feats, rounding=True):
-    """Outputs (n x 2) and the intermediates backward needs."""
+def forward(params, feats, rounding=True, act="silu"):
+    """Outputs (n x 2) and the intermediates backward needs (hidden
+    activation `act`: "silu" or "relu")."""
+    silu = ACTS[act][0]
     nf = feats.shape[1]
     p = unpack(params, nf)
     W = {k: _r(p[k], rounding) for k in ("w1", "w2", "w3", "w4")}
@@ -78,9 +91,10 @@ def forward(params, feats, rounding=True):
     return Y, dict(X=X, Z1=Z1, H1=H1, Z2=Z2, H2=H2, Z3=Z3, H3=H3, W=W)
 
 
-def loss_and_grad(params, feats, targets, rounding=True):
+def loss_and_grad(params, feats, targets, rounding=True, act="silu"):
+    dsilu = ACTS[act][1]
     n, nf = feats.shape
-    Y, c = forward(params, feats, rounding)
+    Y, c = forward(params, feats, rounding, act)
     R = Y - targets
     loss = float(np.sum(R * R) / n)
     dY = 2.0 * R / n

@@ -5,8 +5,13 @@
   primitives within 1e-10 (the primitive tolerance of the parity tests).
 * The input features, the tensor-core forward pass and the training
   gradient against the numpy checker (oracle/mlp_ref.py).
-* A briefly trained guess: the recovered primitives equal the plain ones
-  within 1e-10 and the Noble iteration count drops.
+* A briefly trained guess (SiLU and ReLU hidden activations), evaluated
+  inside the recovery kernel: the recovered primitives equal the plain ones
+  within 1e-10, the Noble iteration count drops, and the cells whose guessed
+  attempt failed (reported per cell) took the plain cold-start cascade.
+* The tabulated EOS with a 9-input network (Ye as the ninth feature) and
+  Palenzuela as the first scheme: same primitives as the plain recovery,
+  fewer Brent iterations.
 """
 import numpy as np
 import pytest
@@ -85,7 +90,8 @@ def test_c2p_cells_matches_reference(engine, ref, solver):
 
 
 @pytest.mark.gpu
-def test_mlp_features_forward_and_gradient(engine):
+@pytest.mark.parametrize("act", ["silu", "relu"])
+def test_mlp_features_forward_and_gradient(engine, act):
     torch = engine.torch
     n = 4096
     cells = W.c2p_cells(n, seed=12, gamma=GAMMA)
@@ -96,12 +102,12 @@ def test_mlp_features_forward_and_gradient(engine):
     got = feats.cpu().numpy()
     assert np.allclose(got, want, rtol=1e-6, atol=1e-6)
 
-    mlp = engine.mlp_create(8, seed=5)
+    mlp = engine.mlp_create(8, seed=5, act=act)
     params = engine.mlp_params(mlp, 8)
     out = torch.zeros((n, 2), dtype=torch.float32, device=engine.device)
     engine.mlp_forward(mlp, feats, out)
     y_gpu = out.cpu().numpy()
-    y_ref, _ = mlp_ref.forward(params, want)
+    y_ref, _ = mlp_ref.forward(params, want, act=act)
     err = np.abs(y_gpu - y_ref)
     # identical rounding points; differences come from the FP32 summation
     # order and the hardware tanh in the inference SiLU (relative error
@@ -114,7 +120,7 @@ def test_mlp_features_forward_and_gradient(engine):
     grad = torch.zeros(params.size, dtype=torch.float32, device=engine.device)
     loss = torch.zeros(1, dtype=torch.float32, device=engine.device)
     engine.mlp_train_step(mlp, feats, tg, loss=loss, grad=grad)
-    l_ref, g_ref = mlp_ref.loss_and_grad(params, want, tgt)
+    l_ref, g_ref = mlp_ref.loss_and_grad(params, want, tgt, act=act)
     g = grad.cpu().numpy()
     assert abs(loss.item() - l_ref) <= 1e-4 * l_ref
     assert np.linalg.norm(g - g_ref) <= 2e-3 * np.linalg.norm(g_ref)
@@ -123,29 +129,34 @@ def test_mlp_features_forward_and_gradient(engine):
     assert not np.array_equal(engine.mlp_params(mlp, 8), params)
 
 
-@pytest.mark.gpu
-def test_learned_guess_same_answer_fewer_iterations(engine):
+def train_guess(engine, nt, seed, gamma, act, nf=8, steps=1500, **kw):
     torch = engine.torch
     dev = engine.device
-    nt = 1 << 17
-    train = W.c2p_cells(nt, seed=101, gamma=GAMMA, device=dev)
+    train = W.c2p_cells(nt, seed=seed, gamma=gamma, device=dev, **kw)
     tt = {k: train[k] for k in abi.CELL_INPUTS}
-    feats = torch.zeros((nt, 8), dtype=torch.float32, device=dev)
-    engine.mlp_features(engine.cells(nt, tt), 8, feats)
+    feats = torch.zeros((nt, nf), dtype=torch.float32, device=dev)
+    engine.mlp_features(engine.cells(nt, tt), nf, feats)
     tgt = torch.stack([train["t_u"], train["t_lnw"]], dim=1).float().contiguous()
-    mlp = engine.mlp_create(8, seed=7, bracket=0.05)
+    mlp = engine.mlp_create(nf, seed=7, bracket=0.05, act=act)
     loss = torch.zeros(1, dtype=torch.float32, device=dev)
     g = torch.Generator(device=dev)
     g.manual_seed(0)
     bs = 8192
-    for step in range(1500):
+    for step in range(steps):
         idx = torch.randint(0, nt, (bs,), generator=g, device=dev)
-        lr = 3e-3 if step < 1000 else 1e-3
+        lr = 3e-3 if step < 2 * steps // 3 else 1e-3
         engine.mlp_train_step(mlp, feats[idx].contiguous(), tgt[idx].contiguous(), lr=lr,
                               loss=loss)
-    final = loss.item()
-    assert final < 0.2, final
+    return mlp, loss.item()
 
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("act", ["silu", "relu"])
+def test_learned_guess_same_answer_fewer_iterations(engine, act):
+    torch = engine.torch
+    dev = engine.device
+    mlp, final = train_guess(engine, 1 << 17, 101, GAMMA, act)
+    assert final < 0.2, final
     n = 1 << 14
     cells = W.c2p_cells(n, seed=202, gamma=GAMMA, device=dev)
     p = abi.default_params(c2p_prime="noble", c2p_second="palenzuela", **PARAMS)
@@ -153,11 +164,19 @@ def test_learned_guess_same_answer_fewer_iterations(engine):
     res = {}
     for name, m in (("plain", None), ("learned", mlp)):
         t = {k: cells[k] for k in abi.CELL_INPUTS}
-        for k in OUT:
+        for k in OUT + ["fallback"]:
             t[k] = torch.full((n,), float("nan"), dtype=torch.float64, device=dev)
         engine.c2p_cells(engine.cells(n, t), p, eos, mlp=m)
-        res[name] = {k: t[k].cpu().numpy() for k in OUT}
+        res[name] = {k: t[k].cpu().numpy() for k in OUT + ["fallback"]}
     a, b = res["plain"], res["learned"]
+    # every cell reports whether its guessed attempt fell back; the plain run
+    # has no guess and no fallback
+    assert np.isin(b["fallback"], (0.0, 1.0)).all() and (a["fallback"] == 0).all()
+    assert b["fallback"].mean() < 0.05, b["fallback"].mean()
+    # the plain cascade takes over after a failed guess: those cells end as
+    # the plain run ended them
+    fb = b["fallback"] == 1
+    assert np.array_equal(a["flag"][fb] == abi.C2P_FAIL, b["flag"][fb] == abi.C2P_FAIL)
     both = (a["flag"] == abi.C2P_PRIME) & (b["flag"] == abi.C2P_PRIME)
     assert both.mean() > 0.9
     for k in ("rho", "w_lorentz", "velx", "vely", "velz"):
@@ -169,4 +188,38 @@ def test_learned_guess_same_answer_fewer_iterations(engine):
     ra = a["rho"][both]
     scale = ra * (1.0 + ea) + a["press"][both]
     assert (np.abs(b["press"][both] - a["press"][both]) / scale).max() <= 1e-10
+    ok = both & ~fb
+    assert b["iters"][ok].mean() < a["iters"][ok].mean()
+
+
+@pytest.mark.gpu
+def test_learned_guess_tabulated_ye(engine):
+    """Tabulated EOS: a 9-input network (Ye the ninth feature), Palenzuela
+    first (the reference has no tabulated Noble): the guessed bracket gives
+    the plain primitives within the tolerance in fewer Brent steps."""
+    torch = engine.torch
+    dev = engine.device
+    lr, lt, ye, table = W.synthetic_table()
+    eos = engine.eos_tabulated(lr, lt, ye, table)
+    kw = dict(ye=(0.05, 0.5), rho_range=(1e-10, 1e-3), eps_range=(0.05, 5.0),
+              w_range=(1.0, 5.0), sigma_range=(1e-3, 1.0))
+    mlp, final = train_guess(engine, 1 << 15, 303, GAMMA, "relu", nf=9, steps=600, **kw)
+    assert np.isfinite(final)
+    n = 1 << 12
+    cells = W.c2p_cells(n, seed=404, gamma=GAMMA, device=dev, **kw)
+    p = abi.default_params(c2p_prime="palenzuela", c2p_second="none", c2p_tol=1e-12,
+                           max_iter=100, vw_lim=60.0, B_lim=1e8, rho_abs_min=1e-20,
+                           t_atmo=0.011)
+    res = {}
+    for name, m in (("plain", None), ("learned", mlp)):
+        t = {k: cells[k] for k in abi.CELL_INPUTS}
+        for k in OUT + ["fallback"]:
+            t[k] = torch.full((n,), float("nan"), dtype=torch.float64, device=dev)
+        engine.c2p_cells(engine.cells(n, t), p, eos, mlp=m)
+        res[name] = {k: t[k].cpu().numpy() for k in OUT + ["fallback"]}
+    a, b = res["plain"], res["learned"]
+    both = (a["flag"] == abi.C2P_PRIME) & (b["flag"] == abi.C2P_PRIME)
+    assert both.mean() > 0.8, both.mean()
+    for k in ("rho", "w_lorentz"):
+        assert relerr(b[k][both], a[k][both]).max() <= 1e-9, k
     assert b["iters"][both].mean() < a["iters"][both].mean()
