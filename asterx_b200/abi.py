@@ -65,6 +65,11 @@ C2P = {"none": 0, "noble": 1, "palenzuela": 2, "entropy": 3}
 C2P_INIT, C2P_PRIME, C2P_SECOND, C2P_ENTROPY, C2P_ATMO, C2P_AVG, C2P_FAIL = range(7)
 # outer-boundary rules (axb_bc)
 BC_PERIODIC, BC_NEUMANN, BC_LINEAR = 0, 1, 2
+# regrid error indicators (axb_regrid), by the regrid_method keyword
+REGRID = {"first derivative": 0, "second derivative": 1, "second derivative norm": 2,
+          "first gradient": 3}
+# the stress-energy tensor components, in the order axb_tmunu takes them
+TMUNU = ["eTtt", "eTtx", "eTty", "eTtz", "eTxx", "eTxy", "eTxz", "eTyy", "eTyz", "eTzz"]
 # device error-word bits (AXB_EW_* in include/asterx_b200.h)
 EW_NAN_FLUX, EW_NAN_RHS, EW_C2P_FAIL, EW_ROOT_CAP, EW_QUEUE_TIMEOUT = 1, 2, 4, 8, 16
 

@@ -21,6 +21,8 @@ enum axb_region {
   AXB_R_C2P,
   AXB_R_C2P_CELLS,
   AXB_R_MLP,
+  AXB_R_TMUNU,
+  AXB_R_ERROR,
   AXB_NREGIONS
 };
 constexpr int AXB_EVENT_POOL = 4096;

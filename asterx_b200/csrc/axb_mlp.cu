@@ -177,6 +177,33 @@ __global__ void __launch_bounds__(256) k_mlp_forward(const MlpDev m, const float
   }
 }
 
+// Learned guess of independent cells, ahead of the recovery: features from
+// the conserved variables and metric, the network, and the decoded guess
+// (x = h W, W) per cell.  A persistent grid: each CTA stages the weights
+// once and its warps walk chunks of 32 cells.  (Evaluated inside the
+// recovery kernel instead, the network's fragments and the recovery's
+// state together exceed the recovery's register budget; the separate
+// launch costs one 8-byte write and read per cell.)
+__global__ void __launch_bounds__(256) k_mlp_guess(const axb_cells c, const MlpDev m,
+                                                   float2 *guess) {
+  __shared__ MlpSmem w;
+  __shared__ uint32_t stage[8][32 * 8];
+  mlp_stage_weights(m, w);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+  const long long nchunks = (c.n + 31) / 32;
+  for (long long ch = warp0; ch < nchunks; ch += nwarps) { // warp-uniform
+    const long long i = ch * 32 + lane;
+    const bool valid = i < c.n;
+    double x, W;
+    mlp_cell_guess(c, i, valid, m.nf, w, stage[threadIdx.x >> 5], x, W);
+    if (valid)
+      guess[i] = make_float2(float(x), float(W));
+  }
+}
+
 // ---------------------------------------------------------------------------
 // training
 // ---------------------------------------------------------------------------
@@ -520,6 +547,22 @@ AXB_API int axb_mlp_forward(axb_ctx *c, const axb_mlp *m, const float *features,
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
 }
 
+
+namespace axb {
+int launch_mlp_guess(const axb_cells &c, const axb_mlp *m, float2 *guess, cudaStream_t s) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long chunks = (c.n + 31) / 32;
+  long long blocks = (chunks + 7) / 8;
+  if (blocks > 4LL * sms) // persistent: a few CTAs per SM amortise the weight copy
+    blocks = 4LL * sms;
+  if (blocks < 1)
+    return AXB_OK;
+  k_mlp_guess<<<(unsigned)blocks, 256, 0, s>>>(c, m->dev(), guess);
+  return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+}
+} // namespace axb
 
 AXB_API int axb_mlp_train_step(axb_ctx *c, axb_mlp *m, const float *features,
                                const float *targets, int64_t n, float lr, float beta1,

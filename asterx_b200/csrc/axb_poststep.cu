@@ -838,6 +838,7 @@ AXB_API int axb_con2prim_group(axb_ctx *c, const axb_box *box,
 namespace axb {
 MlpDev mlp_device_view(const axb_mlp *m);
 int mlp_nf(const axb_mlp *m);
+int launch_mlp_guess(const axb_cells &c, const axb_mlp *m, float2 *guess, cudaStream_t s);
 
 struct C2PCellsArgs {
   axb_cells c;
@@ -862,37 +863,16 @@ AXB_D void run_solver_cells(int which, const EOS &eos, const C2PCellsArgs &a, Pr
     palenzuela_solve(eos, a.cp, a.atmo, pv, cv, glo, rep, xlo, xhi);
 }
 
-// MLP: the learned guess evaluated in this kernel (weights staged in shared
-// memory by the CTA, each warp's 32 cells through the network on the tensor
-// cores, the guess kept in registers).
-template <class EOS, bool MLP>
+template <class EOS>
 __global__ void __launch_bounds__(128, AXB_C2P_MINB)
     k_c2p_cells(const C2PCellsArgs a, const EOS eos) {
   __shared__ unsigned int s_hist[64];
   for (int q = threadIdx.x; q < 64; q += blockDim.x)
     s_hist[q] = 0;
-  const axb_cells &c = a.c;
-  // with the learned guess the grid is persistent: each CTA stages the
-  // network's weights once and walks chunks of 128 cells
-  const MlpSmem *wp = nullptr;
-  uint32_t *stp = nullptr;
-  if constexpr (MLP) {
-    __shared__ MlpSmem w;
-    __shared__ uint32_t stage[4][32 * 8];
-    mlp_stage_weights(a.mlp, w);
-    wp = &w;
-    stp = stage[threadIdx.x >> 5];
-  }
   __syncthreads();
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  // the loop condition is uniform over the CTA (its first cell), so every
-  // warp-level step below sees full warps
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-       i - (long long)threadIdx.x < c.n; i += stride) {
+  const axb_cells &c = a.c;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < c.n;
-  double gx = -1.0, gW = -1.0;
-  if constexpr (MLP)
-    mlp_cell_guess(c, i, valid, a.mlp.nf, *wp, stp, gx, gW);
   Cons cv;
   sym3 glo{1, 0, 0, 1, 0, 1};
   if (valid) {
@@ -906,10 +886,11 @@ __global__ void __launch_bounds__(128, AXB_C2P_MINB)
     cv.DEnt = c.DEnt ? c.DEnt[i] : 0.0;
     glo = sym3{c.g[0][i], c.g[1][i], c.g[2][i], c.g[3][i], c.g[4][i], c.g[5][i]};
   }
-  // learned guess (x = h W, W)
+  // learned guess (x = h W, W) from k_mlp_guess
   double zguess = -1.0, vsqguess = -1.0, xlo = -1.0, xhi = -1.0;
-  if (MLP && valid) {
-    const double x = gx, W = gW;
+  if (a.use_mlp && valid) {
+    const float2 gs = reinterpret_cast<const float2 *>(c.guess)[i];
+    const double x = gs.x, W = gs.y;
     zguess = cv.dens / sqrt(det3(glo)) * x; // Z = rho h W^2 = D (h W)
     vsqguess = 1.0 - 1.0 / (W * W);
     xlo = x * (1.0 - a.bracket);
@@ -1038,7 +1019,6 @@ __global__ void __launch_bounds__(128, AXB_C2P_MINB)
   }
   if (iters_first >= 0)
     atomicAdd(&s_hist[min(iters_first, 63)], 1u);
-  }
   __syncthreads();
   for (int q = threadIdx.x; q < 64; q += blockDim.x)
     if (s_hist[q])
@@ -1075,6 +1055,8 @@ AXB_API int axb_c2p_cells(axb_ctx *ctx, const axb_cells *cells, const axb_params
   a.use_mlp = mlp != nullptr;
   a.bracket = 0.0;
   if (mlp) {
+    if (!cells->guess)
+      return AXB_ERR_ARG;
     a.mlp = mlp_device_view(mlp);
     a.bracket = a.mlp.bracket;
     if (eos->kind == 1 && mlp_nf(mlp) != 9)
@@ -1105,27 +1087,22 @@ AXB_API int axb_c2p_cells(axb_ctx *ctx, const axb_cells *cells, const axb_params
   }
   if (cells->n == 0)
     return AXB_OK;
-  long long blocks = (cells->n + 127) / 128;
+  const long long blocks = (cells->n + 127) / 128;
   if (blocks > 0x7fffffffLL)
     return AXB_ERR_TOO_LARGE;
-  if (mlp) { // persistent: the weight copy is amortised over many cells
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
-    blocks = std::min<long long>(blocks, (long long)AXB_C2P_MINB * sms);
-  }
   cudaStream_t s = (cudaStream_t)stream;
-  axb_mark(ctx, AXB_R_C2P_CELLS, s, true);
-  if (eos->kind == 1) {
-    if (mlp)
-      k_c2p_cells<EosTab, true><<<(unsigned)blocks, 128, 0, s>>>(a, tab_for_launch(*eos, a.status));
-    else
-      k_c2p_cells<EosTab, false><<<(unsigned)blocks, 128, 0, s>>>(a, tab_for_launch(*eos, a.status));
-  } else {
-    if (mlp)
-      k_c2p_cells<EosIdeal, true><<<(unsigned)blocks, 128, 0, s>>>(a, eos->ideal);
-    else
-      k_c2p_cells<EosIdeal, false><<<(unsigned)blocks, 128, 0, s>>>(a, eos->ideal);
+  if (mlp) {
+    axb_mark(ctx, AXB_R_MLP, s, true);
+    const int rc = launch_mlp_guess(*cells, mlp, reinterpret_cast<float2 *>(cells->guess), s);
+    axb_mark(ctx, AXB_R_MLP, s, false);
+    if (rc)
+      return rc;
   }
+  axb_mark(ctx, AXB_R_C2P_CELLS, s, true);
+  if (eos->kind == 1)
+    k_c2p_cells<<<(unsigned)blocks, 128, 0, s>>>(a, tab_for_launch(*eos, a.status));
+  else
+    k_c2p_cells<<<(unsigned)blocks, 128, 0, s>>>(a, eos->ideal);
   axb_mark(ctx, AXB_R_C2P_CELLS, s, false);
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
 }

@@ -55,6 +55,39 @@ struct RhsArgs {
   DevStatus *status;
 };
 
+// Fast magnetosonic speeds of one face state (eigenvalues.hxx:19-79): the
+// roots of a2 l^2 + a1 l + a0 = 0 divided by the lapse, lam_p with +sqrt
+// and lam_m with -sqrt (the reference lists each twice).  One reciprocal of
+// 2 a2 alp instead of the two divisions (last-ulp differences).
+AXB_HD void fast_speeds(double alp, double beta, double uinv, double vdir, double rho,
+                        double cs2, double W, double h, double bsq, double &lam_p,
+                        double &lam_m) {
+  const double a0 = (bsq + cs2 * h * rho) * (sq(beta) - sq(alp) * uinv) -
+                    (-1 + cs2) * h * rho * sq(beta - alp * vdir) * sq(W);
+  const double a1 = 2 * beta * (bsq + cs2 * h * rho) -
+                    2 * (-1 + cs2) * h * rho * (beta - alp * vdir) * sq(W);
+  const double a2 = bsq + h * rho * (cs2 + sq(W) - cs2 * sq(W));
+  double det = sq(a1) - 4 * a2 * a0;
+  if (det < 0)
+    det = 0;
+  const double sd = sqrt(det);
+  const double i2a2alp = 1 / (2 * a2 * alp);
+  lam_p = (-a1 + sd) * i2a2alp;
+  lam_m = (-a1 - sd) * i2a2alp;
+}
+
+// Riemann fluxes of one variable (AsterX/src/fluxes.hxx:20-49) from the
+// bounding speeds cmax = max(0, speeds) and cmin = min(0, speeds):
+// HLLE with the reciprocal icpm = 1 / (cmax - cmin) (a product instead of
+// the division), LxF with ch = max(cmax, -cmin) = max |speed|.
+AXB_HD double hlle_flux(double cmax, double cmin, double icpm, double uL, double uR,
+                        double fL, double fR) {
+  return (cmax * fL - cmin * fR + cmax * cmin * (uR - uL)) * icpm;
+}
+AXB_HD double laxf_flux(double ch, double uL, double uR, double fL, double fR) {
+  return 0.5 * ((fL + fR) - ch * (uR - uL));
+}
+
 // The stage combine U_k <- alpha U_n + beta U_k + gdt RHS with an explicit
 // rounding order, so that the fused and the separate stage update give the
 // same bits.
@@ -258,20 +291,7 @@ AXB_D void side_physics(const FaceMetric &m, const double *r, double Bdir,
     o.F[8] = E0;
     o.F[9] = 0.0;
   }
-  // fast magnetosonic speeds (eigenvalues.hxx:19-79)
-  const double beta = m.beta[DIR];
-  const double a0 = (bsq + cs2 * h * rho) * (sq(beta) - sq(m.alp) * m.uinv) -
-                    (-1 + cs2) * h * rho * sq(beta - m.alp * vel[DIR]) * sq(W);
-  const double a1 = 2 * beta * (bsq + cs2 * h * rho) -
-                    2 * (-1 + cs2) * h * rho * (beta - m.alp * vel[DIR]) * sq(W);
-  const double a2 = bsq + h * rho * (cs2 + sq(W) - cs2 * sq(W));
-  double det = sq(a1) - 4 * a2 * a0;
-  if (det < 0)
-    det = 0;
-  const double sd = sqrt(det);
-  const double i2a2alp = 1 / (2 * a2 * m.alp);
-  o.lam_p = (-a1 + sd) * i2a2alp;
-  o.lam_m = (-a1 - sd) * i2a2alp;
+  fast_speeds(m.alp, m.beta[DIR], m.uinv, vel[DIR], rho, cs2, W, h, bsq, o.lam_p, o.lam_m);
 }
 
 } // namespace axb

@@ -96,12 +96,12 @@ AXB_D void face_fluxes(const RhsArgs &a, const EOS &eos,
     const double icpm = 1 / (cmax - cmin);
 #pragma unroll
     for (int v = 0; v < 10; ++v)
-      F[v] = (cmax * sL.F[v] - cmin * sR.F[v] + cmax * cmin * (sR.U[v] - sL.U[v])) * icpm;
+      F[v] = hlle_flux(cmax, cmin, icpm, sL.U[v], sR.U[v], sL.F[v], sR.F[v]);
   } else {
     const double ch = fmax(cmax, -cmin);
 #pragma unroll
     for (int v = 0; v < 10; ++v)
-      F[v] = 0.5 * ((sL.F[v] + sR.F[v]) - ch * (sR.U[v] - sL.U[v]));
+      F[v] = laxf_flux(ch, sL.U[v], sR.U[v], sL.F[v], sR.F[v]);
   }
 #pragma unroll
   for (int v = 0; v < 10; ++v)

@@ -103,6 +103,12 @@ def load_library(path=LIB_PATH):
                                    _dp, C.POINTER(C.POINTER(Fields)), C.c_double,
                                    C.POINTER(Fields), _vp]
     lib.axb_rk_lincomb.restype = C.c_int
+    lib.axb_tmunu.argtypes = [_vp, C.POINTER(Box), C.POINTER(Fields), C.POINTER(Params),
+                              C.c_int, C.POINTER(_dp), _vp]
+    lib.axb_tmunu.restype = C.c_int
+    lib.axb_estimate_error.argtypes = [_vp, C.POINTER(Box), C.POINTER(_dp), C.c_int, C.c_int,
+                                       C.c_double, _dp, _vp]
+    lib.axb_estimate_error.restype = C.c_int
     lib.axb_probe_fp64.argtypes = [_dp]
     lib.axb_probe_fp64.restype = C.c_int
     lib.axb_timing_begin.argtypes = [_vp]
@@ -254,6 +260,28 @@ class Engine:
                                                len(names), b, self.stream_ptr(stream)),
                     "axb_fill_boundary")
 
+    def tmunu(self, layout, tensors, params, eT, interp_order=2, stream=None):
+        """axb_tmunu: add T_{mu nu} at the interior vertices to the ten
+        tensors eT = [eTtt, eTtx, eTty, eTtz, eTxx, eTxy, eTxz, eTyy, eTyz,
+        eTzz] (the box's layout)."""
+        box = layout.box()
+        f = self.fields_struct(tensors)
+        ptrs = (_dp * 10)(*[C.cast(t.data_ptr(), _dp) for t in eT])
+        self._check(self.lib.axb_tmunu(self.ctx, C.byref(box), C.byref(f), C.byref(params),
+                                       interp_order, ptrs, self.stream_ptr(stream)),
+                    "axb_tmunu")
+
+    def estimate_error(self, layout, vars, method, out, epsilon_err=0.0, stream=None):
+        """axb_estimate_error: the regrid indicator `method` (an abi.REGRID
+        code) of the tensors `vars` at the interior cells, written to `out`."""
+        box = layout.box()
+        ptrs = (_dp * len(vars))(*[C.cast(t.data_ptr(), _dp) for t in vars])
+        self._check(self.lib.axb_estimate_error(self.ctx, C.byref(box), ptrs, len(vars),
+                                                method, epsilon_err,
+                                                C.cast(out.data_ptr(), _dp),
+                                                self.stream_ptr(stream)),
+                    "axb_estimate_error")
+
     def rhs_group_bc(self, layout, tensors, params, eos, bc, stream=None):
         """axb_rhs_group_bc: the RHS group with physical outer boundaries."""
         box = layout.box()
@@ -312,7 +340,7 @@ class Engine:
     def timing_begin(self):
         self._check(self.lib.axb_timing_begin(self.ctx), "axb_timing_begin")
 
-    def timing_end(self, nregions=12):
+    def timing_end(self, nregions=14):
         ms = (C.c_double * nregions)()
         cnt = (C.c_int * nregions)()
         self._check(self.lib.axb_timing_end(self.ctx, ms, cnt, nregions), "axb_timing_end")
@@ -346,6 +374,14 @@ class Engine:
         return abi.cells_struct(n, ptrs)
 
     def c2p_cells(self, cells, params: Params, eos, mlp=None, stream=None):
+        if mlp is not None and not cells.guess:
+            # scratch for the learned guess, kept for later calls of this size
+            n = int(cells.n)
+            buf = getattr(self, "_guess_buf", None)
+            if buf is None or buf.numel() < 2 * n:
+                buf = self.torch.empty(2 * n, dtype=self.torch.float32, device=self.device)
+                self._guess_buf = buf
+            cells.guess = buf.data_ptr()
         self._check(self.lib.axb_c2p_cells(self.ctx, C.byref(cells), C.byref(params), eos,
                                            mlp, self.stream_ptr(stream)), "axb_c2p_cells")
 

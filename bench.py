@@ -34,9 +34,10 @@ UNIT = "zone-updates/s"
 SSPRK3 = [(0.0, 1.0, 1.0), (0.75, 0.25, 0.25), (1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0)]
 GAMMA = 4.0 / 3.0
 CFL_MAX = 0.9
-# the tabulated-EOS substep: temperature reconstructed (the tabulated EOS has
-# no eps(rho, p)), atmosphere temperature inside the table
-TAB_PARAMS = dict(reconstruct_with_temperature=1, t_atmo=0.011)
+# the tabulated-EOS substep: temperature reconstructed and the recovery's
+# limits applied through the temperature (use_temperature), since the
+# tabulated EOS has no eps(rho, p); atmosphere temperature inside the table
+TAB_PARAMS = dict(reconstruct_with_temperature=1, t_atmo=0.011, use_temperature=1)
 # the survey's algorithmic figure for one substep: 112 FP64 values per zone
 # (RHS reads 34, stage 33, post-step reads 23 and writes 22)
 SUBSTEP_BYTES = 112 * 8
@@ -709,7 +710,9 @@ def c2p_bench(args):
     outs = ["rho", "eps", "press", "w_lorentz", "iters", "flag", "fallback"]
     for k in outs:
         t[k] = torch.empty(n, dtype=torch.float64, device=dev)
+    guess = torch.empty(2 * n, dtype=torch.float32, device=dev)
     cstruct = eng.cells(n, t)
+    cstruct.guess = guess.data_ptr()
     stream = torch.cuda.current_stream(dev)
     res = {}
     for name, m in (("plain", None), ("learned", mlp)):
@@ -751,7 +754,7 @@ def c2p_bench(args):
             "fail_rate": float((flag == abi.C2P_FAIL).double().mean().item()),
             "max_rel_err": errs,
             "recovery_kernel_ms": region_ms[REGIONS.index("c2p_cells")] / max(1, args.steps),
-            # (the network runs inside the recovery kernel: no separate launch)
+            "mlp_kernel_ms": region_ms[REGIONS.index("mlp")] / max(1, args.steps),
             "gpu_launches": int(sum(region_n)),
         }
     alg = 8 * (16 + 8)  # bytes per cell: 16 inputs read, 8 outputs written
@@ -766,8 +769,7 @@ def c2p_bench(args):
         "data": "synthetic (seeded cells of the configuration)",
         "config": {"workload": f"{n} independent cells, Noble (Palenzuela backup), "
                                "ideal gas Gamma=5/3, c2p_tol 1e-10, MLP 8-64-64-64-2 "
-                               f"({args.mlp_act}) trained on {nt} pairs, evaluated "
-                               "inside the recovery kernel",
+                               f"({args.mlp_act}) trained on {nt} pairs",
                    "cells": n, "l2": "inputs larger than L2"},
         "plain": res["plain"], "learned": res["learned"],
         "speedup_learned_vs_plain": lr_["cells_per_s"] / res["plain"]["cells_per_s"],

@@ -439,7 +439,7 @@ typedef struct axb_cells {
   const double *seed_rho, *seed_eps, *seed_Ye, *seed_vel[3], *seed_temperature;
   double *rho, *eps, *press, *vel[3], *w_lorentz, *Ye, *temperature, *entropy;
   double *iters, *flag;
-  float *guess;     /* unused (the guess stays in registers); may be NULL */
+  float *guess;     /* scratch, 2 floats per cell; required with a learned guess */
   double *fallback; /* output, may be NULL */
 } axb_cells;
 
@@ -453,9 +453,10 @@ typedef struct axb_cells {
  * (c2p_2DNoble.hxx:374-393), the Palenzuela scheme brackets x by
  * [x (1 - bracket), x (1 + bracket)] when that interval brackets the root
  * and otherwise keeps its own bracket (c2p_1DPalenzuela.hxx:395-401).
- * The network runs inside the recovery kernel: each CTA stages the weights
- * in shared memory, each warp evaluates its 32 cells on the tensor cores and
- * the guess stays in registers.  A cell whose guessed first attempt fails is
+ * The network runs in its own kernel before the recovery (a persistent
+ * grid whose CTAs stage the weights in shared memory once) and leaves
+ * (x, W) per cell in the caller's `guess` scratch.  A cell whose guessed
+ * first attempt fails is
  * retried from the plain cold-start seeds of c2p_2DNoble.hxx:374-393 (and
  * the plain bracket) before the second scheme, so the cascade after a
  * failed guess is exactly the plain one.
@@ -550,11 +551,51 @@ AXB_API int axb_rhs_group_noalloc(const axb_box *box, const axb_fields *fields,
                                   const axb_params *params, const axb_eos *eos,
                                   void *stream);
 
+/* ------------------------------------------------------------------------ */
+/* stress-energy tensor and regrid error                                     */
+/* ------------------------------------------------------------------------ */
+
+/* AsterX_Tmunu (AsterX/src/tmunu.cxx:19-178, scheduled in
+ * TmunuBaseX_AddToTmunu): at every interior vertex, the cell-centred rho,
+ * eps, press, Bvec and velocity (velx.. for recon_type v_vec, zvec_x.. for
+ * z_vec and s_vec, as the reference tests recon_type == "v_vec") are
+ * interpolated to the vertex (interp_order 2: the mean of the 8 cells
+ * around it; 4: cubic Lagrange weights over 4 cells per direction, needs 2
+ * ghost layers; AsterUtils/src/aster_interp.hxx:97-148), and the ideal-MHD
+ * T_{mu nu} is ADDED to eT[0..9] = eTtt, eTtx, eTty, eTtz, eTxx, eTxy,
+ * eTxz, eTyy, eTyz, eTzz (vertex-centred arrays in the box's layout).
+ * Reads rho, eps, press, Bvec, velx or zvec, the metric, alp and beta from
+ * `fields`. */
+AXB_API int axb_tmunu(axb_ctx *ctx, const axb_box *box, const axb_fields *fields,
+                      const axb_params *params, int interp_order, double *const eT[10],
+                      void *stream);
+
+/* Regrid error indicators (AsterX/src/estimate_error.hxx:14-86; the
+ * regrid_method keywords of AsterX/param.ccl). */
+typedef enum axb_regrid {
+  AXB_REGRID_FIRST_DERIV = 0,       /* "first derivative"        */
+  AXB_REGRID_SECOND_DERIV = 1,      /* "second derivative"       */
+  AXB_REGRID_SECOND_DERIV_NORM = 2, /* "second derivative norm"  */
+  AXB_REGRID_FIRST_GRAD = 3         /* "first gradient"          */
+} axb_regrid;
+
+/* AsterX_EstimateError (AsterX/src/estimate_error.cxx:70-144): at every
+ * interior cell, regrid_error = the largest indicator of `method` over the
+ * grid functions vars[0..nvars) (1 <= nvars <= 9, each in the box's layout,
+ * any centring: the cell's own index is used, as the reference does with
+ * each variable's GF3D2), with the undivided differences to the neighbours
+ * +-1 along each direction; epsilon_err is the noise filter of "second
+ * derivative norm". */
+AXB_API int axb_estimate_error(axb_ctx *ctx, const axb_box *box, const double *const *vars,
+                               int nvars, int method, double epsilon_err,
+                               double *regrid_error, void *stream);
+
 /* Optional per-launch timing: after axb_timing_begin every kernel launch of
  * the entry points above is bracketed by CUDA events on its stream;
  * axb_timing_end waits for them and returns, per kernel region (sources,
  * flux x, flux y, flux z, aux, ct+psi, rk stage, sync, bstag, c2p, c2p
- * cells, mlp -- `nregions` entries), the summed milliseconds and launch
+ * cells, mlp, tmunu, regrid error -- `nregions` entries), the summed
+ * milliseconds and launch
  * counts.  Not part of the reference; a measurement aid. */
 AXB_API int axb_timing_begin(axb_ctx *ctx);
 AXB_API int axb_timing_end(axb_ctx *ctx, double *ms, int *count, int nregions);

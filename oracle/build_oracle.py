@@ -1,7 +1,7 @@
 """Build recipe for the CPU checkers (test infrastructure only).
 
 * ``oracle/_ref/libaxref.so``: the reference's own hot-path sources
-  (AsterX/src/{fluxes,source,rhs,computeBfromA,con2prim}.cxx and the ReconX,
+  (AsterX/src/{fluxes,source,rhs,computeBfromA,con2prim,tmunu}.cxx and the ReconX,
   Con2PrimFactory, EOSX and AsterUtils headers they include), compiled
   unmodified from where they lie in the reference checkout against the
   stand-in headers in ``oracle/refshim`` plus the harness
@@ -24,7 +24,7 @@ REPO = os.path.dirname(HERE)
 # The reference checkout is named by the caller (argument or the
 # AXB_REFERENCE_ROOT environment variable); there is no built-in default.
 REF_ROOT = os.environ.get("AXB_REFERENCE_ROOT", "")
-REF_TUS = ["fluxes", "source", "rhs", "computeBfromA", "con2prim"]
+REF_TUS = ["fluxes", "source", "rhs", "computeBfromA", "con2prim", "tmunu"]
 # -DNDEBUG: the reference's device asserts (NaN checks in fluxes.cxx:769,
 # rhs.cxx:206) compile out, as in an optimised build, instead of aborting
 # the test process.

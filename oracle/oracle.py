@@ -42,7 +42,9 @@ REF_ONLY_FIELDS = (
     + ["vtilde_y_xface", "vtilde_z_xface", "vtilde_x_yface", "vtilde_z_yface",
        "vtilde_x_zface", "vtilde_y_zface", "amax_xface", "amin_xface",
        "amax_yface", "amin_yface", "amax_zface", "amin_zface",
-       "aster_mask_vc", "aster_mask_cc"])
+       "aster_mask_vc", "aster_mask_cc"]
+    + ["eTtt", "eTtx", "eTty", "eTtz", "eTxx", "eTxy", "eTxz", "eTyy", "eTyz", "eTzz",
+       "regrid_error"])
 
 
 def _ptr(a):
@@ -71,6 +73,9 @@ class Oracle:
         L.ora_riemann.argtypes = [C.c_int, _dp] + [C.c_double] * 4
         L.ora_riemann.restype = C.c_double
         L.ora_prim2con.argtypes = [_dp, _dp, _dp]
+        if hasattr(L, "ora_tmunu"):
+            L.ora_tmunu.argtypes = [C.c_int]
+            L.ora_estimate_error.argtypes = [C.c_int, C.c_int, C.POINTER(_dp), C.c_double]
         L.ora_c2p_point.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _dp,
                                     C.POINTER(C.c_int)]
         L.ora_eos_tab_query.argtypes = [C.c_int, C.c_double, C.c_double,
@@ -141,6 +146,18 @@ class Oracle:
         self.run("bstag", ext_c=1)
         self.run("dB")
         self.run("c2p")
+
+    def tmunu(self, interp_order=2):
+        """AsterX_Tmunu: adds T_{mu nu} to the bound eTtt .. eTzz."""
+        self._check(self.lib.ora_tmunu(interp_order))
+
+    def estimate_error(self, method, arrays, epsilon_err=0.0):
+        """AsterX_EstimateError's loop with the reference's indicators over
+        `arrays` (the box's layout); returns the bound regrid_error."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in arrays]
+        ptrs = (_dp * len(arrs))(*[_ptr(a) for a in arrs])
+        self._check(self.lib.ora_estimate_error(method, len(arrs), ptrs, epsilon_err))
+        return self.fields["regrid_error"]
 
     # -- per-point ------------------------------------------------------------
     def reconstruct(self, method, v, press=None, vel=None, is_rho=False,

@@ -27,7 +27,9 @@
   X(vtilde_y_xface) X(vtilde_z_xface) X(vtilde_x_yface) X(vtilde_z_yface)      \
   X(vtilde_x_zface) X(vtilde_y_zface)                                          \
   X(amax_xface) X(amin_xface) X(amax_yface) X(amin_yface) X(amax_zface)        \
-  X(amin_zface) X(aster_mask_vc) X(aster_mask_cc)
+  X(amin_zface) X(aster_mask_vc) X(aster_mask_cc)                             \
+  X(eTtt) X(eTtx) X(eTty) X(eTtz) X(eTxx) X(eTxy) X(eTxz) X(eTyy) X(eTyz)      \
+  X(eTzz) X(regrid_error)
 
 enum axref_field_id {
 #define AXREF_ENUM(name) AXREF_F_##name,

@@ -1,5 +1,5 @@
 // Test infrastructure only.  Drives the reference hot-path translation units
-// (AsterX/src/{fluxes,source,rhs,computeBfromA,con2prim}.cxx, compiled
+// (AsterX/src/{fluxes,source,rhs,computeBfromA,con2prim,tmunu}.cxx, compiled
 // unmodified against the stand-in headers of this directory) and the
 // reference per-point headers through a small C ABI, so that tests can
 // compare the oracle restatement and the CUDA kernels with the reference's
@@ -17,6 +17,11 @@
 #include "prim2con.hxx"
 #include "reconstruct.hxx"
 #include "setup_eos.hxx"
+
+#include <sstream>
+#include <vector>
+
+#include "estimate_error.hxx"
 
 #include "../../include/asterx_b200.h"
 
@@ -46,7 +51,18 @@ extern "C" void AsterX_RHS(CCTK_ARGUMENTS);
 extern "C" void AsterX_ComputedBstagFromA(CCTK_ARGUMENTS);
 extern "C" void AsterX_ComputedBFromdBstag(CCTK_ARGUMENTS);
 extern "C" void AsterX_Con2Prim(CCTK_ARGUMENTS);
+extern "C" void AsterX_Tmunu(CCTK_ARGUMENTS);
 } // namespace AsterX
+
+// The Cactus group tables that estimate_error.hxx's parameter parsing reads
+// (never reached: the checker passes the regrid variables itself).
+int CCTK_GroupTagsTableI(int) { axref_fatal("CCTK_GroupTagsTableI is not available"); }
+int CCTK_GroupCenteringTableI(int) {
+  axref_fatal("CCTK_GroupCenteringTableI is not available");
+}
+int Util_TableGetIntArray(int, int, int *, const char *) {
+  axref_fatal("Util_TableGetIntArray is not available");
+}
 
 namespace {
 double *g_fields[AXREF_NFIELDS];
@@ -467,4 +483,45 @@ ORA_API double ora_eos_tab_query(int which, double rho, double x, double ye,
   if (eps_io)
     *eps_io = e;
   return r;
+}
+
+// ---------------------------------------------------------------------------
+// stress-energy tensor and regrid error
+// ---------------------------------------------------------------------------
+// AsterX_Tmunu (AsterX/src/tmunu.cxx:158-176) at interpolation order 2 or 4.
+ORA_API int ora_tmunu(int interp_order) {
+  axref_params.tmunu_interp_order = interp_order;
+  return guarded([] { AsterX::AsterX_Tmunu(&g_gh); });
+}
+
+// The loop of AsterX_EstimateError (AsterX/src/estimate_error.cxx:96-140)
+// over the interior cells with the reference's indicators
+// (AsterX/src/estimate_error.hxx:14-86), for the grid functions `vars`
+// (the box's layout) given directly instead of through the regrid_groups
+// parameter; writes regrid_error.
+ORA_API int ora_estimate_error(int method, int nvars, double *const *vars,
+                               double epsilon_err) {
+  return guarded([&] {
+    std::vector<Loop::GF3D2<const CCTK_REAL> > gfs;
+    for (int i = 0; i < nvars; ++i)
+      gfs.emplace_back(vars[i], g_sy, g_sz);
+    const Loop::GF3D2<CCTK_REAL> regrid_error(g_fields[AXREF_F_regrid_error], g_sy,
+                                              g_sz);
+    g_grid.loop_int_device<1, 1, 1>(
+        g_grid.nghostzones, [&](const Loop::PointDesc &p) {
+          regrid_error(p.I) = 0.0;
+          for (int i = 0; i < nvars; i++) {
+            CCTK_REAL e = 0;
+            switch (method) {
+            case AXB_REGRID_FIRST_DERIV: e = AsterX::calc_deriv_1st(gfs[i], p); break;
+            case AXB_REGRID_SECOND_DERIV: e = AsterX::calc_deriv_2nd(gfs[i], p); break;
+            case AXB_REGRID_SECOND_DERIV_NORM:
+              e = AsterX::calc_deriv_2nd_norm(gfs[i], p, epsilon_err);
+              break;
+            default: e = AsterX::calc_grad_1st(gfs[i], p); break;
+            }
+            regrid_error(p.I) = std::max({regrid_error(p.I), e});
+          }
+        });
+  });
 }

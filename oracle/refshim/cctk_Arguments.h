@@ -102,6 +102,14 @@ const CCTK_REAL *axref_delta_space();
   AXREF_RW(Avec_x_rhs) AXREF_RW(Avec_y_rhs) AXREF_RW(Avec_z_rhs)               \
   AXREF_RW(Psi_rhs)
 
+#define DECLARE_CCTK_ARGUMENTSX_AsterX_Tmunu                                   \
+  AXREF_COMMON AXREF_METRIC_RO                                                 \
+  AXREF_RO(rho) AXREF_RO(eps) AXREF_RO(press) AXREF_RO(velx) AXREF_RO(vely)    \
+  AXREF_RO(velz) AXREF_RO(zvec_x) AXREF_RO(zvec_y) AXREF_RO(zvec_z)            \
+  AXREF_RO(Bvecx) AXREF_RO(Bvecy) AXREF_RO(Bvecz)                              \
+  AXREF_RW(eTtt) AXREF_RW(eTtx) AXREF_RW(eTty) AXREF_RW(eTtz) AXREF_RW(eTxx)   \
+  AXREF_RW(eTxy) AXREF_RW(eTxz) AXREF_RW(eTyy) AXREF_RW(eTyz) AXREF_RW(eTzz)
+
 #define DECLARE_CCTK_ARGUMENTSX_AsterX_ComputedBstagFromA                      \
   AXREF_COMMON AXREF_RO(Avec_x) AXREF_RO(Avec_y) AXREF_RO(Avec_z)              \
   AXREF_RW(dBx_stag) AXREF_RW(dBy_stag) AXREF_RW(dBz_stag)

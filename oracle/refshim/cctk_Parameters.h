@@ -15,7 +15,8 @@ struct axref_params_t {
   CCTK_INT reconstruct_with_temperature, ppm_shock_detection,
       ppm_zone_flattening, use_uct, local_spatial_order, thermal_eos_atmo,
       use_press_atmo, max_iter, use_mask, excise, debug_mode, use_entropy_fix,
-      Ye_lenient, use_z, use_temperature, interpolate_failed_c2p;
+      Ye_lenient, use_z, use_temperature, interpolate_failed_c2p,
+      tmunu_interp_order;
   // reals
   CCTK_REAL poly_k, poly_gamma, ppm_eta1, ppm_eta2, ppm_eps, ppm_eps_shock,
       ppm_small, ppm_omega1, ppm_omega2, enhanced_ppm_C2, weno_eps, mp5_alpha,
@@ -39,6 +40,7 @@ extern axref_params_t axref_params;
   AXREF_P(use_mask) AXREF_P(excise) AXREF_P(debug_mode)                        \
   AXREF_P(use_entropy_fix) AXREF_P(Ye_lenient) AXREF_P(use_z)                  \
   AXREF_P(use_temperature) AXREF_P(interpolate_failed_c2p)                     \
+  AXREF_P(tmunu_interp_order)                                                  \
   AXREF_P(poly_k) AXREF_P(poly_gamma) AXREF_P(ppm_eta1) AXREF_P(ppm_eta2)      \
   AXREF_P(ppm_eps) AXREF_P(ppm_eps_shock) AXREF_P(ppm_small)                   \
   AXREF_P(ppm_omega1) AXREF_P(ppm_omega2) AXREF_P(enhanced_ppm_C2)             \

@@ -52,3 +52,51 @@ def test_rhs_balsara_and_fd4(engine, ref, fd_order):
     for n in RHS_OUT:
         emax, el2 = errors(interior(L, n, gpu[n]), interior(L, n, host[n]))
         assert emax <= TOL, (n, emax, el2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("recon,lo", [("wenoz", "godunov"), ("ppm", "minmod"),
+                                      ("mp5", "monocentral")])
+def test_rhs_loworder_redo(engine, ref, recon, lo):
+    """The low-order redo of a face (fluxes.cxx:313-343): where a
+    reconstructed rho, entropy, Ye or pressure is <= 0 on either side, every
+    variable of that face is reconstructed again with loworder_method.  A
+    sign-changing entropy and a Ye that dips below zero make a large share
+    of the faces take that path."""
+    L, f = W.curved_box(n=12, ng=5, seed=13, wmax=3.0)
+    rng = np.random.default_rng(14)
+    f = full_fields(L, f)
+    f["entropy"] = rng.normal(0.2, 1.0, L.size)
+    f["Ye"] = rng.uniform(-0.05, 0.5, L.size)
+    v = L.view(f["entropy"])[L.interior((1, 1, 1))]
+    assert (v <= 0).mean() > 0.2  # the trigger is exercised
+    p = abi.default_params(reconstruction_method=recon, loworder_method=lo, flux_type="hlle")
+    host, gpu, st = run_both(engine, ref, L, f, p, 4.0 / 3.0)
+    for n in RHS_OUT:
+        emax, el2 = errors(interior(L, n, gpu[n]), interior(L, n, host[n]))
+        assert emax <= TOL, (n, emax, el2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("recon", ["wenoz", "mp5"])
+def test_max_char_speed_matches_reference(engine, ref, recon):
+    """The engine's largest characteristic speed of a launch equals the
+    largest of the reference's amax / amin face grid functions
+    (fluxes.cxx:779-785) over the same faces: the interior faces widened by
+    one transverse layer, as the engine computes them."""
+    L, f = W.curved_box(n=12, ng=5, seed=15, wmax=5.0)
+    f = full_fields(L, f)
+    p = abi.default_params(reconstruction_method=recon, flux_type="hlle")
+    host = {n: a.copy() for n, a in f.items()}
+    ref.setup(L, p, host)
+    ref.eos_idealgas(4.0 / 3.0, rho=(1e-40, 1e10), eps=(0.0, 1e10))
+    ref.run("fluxes", ext_c=1, ext_v=0)
+    want = max(float(np.max(ref.fields[f"a{m}_{d}face"])) for m in ("max", "min")
+               for d in "xyz")
+    eos = engine.eos_idealgas(4.0 / 3.0, rho=(1e-40, 1e10), eps=(0.0, 1e10))
+    dev = engine.upload(L, f)
+    engine.status_reset()
+    engine.rhs_group(L, dev, p, eos)
+    got = engine.status()["max_speed"]
+    assert want > 0.5
+    assert abs(got - want) <= 1e-13 * want, (got, want)
