@@ -847,4 +847,134 @@ AXB_HD void palenzuela_solve(const EOS &eos, const C2PParams &cp, const Atmo &at
     cv.scale(sqrt_detg);
 }
 
+// Root function of the entropy scheme (c2p_1DEntropy.hxx:262-303, Appendix
+// A.4 of arXiv:1112.0568): with rho = x, p and eps from the conserved
+// entropy, W = rho h Lorentz^2 (A60), S_f^2 (A61), rho (A62); returns
+// x - rho.  Written as the reference writes it (a backup scheme).
+template <class EOS>
+AXB_HD double ent_froot(const EOS &eos, double Ssq, double Bsq, double BiSi, double x,
+                        const Cons &cv) {
+  const double ent_loc = cv.DEnt / cv.dens;
+  const double ye_loc = cv.DYe / cv.dens;
+  const double press_loc = eos.press_from_valid_rho_kappa_ye(x, ent_loc, ye_loc);
+  const double eps_loc = eos.eps_from_valid_rho_kappa_ye(x, ent_loc, ye_loc);
+  const double lor_loc = cv.dens / x;
+  const double h_loc = (1.0 + eps_loc + press_loc / x);
+  const double W = x * h_loc * lor_loc * lor_loc;
+  const double Sfsq = (W * W * Ssq + BiSi * BiSi * (Bsq + 2.0 * W)) / ((W + Bsq) * (W + Bsq));
+  const double rho = cv.dens / sqrt(1.0 + Sfsq / (cv.dens * cv.dens * h_loc * h_loc));
+  return x - rho;
+}
+
+// Entropy 1D (c2p_1DEntropy::solve, c2p_1DEntropy.hxx:306-469): Brent on
+// rho in [D / sqrt(1 + S^2 / D^2), D] (A59), primitives from the conserved
+// entropy (xEntropyToPrim, :143-225), tau recomputed from them.  The
+// conservative-variable check of an unconverged bracket omits tau and
+// rejects at max_error >= cons_error, as the reference does.
+template <class EOS>
+AXB_HD void entropy_solve(const EOS &eos, const C2PParams &cp, const Atmo &atmo, Prim &pv,
+                          Cons &cv, const sym3 &glo, Report &rep) {
+  rep.iters = 0;
+  rep.adjust_cons = false;
+  rep.set_atmo = false;
+  rep.status = REP_SUCCESS;
+  const double spatial_detg = det3(glo);
+  const double sqrt_detg = sqrt(spatial_detg);
+  const bool minor1 = glo.xx > 0.0;
+  const bool minor2 = glo.xx * glo.yy - glo.xy * glo.xy > 0.0;
+  const bool minor3 = spatial_detg > 0.0;
+  if (!(minor1 && minor2 && minor3)) {
+    rep.fail(REP_INVALID_DETG);
+    pv.set_nan();
+    cv.set_nan();
+    return;
+  }
+  const sym3 gup = inv3(glo, spatial_detg);
+  cv.unscale(sqrt_detg);
+  double mom_up[3];
+  lower3(gup, cv.mom, mom_up);
+  const double Ssq = cv.mom[0] * mom_up[0] + cv.mom[1] * mom_up[1] + cv.mom[2] * mom_up[2];
+  double B_low[3];
+  lower3(glo, cv.dBvec, B_low);
+  const double Bsq = dot3(B_low, cv.dBvec);
+  const double BiSi =
+      cv.dBvec[0] * cv.mom[0] + cv.dBvec[1] * cv.mom[1] + cv.dBvec[2] * cv.mom[2];
+  if (!isfinite(cv.dens) || !isfinite(Ssq) || !isfinite(Bsq) || !isfinite(BiSi) ||
+      !isfinite(cv.DYe) || !isfinite(cv.DEnt)) {
+    rep.fail(REP_NANS_IN_CONS);
+    pv.set_nan();
+    cv.set_nan();
+    return;
+  }
+  if (Bsq > cp.Bsq_lim) {
+    rep.fail(REP_B_LIMIT);
+    pv.set_nan();
+    cv.set_nan();
+    return;
+  }
+  const double a = cv.dens / sqrt(1.0 + Ssq / (cv.dens * cv.dens));
+  const double b = cv.dens;
+  auto fn = [&](double x) { return ent_froot(eos, Ssq, Bsq, BiSi, x, cv); };
+  double r0, r1;
+  brent_bracket(fn, a, b, fn(a), fn(b), cp.minbits, cp.maxIter, rep.iters, r0, r1);
+  const double x_sol = 0.5 * (r0 + r1);
+  // xEntropyToPrim
+  pv.rho = x_sol;
+  pv.entropy = cv.DEnt / cv.dens;
+  pv.Ye = cv.DYe / cv.dens;
+  pv.w_lor = cv.dens / x_sol;
+  pv.press = eos.press_from_valid_rho_kappa_ye(x_sol, pv.entropy, pv.Ye);
+  pv.eps = eos.eps_from_valid_rho_kappa_ye(x_sol, pv.entropy, pv.Ye);
+  pv.temperature = eos.temp_from_valid_rho_eps_ye(x_sol, pv.eps, pv.Ye);
+  const double Z_Sol = (x_sol + pv.eps * x_sol + pv.press) * pv.w_lor * pv.w_lor;
+  vel_from_Z(Z_Sol, pv.w_lor, Bsq, BiSi, cp.use_zprim, pv, cv, gup, glo);
+  for (int i = 0; i < 3; ++i)
+    pv.Bvec[i] = cv.dBvec[i];
+  set_E(pv, gup);
+  if (pv.rho <= 0.0) {
+    rep.fail(REP_RANGE_RHO);
+    cv.scale(sqrt_detg);
+    return;
+  }
+  if (fabs(r0 - r1) > cp.tolerance_0 * fmin(fabs(r0), fabs(r1))) {
+    Cons ck;
+    cons_from_prim(ck, pv, glo);
+    ck.unscale(sqrt_detg);
+    const double small = 1e-50;
+    const double e0 = sq((ck.dens - cv.dens) / (cv.dens + small));
+    const double e1 = sq((ck.mom[0] - cv.mom[0]) / (cv.mom[0] + small));
+    const double e2 = sq((ck.mom[1] - cv.mom[1]) / (cv.mom[1] + small));
+    const double e3 = sq((ck.mom[2] - cv.mom[2]) / (cv.mom[2] + small));
+    double m = e0; // std::max over an initializer list (first of equal maxima)
+    if (m < e1) m = e1;
+    if (m < e2) m = e2;
+    if (m < e3) m = e3;
+    if (sqrt(m) >= cp.cons_error) {
+      rep.fail(REP_ROOT_FAIL_CONV);
+      cv.scale(sqrt_detg);
+      return;
+    }
+  }
+  // tau from the recovered primitives (undensitised)
+  double v_low[3];
+  lower3(glo, pv.vel, v_low);
+  const double bst = pv.w_lor * dot3(pv.Bvec, v_low);
+  const double bs2 = (Bsq + bst * bst) / (pv.w_lor * pv.w_lor);
+  cv.tau = (pv.w_lor * pv.w_lor * (pv.rho * (1.0 + pv.eps) + pv.press + bs2) -
+            (pv.press + 0.5 * bs2) - bst * bst) -
+           cv.dens;
+  if (pv.rho < atmo.rho_cut) {
+    rep.status = REP_SUCCESS;
+    rep.set_atmo = true;
+    rep.adjust_cons = true;
+    atmo.set(pv, cv, glo);
+    return;
+  }
+  prims_floors(eos, cp, atmo, pv, cv, glo, rep);
+  if (rep.adjust_cons)
+    cons_from_prim(cv, pv, glo);
+  else
+    cv.scale(sqrt_detg);
+}
+
 } // namespace axb

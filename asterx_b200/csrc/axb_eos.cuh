@@ -55,6 +55,15 @@ struct EosIdeal {
     double eps = eps_from_valid_rho_temp_ye(rho, temp, ye);
     return press_from_valid_rho_eps_ye(rho, eps, ye);
   }
+  // p = kappa rho^Gamma and eps = kappa rho^(Gamma-1) / (Gamma-1) of the
+  // evolved entropy (eos_3p_idealgas.hxx:201-215), with pow as there: the
+  // entropy recovery's root function, not on a hot path
+  AXB_HD double press_from_valid_rho_kappa_ye(double rho, double kappa, double) const {
+    return kappa * pow(rho, gamma);
+  }
+  AXB_HD double eps_from_valid_rho_kappa_ye(double rho, double kappa, double) const {
+    return kappa * pow(rho, gamma - 1.0) / (gamma - 1.0);
+  }
   AXB_HD double kappa_from_valid_rho_eps_ye(double rho, double &eps, double) const {
     double r;
     if (kappa_root == 3) {

@@ -30,6 +30,7 @@ struct C2PBoxArgs {
   // settings
   C2PParams cp;
   int c2p_prime, c2p_second, excise, thermal_eos_atmo, use_press_atmo;
+  int use_entropy_fix; // the entropy scheme after both schemes failed
   int atmo_uniform;
   Atmo atmo_const; // when atmo_uniform
   double rho_abs_min, r_atmo, n_rho_atmo, p_atmo, n_press_atmo, t_atmo,
@@ -110,6 +111,38 @@ AXB_D void run_solver(int which, const EOS &eos, const C2PBoxArgs &a,
     noble_solve(eos, a.cp, atmo, a.gamma_noble, a.Zmin, pv, seeds, cv, glo, rep);
   else if (which == AXB_C2P_PALENZUELA)
     palenzuela_solve(eos, a.cp, atmo, pv, cv, glo, rep);
+  else if (which == AXB_C2P_ENTROPY)
+    entropy_solve(eos, a.cp, atmo, pv, cv, glo, rep);
+}
+
+// Both schemes failed (con2prim.cxx:308-416): the entropy scheme when
+// use_entropy_fix, then, if that fails too (or without it), the failure
+// treatment -- BH-interior values inside the mask, else atmosphere with the
+// cell's B.  Returns the flag code; `failed` marks a cell nothing recovered.
+template <class EOS>
+AXB_D int after_both_failed(const EOS &eos, const C2PBoxArgs &a, const Atmo &atmo,
+                            double mask_local, double sqrt_detg, const double (&Bup)[3],
+                            Prim &pv, Prim &seeds, Cons &cv, const sym3 &glo,
+                            bool &flag_local, bool &failed) {
+  if (a.use_entropy_fix) {
+    Report re;
+    entropy_solve(eos, a.cp, atmo, pv, cv, glo, re);
+    if (!re.failed())
+      return AXB_C2P_ENTROPY_OK;
+  }
+  flag_local = false;
+  failed = true;
+  if (mask_local != 1.0) {
+    bh_interior<false>(eos, a.cp, atmo, seeds, cv, glo);
+    pv = seeds;
+  } else {
+    for (int q = 0; q < 3; ++q) {
+      cv.dBvec[q] = sqrt_detg * Bup[q];
+      pv.Bvec[q] = Bup[q];
+    }
+    atmo.set(pv, cv, glo);
+  }
+  return AXB_C2P_FAIL;
 }
 
 // One cell of AsterX_Con2Prim_typeEoS (con2prim.cxx:81-453), preceded by
@@ -257,21 +290,9 @@ AXB_D bool c2p_cell(const C2PBoxArgs &a, const EOS &eos, const int i, const int 
         code = AXB_C2P_SECOND;
         run_solver(a.c2p_second, eos, a, atmo, pv, seeds, cv, glo, r2);
       }
-      if (r1.failed() && r2.failed()) {
-        flag_local = false;
-        code = AXB_C2P_FAIL;
-        failed = true;
-        if (mask_local != 1.0) {
-          bh_interior<false>(eos, a.cp, atmo, seeds, cv, glo);
-          pv = seeds;
-        } else {
-          for (int q = 0; q < 3; ++q) {
-            cv.dBvec[q] = sqrt_detg * Bup[q];
-            pv.Bvec[q] = Bup[q];
-          }
-          atmo.set(pv, cv, glo);
-        }
-      }
+      if (r1.failed() && r2.failed())
+        code = after_both_failed(eos, a, atmo, mask_local, sqrt_detg, Bup, pv, seeds, cv, glo,
+                                 flag_local, failed);
       if ((mask_local != 1.0) && flag_local)
         bh_interior<true>(eos, a.cp, atmo, pv, cv, glo);
     }
@@ -539,11 +560,17 @@ int fill_c2p_args(axb_ctx *c, const axb_box *box, const axb_fields *f,
   if (!f || !p || !eos)
     return AXB_ERR_ARG;
   const bool ok_solver = [](int s) {
-    return s == AXB_C2P_NOBLE || s == AXB_C2P_PALENZUELA;
+    return s == AXB_C2P_NOBLE || s == AXB_C2P_PALENZUELA || s == AXB_C2P_ENTROPY;
   }(p->c2p_prime);
-  if (!ok_solver || p->use_entropy_fix || p->use_mask ||
+  if (!ok_solver || p->use_mask ||
       !(p->c2p_second == AXB_C2P_NOBLE || p->c2p_second == AXB_C2P_PALENZUELA ||
-        p->c2p_second == AXB_C2P_NONE))
+        p->c2p_second == AXB_C2P_ENTROPY || p->c2p_second == AXB_C2P_NONE))
+    return AXB_ERR_UNSUPPORTED;
+  // the entropy scheme needs p(rho, kappa), which a table does not define
+  // (eos_3p_tabulated3d.hxx:315-333)
+  const bool entropy = p->use_entropy_fix || p->c2p_prime == AXB_C2P_ENTROPY ||
+                       p->c2p_second == AXB_C2P_ENTROPY;
+  if (entropy && eos->kind != 0)
     return AXB_ERR_UNSUPPORTED;
   if (!(p->c2p_tol > 0) || p->max_iter < 1)
     return AXB_ERR_ARG;
@@ -609,6 +636,7 @@ int fill_c2p_args(axb_ctx *c, const axb_box *box, const axb_fields *f,
   a.cp = make_c2p_params(*p);
   a.c2p_prime = p->c2p_prime;
   a.c2p_second = p->c2p_second;
+  a.use_entropy_fix = p->use_entropy_fix;
   a.excise = p->excise;
   a.thermal_eos_atmo = p->thermal_eos_atmo;
   a.use_press_atmo = p->use_press_atmo;
@@ -843,7 +871,7 @@ int launch_mlp_guess(const axb_cells &c, const axb_mlp *m, float2 *guess, cudaSt
 struct C2PCellsArgs {
   axb_cells c;
   C2PParams cp;
-  int c2p_prime, c2p_second;
+  int c2p_prime, c2p_second, use_entropy_fix;
   Atmo atmo;
   double gamma_noble, Zmin;
   int use_mlp;
@@ -861,6 +889,8 @@ AXB_D void run_solver_cells(int which, const EOS &eos, const C2PCellsArgs &a, Pr
                 vsqguess);
   else if (which == AXB_C2P_PALENZUELA)
     palenzuela_solve(eos, a.cp, a.atmo, pv, cv, glo, rep, xlo, xhi);
+  else if (which == AXB_C2P_ENTROPY)
+    entropy_solve(eos, a.cp, a.atmo, pv, cv, glo, rep);
 }
 
 template <class EOS>
@@ -978,7 +1008,15 @@ __global__ void __launch_bounds__(128, AXB_C2P_MINB)
         run_solver_cells(a.c2p_second, eos, a, pv, seeds, cv, glo, r2, -1.0, -1.0, -1.0,
                          -1.0);
       }
-      if (r1.failed() && r2.failed()) {
+      bool recovered = false;
+      if (r1.failed() && r2.failed() && a.use_entropy_fix) {
+        Report re;
+        entropy_solve(eos, a.cp, a.atmo, pv, cv, glo, re);
+        recovered = !re.failed();
+        if (recovered)
+          code = AXB_C2P_ENTROPY_OK;
+      }
+      if (r1.failed() && r2.failed() && !recovered) {
         code = AXB_C2P_FAIL;
         failed = true;
         for (int q = 0; q < 3; ++q) {
@@ -1041,9 +1079,17 @@ AXB_API int axb_c2p_cells(axb_ctx *ctx, const axb_cells *cells, const axb_params
   if (cells->seed_rho && (!cells->seed_eps || !cells->seed_Ye || !cells->seed_vel[0] ||
                           !cells->seed_vel[1] || !cells->seed_vel[2]))
     return AXB_ERR_ARG;
-  auto ok_solver = [](int s) { return s == AXB_C2P_NOBLE || s == AXB_C2P_PALENZUELA; };
+  auto ok_solver = [](int s) {
+    return s == AXB_C2P_NOBLE || s == AXB_C2P_PALENZUELA || s == AXB_C2P_ENTROPY;
+  };
   if (!ok_solver(p->c2p_prime) || !(ok_solver(p->c2p_second) || p->c2p_second == AXB_C2P_NONE))
     return AXB_ERR_UNSUPPORTED;
+  const bool entropy = p->use_entropy_fix || p->c2p_prime == AXB_C2P_ENTROPY ||
+                       p->c2p_second == AXB_C2P_ENTROPY;
+  if (entropy && eos->kind != 0)
+    return AXB_ERR_UNSUPPORTED; // p(rho, kappa) is not defined for a table
+  if (entropy && !cells->DEnt)
+    return AXB_ERR_ARG; // the entropy scheme reads the conserved entropy
   if (!(p->c2p_tol > 0) || p->max_iter < 1)
     return AXB_ERR_ARG;
   C2PCellsArgs a;
@@ -1051,6 +1097,7 @@ AXB_API int axb_c2p_cells(axb_ctx *ctx, const axb_cells *cells, const axb_params
   a.cp = make_c2p_params(*p);
   a.c2p_prime = p->c2p_prime;
   a.c2p_second = p->c2p_second;
+  a.use_entropy_fix = p->use_entropy_fix;
   a.status = ctx->status;
   a.use_mlp = mlp != nullptr;
   a.bracket = 0.0;

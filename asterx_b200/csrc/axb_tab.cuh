@@ -206,6 +206,11 @@ struct EosTab {
   AXB_HD double kappa_from_valid_rho_eps_ye(double rho, double &eps, double ye) const {
     return entropy_from_valid_rho_temp_ye(rho, temp_from_valid_rho_eps_ye(rho, eps, ye), ye);
   }
+  // not defined for a table (the reference prints and asserts,
+  // eos_3p_tabulated3d.hxx:315-333); the entry points reject the entropy
+  // scheme with a tabulated EOS, so these are never reached
+  AXB_HD double press_from_valid_rho_kappa_ye(double, double, double) const { return nan(""); }
+  AXB_HD double eps_from_valid_rho_kappa_ye(double, double, double) const { return nan(""); }
 };
 
 } // namespace axb

@@ -260,15 +260,19 @@ AXB_API int axb_rhs_group(axb_ctx *ctx, const axb_box *box,
  * AsterX_ComputedBstagFromA (AsterX/src/computeBfromA.cxx:58-65),
  * AsterX_ComputedBFromdBstag (:67-85) and AsterX_Con2Prim
  * (AsterX/src/con2prim.cxx:457-502) with the Con2PrimFactory functors
- * c2p_2DNoble::solve (Con2PrimFactory/src/c2p_2DNoble.hxx:275-594) and
- * c2p_1DPalenzuela::solve (Con2PrimFactory/src/c2p_1DPalenzuela.hxx:306-556).
+ * c2p_2DNoble::solve (Con2PrimFactory/src/c2p_2DNoble.hxx:275-594),
+ * c2p_1DPalenzuela::solve (Con2PrimFactory/src/c2p_1DPalenzuela.hxx:306-556)
+ * and c2p_1DEntropy::solve (Con2PrimFactory/src/c2p_1DEntropy.hxx:306-469).
  * Reads: Avec_* (interior edges + one ghost layer), conserved variables,
  *   saved_* and temperature (seeds), metric and lapse.
  * Writes: dB*_stag on the interior faces and one transverse ghost layer,
  *   dB*, the HydroBaseX primitives, conserved variables (after floors),
  *   saved_*, con2prim_flag, and zvec_* / svec_* when given.
- * c2p_prime and c2p_second must be Noble or Palenzuela (second may be None);
- * use_entropy_fix and use_mask are not supported (AXB_ERR_UNSUPPORTED).
+ * c2p_prime and c2p_second are Noble, Palenzuela or Entropy (second may be
+ * None); use_entropy_fix runs the entropy scheme on cells both failed
+ * (flag AXB_C2P_ENTROPY_OK when it recovers them).  The entropy scheme
+ * needs the ideal gas (a table defines no p(rho, kappa)); use_mask is not
+ * supported (AXB_ERR_UNSUPPORTED).
  * C2P_FAIL cells are counted in the context status. */
 AXB_API int axb_con2prim_group(axb_ctx *ctx, const axb_box *box,
                                const axb_fields *fields,

@@ -94,3 +94,57 @@ def test_ssprk3_step(engine, ref, recon):
     for n in ["rho", "eps", "press", "velx", "vely", "velz", "Bvecx"] + EVOLVED:
         emax, _ = errors(interior(L, n, got[n]), interior(L, n, host[n]))
         assert emax <= TOL, (n, emax)
+
+
+def run_c2p_both(engine, ref, L, f, p):
+    host = {n: a.copy() for n, a in f.items()}
+    ref.setup(L, p, host)
+    ref.eos_idealgas(GAMMA, **EOS_KW)
+    ref.con2prim_group()
+    eos = engine.eos_idealgas(GAMMA, **EOS_KW)
+    dev = engine.upload(L, f)
+    engine.status_reset()
+    engine.con2prim_group(L, dev, p, eos)
+    st = engine.status()
+    return host, {n: dev[n].cpu().numpy() for n in dev}, st
+
+
+@pytest.mark.gpu
+def test_entropy_scheme_first(engine, ref):
+    """c2p_1DEntropy::solve (Con2PrimFactory/src/c2p_1DEntropy.hxx) as the
+    first scheme on every cell: flags identical, primitives within 1e-10."""
+    L, f = case(23)
+    p = abi.default_params(c2p_prime="entropy", c2p_second="none", c2p_tol=1e-14,
+                           max_iter=100, vw_lim=1e3, B_lim=1e4)
+    host, got, st = run_c2p_both(engine, ref, L, f, p)
+    flags_r = interior(L, "x", host["con2prim_flag"])
+    assert np.array_equal(interior(L, "x", got["con2prim_flag"]), flags_r)
+    assert (flags_r == abi.C2P_PRIME).mean() > 0.9
+    for n in OUT_C2P:
+        emax, _ = errors(interior(L, n, got[n]), interior(L, n, host[n]))
+        assert emax <= TOL, (n, emax)
+
+
+@pytest.mark.gpu
+def test_entropy_fix_after_both_schemes_fail(engine, ref):
+    """use_entropy_fix (con2prim.cxx:308-364): cells whose tau is far below
+    what their other conserved variables need fail Noble and Palenzuela
+    (negative eps); the entropy scheme, which does not read tau, recovers
+    them and recomputes tau.  Flags identical (C2P_ENTROPY among them),
+    primitives and conserved variables within 1e-10."""
+    L, f = case(24)
+    rng = np.random.default_rng(25)
+    sl = L.interior((1, 1, 1))
+    tau = L.view(f["tau"])
+    hit = rng.uniform(size=tau[sl].shape) < 0.15
+    tau[sl] = np.where(hit, -np.abs(tau[sl]), tau[sl])
+    p = abi.default_params(c2p_prime="noble", c2p_second="palenzuela", c2p_tol=1e-12,
+                           max_iter=100, vw_lim=1e3, B_lim=1e4, use_entropy_fix=1)
+    host, got, st = run_c2p_both(engine, ref, L, f, p)
+    flags_r = interior(L, "x", host["con2prim_flag"])
+    assert np.array_equal(interior(L, "x", got["con2prim_flag"]), flags_r)
+    assert (flags_r == abi.C2P_ENTROPY).sum() > 0.05 * flags_r.size
+    for n in OUT_C2P:
+        emax, _ = errors(interior(L, n, got[n]), interior(L, n, host[n]))
+        assert emax <= TOL, (n, emax)
+    assert st["c2p_fail"] == int((flags_r == abi.C2P_FAIL).sum())
