@@ -35,6 +35,10 @@ GF_NAMES = [
     "fxBy", "fxBz", "fyBx", "fyBz", "fzBx", "fzBy",
     "acc_dens", "acc_momx", "acc_momy", "acc_momz", "acc_tau", "acc_DYe",
     "acc_DEnt",
+    # upwind CT face data
+    "vtilde_y_xface", "vtilde_z_xface", "vtilde_z_yface", "vtilde_x_yface",
+    "vtilde_x_zface", "vtilde_y_zface", "amax_xface", "amin_xface",
+    "amax_yface", "amin_yface", "amax_zface", "amin_zface",
 ]
 GF = {n: i for i, n in enumerate(GF_NAMES)}
 NUM_GF = len(GF_NAMES)
@@ -55,6 +59,11 @@ AUX = ["Fx", "Fy", "Fz", "Fbetax", "Fbetay", "Fbetaz", "G"]
 BFLUX = ["fxBy", "fxBz", "fyBx", "fyBz", "fzBx", "fzBy"]
 ACC = ["acc_dens", "acc_momx", "acc_momy", "acc_momz", "acc_tau", "acc_DYe",
        "acc_DEnt"]
+UCT = ["vtilde_y_xface", "vtilde_z_xface", "amax_xface", "amin_xface",
+       "vtilde_z_yface", "vtilde_x_yface", "amax_yface", "amin_yface",
+       "vtilde_x_zface", "vtilde_y_zface", "amax_zface", "amin_zface"]
+# centring (x, y, z; 1 = cell, 0 = vertex) of the upwind-CT face data
+UCT_CENT = {n: {"x": (0, 1, 1), "y": (1, 0, 1), "z": (1, 1, 0)}[n[-5]] for n in UCT}
 
 RECON = {"godunov": 0, "minmod": 1, "monocentral": 2, "ppm": 3, "eppm": 4,
          "wenoz": 5, "mp5": 6}

@@ -29,10 +29,13 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
 # the surrounding code, and the Brent bracket amplifies a last-bit
 # difference to the root-finder tolerance.  It also follows the per-operation
 # rounding of the reference's CPU build.
+# The recovery is split over three translation units (single box, batched,
+# independent cells) that share axb_c2p_box.cuh, so they compile in parallel.
 # The stress-energy tensor and the regrid error follow the reference's
 # operation order without contraction as well, which makes them bit-equal to
 # the reference's CPU build.
-FILE_FLAGS = {"axb_poststep.cu": ["-fmad=false"], "axb_tmunu.cu": ["-fmad=false"]}
+FILE_FLAGS = {"axb_poststep.cu": ["-fmad=false"], "axb_c2p_batch.cu": ["-fmad=false"],
+              "axb_c2p_cells.cu": ["-fmad=false"], "axb_tmunu.cu": ["-fmad=false"]}
 
 
 def _includes(path, seen=None):

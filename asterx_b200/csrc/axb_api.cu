@@ -372,7 +372,7 @@ int fill_rhs_args(axb_ctx *c, const axb_box *box, const axb_fields *f,
     return rc;
   if (!f || !p)
     return AXB_ERR_ARG;
-  if (p->recon_type < AXB_RECVAR_V || p->recon_type > AXB_RECVAR_S || p->use_uct ||
+  if (p->recon_type < AXB_RECVAR_V || p->recon_type > AXB_RECVAR_S ||
       p->reconstruction_method == AXB_RECON_EPPM ||
       !(p->local_spatial_order == 2 || p->local_spatial_order == 4))
     return AXB_ERR_UNSUPPORTED;
@@ -440,6 +440,17 @@ int fill_rhs_args(axb_ctx *c, const axb_box *box, const axb_fields *f,
                         AXB_GF_Fbetay, AXB_GF_Fbetaz, AXB_GF_G};
   for (int q = 0; q < 7; ++q)
     a.aux[q] = f->gf[auxid[q]];
+  // upwind CT: per face direction vtilde^{d+1}, vtilde^{d+2}, amax, amin
+  static const int uctid[12] = {
+      AXB_GF_vtilde_y_xface, AXB_GF_vtilde_z_xface, AXB_GF_amax_xface, AXB_GF_amin_xface,
+      AXB_GF_vtilde_z_yface, AXB_GF_vtilde_x_yface, AXB_GF_amax_yface, AXB_GF_amin_yface,
+      AXB_GF_vtilde_x_zface, AXB_GF_vtilde_y_zface, AXB_GF_amax_zface, AXB_GF_amin_zface};
+  a.use_uct = p->use_uct != 0;
+  for (int q = 0; q < 12; ++q)
+    a.uct[q] = a.use_uct ? f->gf[uctid[q]] : nullptr;
+  // the flux passes cover 1 transverse ghost layer, 3 with upwind CT
+  a.text = a.use_uct ? 3 : 1;
+  a.recon_method = p->reconstruction_method;
   a.Arhs[0] = GFP(Avec_x_rhs);
   a.Arhs[1] = GFP(Avec_y_rhs);
   a.Arhs[2] = GFP(Avec_z_rhs);
@@ -469,6 +480,9 @@ int fill_rhs_args(axb_ctx *c, const axb_box *box, const axb_fields *f,
       return AXB_ERR_ARG;
   for (int q = 0; q < 3; ++q)
     if (!a.recv[q])
+      return AXB_ERR_ARG;
+  for (int q = 0; q < 12; ++q)
+    if (a.use_uct && !a.uct[q])
       return AXB_ERR_ARG;
   return AXB_OK;
 }
@@ -551,6 +565,14 @@ int rhs_group_run(axb_ctx *c, const axb_box *box, const axb_fields *f,
                                  AXB_GF_Fbetay, AXB_GF_Fbetaz, AXB_GF_G};
   if (bc && (rc = axb_fill_boundary(c, box, f, bflux_ids, 6, bc, stream)))
     return rc;
+  // upwind CT: its face data of the ghost layers likewise (the reference
+  // SYNCs vtilde_*face and a_*face, AsterX/schedule.ccl:189-193)
+  static const int uct_ids[12] = {
+      AXB_GF_vtilde_y_xface, AXB_GF_vtilde_z_xface, AXB_GF_amax_xface, AXB_GF_amin_xface,
+      AXB_GF_vtilde_z_yface, AXB_GF_vtilde_x_yface, AXB_GF_amax_yface, AXB_GF_amin_yface,
+      AXB_GF_vtilde_x_zface, AXB_GF_vtilde_y_zface, AXB_GF_amax_zface, AXB_GF_amin_zface};
+  if (bc && a.use_uct && (rc = axb_fill_boundary(c, box, f, uct_ids, 12, bc, stream)))
+    return rc;
   axb_mark(c, AXB_R_AUX, s, true);
   rc = launch_rhs_misc(2, a, s);
   axb_mark(c, AXB_R_AUX, s, false);
@@ -615,8 +637,21 @@ int launch_rhs_misc(int which, const RhsArgs &a, cudaStream_t s) {
     const dim3 grid(unsigned((plane + T - 1) / T), 1, b.n[2] + e);
     if (which == 2)
       k_aux<<<grid, T, 0, s>>>(ap);
-    else
+    else if (!a.use_uct)
       k_ct_psi<<<grid, T, 0, s>>>(ap);
+    else {
+      switch (a.recon_method) {
+      case AXB_RECON_GODUNOV: k_ct_psi_uct<AXB_RECON_GODUNOV><<<grid, T, 0, s>>>(ap); break;
+      case AXB_RECON_MINMOD: k_ct_psi_uct<AXB_RECON_MINMOD><<<grid, T, 0, s>>>(ap); break;
+      case AXB_RECON_MONOCENTRAL:
+        k_ct_psi_uct<AXB_RECON_MONOCENTRAL><<<grid, T, 0, s>>>(ap);
+        break;
+      case AXB_RECON_PPM: k_ct_psi_uct<AXB_RECON_PPM><<<grid, T, 0, s>>>(ap); break;
+      case AXB_RECON_WENOZ: k_ct_psi_uct<AXB_RECON_WENOZ><<<grid, T, 0, s>>>(ap); break;
+      case AXB_RECON_MP5: k_ct_psi_uct<AXB_RECON_MP5><<<grid, T, 0, s>>>(ap); break;
+      default: return AXB_ERR_UNSUPPORTED;
+      }
+    }
   }
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
 }
@@ -640,7 +675,7 @@ __global__ void __launch_bounds__(128) k_aux_batch(const RhsArgs *args, const Ti
   batch_loop(args, t, ctr, [&](const RhsArgs &a, const uint3 bid) { aux_body(a, bid); });
 }
 __global__ void __launch_bounds__(128) k_ct_psi_batch(const RhsArgs *args, const TileTable t, unsigned long long *ctr) {
-  batch_loop(args, t, ctr, [&](const RhsArgs &a, const uint3 bid) { ct_psi_body(a, bid); });
+  batch_loop(args, t, ctr, [&](const RhsArgs &a, const uint3 bid) { ct_psi_body<-1>(a, bid); });
 }
 } // namespace
 
@@ -655,6 +690,8 @@ int batch_rhs_setup(axb_ctx *c, int nbox, const axb_box *boxes, const axb_fields
     return AXB_ERR_ARG;
   for (int b = 0; b < nbox; ++b) {
     int rc = fill_rhs_args(c, boxes + b, f + b, p, h[b]);
+    if (!rc && p->use_uct)
+      rc = AXB_ERR_UNSUPPORTED; // the batched CT kernel is flux CT only
     h[b].b.packed = 1;
     if (!rc && eos->kind == 1 && !h[b].rec_temp)
       rc = AXB_ERR_UNSUPPORTED;

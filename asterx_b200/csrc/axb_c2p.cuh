@@ -82,7 +82,9 @@ enum RepStatus {
   REP_PREP_ROOT_FAIL_BRACKET,
   REP_NOT_SET,
   // (engine only) the fast pass left the cell to the full cascade
-  REP_DEFER
+  REP_DEFER,
+  // (engine only) the staged solve handed its bracket over (PAL_SETUP)
+  REP_PENDING
 };
 struct Report {
   int status = REP_NOT_SET;
@@ -543,6 +545,108 @@ AXB_HD void noble_solve(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
     cv.scale(sqrt_detg);
 }
 
+// Brent's method as a resumable state: brent_init handles the bracket's
+// degenerate cases (a root at an end, no sign change), brent_step does one
+// iteration of the loop.  brent_bracket runs them to completion; the pooled
+// recovery pass runs one step at a time, so a lane whose cell converged can
+// take the next cell.  Both produce the same iterates and the same bits.
+struct BrentState {
+  double a, b, c, d, fa, fb, fc;
+  int iters;
+  bool mflag;
+};
+// true: the result (lo, hi) is final without an iteration
+AXB_HD bool brent_init(BrentState &st, double a, double b, double fa, double fb, double &lo,
+                       double &hi) {
+  st.iters = 0;
+  if (fa == 0) {
+    lo = hi = a;
+    return true;
+  }
+  if (fb == 0) {
+    lo = hi = b;
+    return true;
+  }
+  if (fa * fb > 0) {
+    lo = fmin(a, b);
+    hi = fmax(a, b);
+    return true;
+  }
+  if (fabs(fa) < fabs(fb)) {
+    double t = a; a = b; b = t;
+    t = fa; fa = fb; fb = t;
+  }
+  st.a = a;
+  st.b = b;
+  st.fa = fa;
+  st.fb = fb;
+  st.c = a;
+  st.fc = fa;
+  st.d = a;
+  st.mflag = true;
+  return false;
+}
+// One pass of the loop; true when (lo, hi) is final.  `eps` = 2^-minbits.
+template <class F>
+AXB_HD bool brent_step(BrentState &st, const F &f, double eps, int maxiters, double &lo,
+                       double &hi) {
+  double a = st.a, b = st.b, c = st.c, d = st.d, fa = st.fa, fb = st.fb, fc = st.fc;
+  if (st.iters >= maxiters || fabs(b - a) <= eps * fmin(fabs(a), fabs(b))) {
+    lo = fmin(a, b);
+    hi = fmax(a, b);
+    return true;
+  }
+  ++st.iters;
+  double s;
+  if (fa != fc && fb != fc) {
+    // inverse quadratic interpolation over one common denominator
+    // (fa-fb)(fa-fc)(fb-fc) instead of three (last-ulp differences)
+    const double dab = fa - fb, dac = fa - fc, dbc = fb - fc;
+    s = (a * fb * fc * dbc - b * fa * fc * dac + c * fa * fb * dab) / (dab * dac * dbc);
+  } else {
+    s = b - fb * (b - a) / (fb - fa);
+  }
+  const double delta = eps * fabs(b);
+  const double q = (3 * a + b) / 4;
+  const bool mflag = st.mflag;
+  const bool out_of_range = !((s > fmin(q, b)) && (s < fmax(q, b)));
+  if (out_of_range || (mflag && fabs(s - b) >= fabs(b - c) / 2) ||
+      (!mflag && fabs(s - b) >= fabs(c - d) / 2) || (mflag && fabs(b - c) < delta) ||
+      (!mflag && fabs(c - d) < delta)) {
+    s = (a + b) / 2;
+    st.mflag = true;
+  } else {
+    st.mflag = false;
+  }
+  const double fs = f(s);
+  d = c;
+  c = b;
+  fc = fb;
+  if (fa * fs < 0) {
+    b = s;
+    fb = fs;
+  } else {
+    a = s;
+    fa = fs;
+  }
+  if (fabs(fa) < fabs(fb)) {
+    double t = a; a = b; b = t;
+    t = fa; fa = fb; fb = t;
+  }
+  st.a = a;
+  st.b = b;
+  st.c = c;
+  st.d = d;
+  st.fa = fa;
+  st.fb = fb;
+  st.fc = fc;
+  if (fb == 0) {
+    lo = hi = b;
+    return true;
+  }
+  return false;
+}
+
 // ---------------------------------------------------------------------------
 // Brent's bracketing root finder with the contract of CarpetX's Algo::brent
 // as used at c2p_1DPalenzuela.hxx:380-417: returns a bracket (lo, hi) of a
@@ -558,74 +662,14 @@ template <class F>
 AXB_HD void brent_bracket(const F &f, double a, double b, double fa0, double fb0,
                           int minbits, int maxiters, int &iters, double &lo, double &hi) {
   const double eps = ldexp(1.0, -minbits);
-  double fa = fa0;
-  double fb = fb0;
-  iters = 0;
-  if (fa == 0) {
-    lo = hi = a;
+  BrentState st;
+  if (brent_init(st, a, b, fa0, fb0, lo, hi)) {
+    iters = 0;
     return;
   }
-  if (fb == 0) {
-    lo = hi = b;
-    return;
+  while (!brent_step(st, f, eps, maxiters, lo, hi)) {
   }
-  if (fa * fb > 0) {
-    lo = fmin(a, b);
-    hi = fmax(a, b);
-    return;
-  }
-  if (fabs(fa) < fabs(fb)) {
-    double t = a; a = b; b = t;
-    t = fa; fa = fb; fb = t;
-  }
-  double c = a, fc = fa, d = a;
-  bool mflag = true;
-  while (iters < maxiters) {
-    if (fabs(b - a) <= eps * fmin(fabs(a), fabs(b)))
-      break;
-    ++iters;
-    double s;
-    if (fa != fc && fb != fc) {
-      // inverse quadratic interpolation over one common denominator
-      // (fa-fb)(fa-fc)(fb-fc) instead of three (last-ulp differences)
-      const double dab = fa - fb, dac = fa - fc, dbc = fb - fc;
-      s = (a * fb * fc * dbc - b * fa * fc * dac + c * fa * fb * dab) / (dab * dac * dbc);
-    } else {
-      s = b - fb * (b - a) / (fb - fa);
-    }
-    const double delta = eps * fabs(b);
-    const double q = (3 * a + b) / 4;
-    const bool out_of_range = !((s > fmin(q, b)) && (s < fmax(q, b)));
-    if (out_of_range || (mflag && fabs(s - b) >= fabs(b - c) / 2) ||
-        (!mflag && fabs(s - b) >= fabs(c - d) / 2) || (mflag && fabs(b - c) < delta) ||
-        (!mflag && fabs(c - d) < delta)) {
-      s = (a + b) / 2;
-      mflag = true;
-    } else {
-      mflag = false;
-    }
-    const double fs = f(s);
-    d = c;
-    c = b;
-    fc = fb;
-    if (fa * fs < 0) {
-      b = s;
-      fb = fs;
-    } else {
-      a = s;
-      fa = fs;
-    }
-    if (fabs(fa) < fabs(fb)) {
-      double t = a; a = b; b = t;
-      t = fa; fa = fb; fb = t;
-    }
-    if (fb == 0) {
-      lo = hi = b;
-      return;
-    }
-  }
-  lo = fmin(a, b);
-  hi = fmax(a, b);
+  iters = st.iters;
 }
 
 // Palenzuela invariants (c2p_1DPalenzuela.hxx:150-153,267-270), plus the
@@ -640,8 +684,8 @@ struct PalQRST {
 // division, and P/rho comes from the EOS without a division (last-ulp
 // differences; the bracket search converges to the same tolerance).
 template <class EOS>
-AXB_HD double pal_froot(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
-                        const PalQRST &k, double x, const Cons &cv) {
+AXB_HD double pal_froot_s(const EOS &eos, int use_temp, double atmo_eps, const PalQRST &k,
+                          double x, double dens) {
   const double xs = x + k.s;
   const double ixxs = 1.0 / (x * xs); // 1/(x (x+s)); 1/x = (x+s)/(x (x+s))
   const double ix = xs * ixxs;
@@ -649,16 +693,35 @@ AXB_HD double pal_froot(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
   Wminus2 = fmin(fmax(Wminus2, 1e-10), 1);
   const double W_loc = rsqrt(Wminus2);
   const double iW = Wminus2 * W_loc;
-  const double rho_loc = cv.dens * iW;
+  const double rho_loc = dens * iW;
   const double Ye_loc = k.ye;
   double eps_loc = W_loc - 1.0 + (1.0 - W_loc * W_loc) * x * iW +
                    W_loc * (k.q - k.s + 0.5 * k.t * k.t * (ix * ix) + 0.5 * k.s * Wminus2);
-  if (cp.use_temp) {
-    eps_loc = fmax(eps_loc, atmo.eps);
+  if (use_temp) {
+    eps_loc = fmax(eps_loc, atmo_eps);
     eps_loc = fmin(eps_loc, eos.rgeps.max);
   }
   return (x - (1.0 + eps_loc + eos.press_over_rho(rho_loc, eps_loc, Ye_loc)) * W_loc);
 }
+template <class EOS>
+AXB_HD double pal_froot(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
+                        const PalQRST &k, double x, const Cons &cv) {
+  return pal_froot_s(eos, cp.use_temp, atmo.eps, k, x, cv.dens);
+}
+
+// The Palenzuela solve in stages (the pooled recovery pass): PAL_SETUP stops
+// once the bracket and its end values are known and hands them over
+// (status REP_PENDING); PAL_FINISH takes the finished bracket and its
+// iteration count instead of running the root finder.  PAL_ALL is the solve
+// in one piece.
+enum { PAL_ALL = 0, PAL_SETUP = 1, PAL_FINISH = 2 };
+struct PalHandoff {
+  PalQRST k;
+  double dens, atmo_eps;
+  double a, b, fa, fb; // PAL_SETUP out
+  double lo, hi;       // PAL_FINISH in
+  int iters;           // PAL_FINISH in
+};
 
 // Palenzuela 1D (c2p_1DPalenzuela::solve, c2p_1DPalenzuela.hxx:306-556).
 // `xlo`/`xhi` > 0 narrow the initial bracket (learned initial guess); the
@@ -666,10 +729,13 @@ AXB_HD double pal_froot(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
 // FAST: the common path only -- every failure, and a bracket that did not
 // converge (which needs the conservative-variable check), returns REP_DEFER
 // before anything else, so the caller can hand the cell to the full cascade.
-template <class EOS, bool FAST = false>
+// STAGE / `h`: see PalHandoff (the staged form is only used with FAST).
+template <class EOS, bool FAST = false, int STAGE = PAL_ALL>
 AXB_HD void palenzuela_solve(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
                              Prim &pv, Cons &cv, const sym3 &glo, Report &rep,
-                             double xlo = -1.0, double xhi = -1.0) {
+                             double xlo = -1.0, double xhi = -1.0,
+                             PalHandoff *h = nullptr) {
+  static_assert(STAGE == PAL_ALL || FAST, "the staged solve is the fast path's");
   rep.iters = 0;
   rep.adjust_cons = false;
   rep.set_atmo = false;
@@ -734,28 +800,46 @@ AXB_HD void palenzuela_solve(const EOS &eos, const C2PParams &cp, const Atmo &at
   double a = fmax(1e-10, 1.0 + qP - sP);
   double b = 2.0 + 2.0 * qP - sP;
   auto fn = [&](double x) { return pal_froot(eos, cp, atmo, k, x, cv); };
-  bool narrowed = false;
-  double fa = 0.0, fb = 0.0;
-  if (xlo > 0.0 && xhi > xlo) {
-    const double flo = fn(xlo), fhi = fn(xhi);
-    if (flo * fhi < 0) {
-      a = xlo;
-      b = xhi;
-      fa = flo;
-      fb = fhi;
-      narrowed = true;
-    }
-  }
-  if (!narrowed) {
-    fa = fn(a);
-    fb = fn(b);
-    if (fa * fb > 0) {
-      b = 3.0 + 3.0 * qP - 1.5 * sP;
-      fb = fn(b);
-    }
-  }
   double r0, r1;
-  brent_bracket(fn, a, b, fa, fb, cp.minbits, cp.maxIter, rep.iters, r0, r1);
+  if constexpr (STAGE == PAL_FINISH) {
+    r0 = h->lo;
+    r1 = h->hi;
+    rep.iters = h->iters;
+  } else {
+    bool narrowed = false;
+    double fa = 0.0, fb = 0.0;
+    if (xlo > 0.0 && xhi > xlo) {
+      const double flo = fn(xlo), fhi = fn(xhi);
+      if (flo * fhi < 0) {
+        a = xlo;
+        b = xhi;
+        fa = flo;
+        fb = fhi;
+        narrowed = true;
+      }
+    }
+    if (!narrowed) {
+      fa = fn(a);
+      fb = fn(b);
+      if (fa * fb > 0) {
+        b = 3.0 + 3.0 * qP - 1.5 * sP;
+        fb = fn(b);
+      }
+    }
+    if constexpr (STAGE == PAL_SETUP) {
+      h->k = k;
+      h->dens = cv.dens;
+      h->atmo_eps = atmo.eps;
+      h->a = a;
+      h->b = b;
+      h->fa = fa;
+      h->fb = fb;
+      rep.status = REP_PENDING;
+      return;
+    } else {
+      brent_bracket(fn, a, b, fa, fb, cp.minbits, cp.maxIter, rep.iters, r0, r1);
+    }
+  }
   const bool converged = !(fabs(r0 - r1) > cp.tolerance_0 * fmin(fabs(r0), fabs(r1)));
   if constexpr (FAST) {
     if (!converged) {

@@ -13,8 +13,8 @@ int launch_flux_pass_eos(int dir, const RhsArgs &a, const EOS &eos, int seglen,
                          cudaStream_t s) {
   const BoxDev &b = a.b;
   if (dir == 0) {
-    // one warp per (y, z) row of the transverse range [ng-1, ng+n]^2
-    const long long warps = (long long)(b.n[1] + 2) * (b.n[2] + 2);
+    // one warp per (y, z) row of the transverse range [ng-te, ng+n+te-1]^2
+    const long long warps = (long long)(b.n[1] + 2 * a.text) * (b.n[2] + 2 * a.text);
     const long long blocks = (warps * 32 + 127) / 128;
     if (blocks > 0x7fffffffLL)
       return AXB_ERR_TOO_LARGE;
@@ -30,7 +30,7 @@ int launch_flux_pass_eos(int dir, const RhsArgs &a, const EOS &eos, int seglen,
   // share the face metric's second vertex row in L1).
   constexpr bool packed = RECON != AXB_RECON_MP5;
   if (!packed) {
-    const dim3 grid((b.n[T0] + 2 + 31) / 32, (b.n[T1] + 2 + 3) / 4,
+    const dim3 grid((b.n[T0] + 2 * a.text + 31) / 32, (b.n[T1] + 2 * a.text + 3) / 4,
                     (b.n[dir] + seglen - 1) / seglen);
     if (dir == 1)
       k_flux_pass<1, RECON, EOS><<<grid, block, 0, s>>>(a, eos, seglen);
@@ -43,7 +43,7 @@ int launch_flux_pass_eos(int dir, const RhsArgs &a, const EOS &eos, int seglen,
   // not leave most of a warp idle
   RhsArgs ap = a;
   ap.b.packed = 1;
-  const long long plane = (long long)(b.n[T0] + 2) * (b.n[T1] + 2);
+  const long long plane = (long long)(b.n[T0] + 2 * a.text) * (b.n[T1] + 2 * a.text);
   const dim3 grid(unsigned((plane + 127) / 128), 1, (b.n[dir] + seglen - 1) / seglen);
   if (dir == 1)
     k_flux_pass<1, RECON, EOS><<<grid, block, 0, s>>>(ap, eos, seglen);

@@ -38,6 +38,16 @@ struct RhsArgs {
   double *acc[NHYDRO];
   double *rhs[NHYDRO];
   double *bflux[6]; // fxBy fxBz fyBx fyBz fzBx fzBy
+  // upwind CT face data (fluxes.cxx:776-794), per face direction d:
+  // uct[4d] = vtilde^{d+1}, uct[4d+1] = vtilde^{d+2} (upwind-averaged),
+  // uct[4d+2] = amax, uct[4d+3] = amin; written when use_uct
+  double *uct[12];
+  int use_uct;
+  // transverse ghost layers the flux passes cover: 1 (the edge field of
+  // flux CT needs one), 3 with upwind CT (its reconstructions to the edges
+  // reach three faces out)
+  int text;
+  int recon_method; // reconstruction of the upwind-CT edge values
   double *aux[7];   // Fx Fy Fz Fbetax Fbetay Fbetaz G
   double *Arhs[3], *Psi_rhs;
   // The stage update fused into the group (axb_substep): with fuse_stage
@@ -155,6 +165,7 @@ enum { R_RHO = 0, R_ENT, R_YE, R_PRESS, R_VX, R_VY, R_VZ, R_B1, R_B2, NREC };
 struct SideOut {
   double U[10], F[10]; // conserved and flux: dens momx momy momz tau DYe DEnt Bx By Bz
   double lam_p, lam_m; // the two distinct fast speeds of this side
+  double vt1, vt2;     // vtilde^{dir+1}, vtilde^{dir+2} (upwind CT)
 };
 
 // Per-side physics of CalcFlux (fluxes.cxx:357-654).
@@ -222,6 +233,8 @@ AXB_D void side_physics(const FaceMetric &m, const double *r, double Bdir,
   double vt[3];
   for (int i = 0; i < 3; ++i)
     vt[i] = m.alp * vel[i] - m.beta[i];
+  o.vt1 = vt[D1];
+  o.vt2 = vt[D2];
   const double alp_b0 = W * dot3(B, vlow);
   double Blow[3];
   lower3(m.g, B, Blow);

@@ -113,6 +113,15 @@ AXB_D void face_fluxes(const RhsArgs &a, const EOS &eos,
     a.bflux[2 * DIR + 0][I] = F[7 + BLO];
     a.bflux[2 * DIR + 1][I] = F[7 + BHI];
   }
+  if (a.use_uct) {
+    // upwind-CT face data (fluxes.cxx:776-794): the bounding speeds and the
+    // transverse vtilde averaged with them
+    const double amax = cmax, amin = -cmin;
+    a.uct[4 * DIR + 0][I] = (amax * sL.vt1 + amin * sR.vt1) / (amax + amin);
+    a.uct[4 * DIR + 1][I] = (amax * sL.vt2 + amin * sR.vt2) / (amax + amin);
+    a.uct[4 * DIR + 2][I] = amax;
+    a.uct[4 * DIR + 3][I] = amin;
+  }
 }
 
 // Fold F(face c+1) - F(face c) into the partial divergence of cell c (at I),
@@ -193,20 +202,21 @@ AXB_D void flux_pass_body(const RhsArgs &a, const EOS &eos, const int &seglen, c
   constexpr int T1 = (DIR == 2) ? 1 : 2;
   const BoxDev &b = a.b;
   const int ng = b.ng;
+  const int te = a.text;
   int t0, t1;
   bool active;
   if (b.packed) {
     // (batched small boxes) the block's threads walk the transverse plane
-    // [ng-1, ng+n]^2 row after row, so short rows leave no lane idle
-    const int w0 = b.n[T0] + 2;
+    // [ng-te, ng+n+te-1]^2 row after row, so short rows leave no lane idle
+    const int w0 = b.n[T0] + 2 * te;
     const int flat = bid.x * (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x;
-    t0 = ng - 1 + flat % w0;
-    t1 = ng - 1 + flat / w0;
-    active = flat < w0 * (b.n[T1] + 2);
+    t0 = ng - te + flat % w0;
+    t1 = ng - te + flat / w0;
+    active = flat < w0 * (b.n[T1] + 2 * te);
   } else {
-    t0 = ng - 1 + bid.x * blockDim.x + threadIdx.x;
-    t1 = ng - 1 + bid.y * blockDim.y + threadIdx.y;
-    active = (t0 <= ng + b.n[T0]) && (t1 <= ng + b.n[T1]);
+    t0 = ng - te + bid.x * blockDim.x + threadIdx.x;
+    t1 = ng - te + bid.y * blockDim.y + threadIdx.y;
+    active = (t0 <= ng + b.n[T0] + te - 1) && (t1 <= ng + b.n[T1] + te - 1);
   }
   double smax = 0.0;
   bool bad = false, bad_rhs = false;
@@ -335,13 +345,14 @@ AXB_D void flux_x_body(const RhsArgs &a, const EOS &eos, const uint3 bid) {
   const int ng = b.ng;
   const int lane = threadIdx.x & 31;
   const int warp = (bid.x * blockDim.x + threadIdx.x) >> 5;
-  const int ny = b.n[1] + 2; // rows j, k in [ng-1, ng+n]
-  const int nz = b.n[2] + 2;
+  const int te = a.text;
+  const int ny = b.n[1] + 2 * te; // rows j, k in [ng-te, ng+n+te-1]
+  const int nz = b.n[2] + 2 * te;
   double smax = 0.0;
   bool bad = false;
   if (warp < ny * nz) { // warp-uniform
-    const int j = ng - 1 + warp % ny;
-    const int k = ng - 1 + warp / ny;
+    const int j = ng - te + warp % ny;
+    const int k = ng - te + warp / ny;
     const bool trans_int = (j >= ng) && (j < ng + b.n[1]) && (k >= ng) && (k < ng + b.n[2]);
     const double *const fld[NREC] = {a.rho,     a.entropy, a.Ye,      a.thermo, a.recv[0],
                                      a.recv[1], a.recv[2], a.Bvec[1], a.Bvec[2]};

@@ -349,6 +349,49 @@ __global__ void __launch_bounds__(128)
 // stored face B fluxes, rhs.cxx:171-185), and the vertex gets Psi_rhs
 // (rhs.cxx:227-252).
 // ---------------------------------------------------------------------------
+// Upwind-CT edge electric field (AsterX_RHS with use_uct, rhs.cxx:124-168)
+// of the e-edge at I: the staggered B and the upwind-averaged vtilde of the
+// two adjacent face sets, reconstructed to the edge along the other
+// transverse direction (ReconX reconstruct with the cell-centred press and
+// velocity, not rho), weighted by the bounding speeds of the faces.
+template <int RECON>
+AXB_D double uct_edge_E(const RhsArgs &a, long long I, int e) {
+  const BoxDev &b = a.b;
+  const int ej = (e + 1) % 3, ek = (e + 2) % 3;
+  // the interface values at I along d: upper value of the cell at I - s
+  // (left) and lower value of the cell at I (right)
+  auto rc = [&](const double *f, int d, double &L, double &R) {
+    const long long s = b.stride(d);
+    double q[5], pr[5], vd[5];
+    load_pencil<5>(f, I - s, s, q);
+    load_pencil<5>(a.press, I - s, s, pr);
+    load_pencil<5>(a.vel[d], I - s, s, vd);
+    L = recon_cell<RECON>(q, pr, vd, false, a.rp).up;
+    load_pencil<5>(f, I, s, q);
+    load_pencil<5>(a.press, I, s, pr);
+    load_pencil<5>(a.vel[d], I, s, vd);
+    R = recon_cell<RECON>(q, pr, vd, false, a.rp).lo;
+  };
+  // one: B and vtilde^{ek} on the ej-faces, along ek, speeds of the ek-face
+  double B1L, B1R, v1L, v1R;
+  rc(a.dBstag[ej], ek, B1L, B1R);
+  rc(a.uct[4 * ej + 0], ek, v1L, v1R);
+  const double amax1 = a.uct[4 * ek + 2][I], amin1 = a.uct[4 * ek + 3][I];
+  // two: B and vtilde^{ej} on the ek-faces, along ej, speeds of the ej-face
+  double B2L, B2R, v2L, v2R;
+  rc(a.dBstag[ek], ej, B2L, B2R);
+  rc(a.uct[4 * ek + 1], ej, v2L, v2R);
+  const double amax2 = a.uct[4 * ej + 2][I], amin2 = a.uct[4 * ej + 3][I];
+  double E = (amax1 * v1L * B1L + amin1 * v1R * B1R - amax1 * amin1 * (B1R - B1L)) /
+             (amax1 + amin1);
+  E -= (amax2 * v2L * B2L + amin2 * v2R * B2R - amax2 * amin2 * (B2R - B2L)) /
+       (amax2 + amin2);
+  return E;
+}
+
+// UCT_RECON < 0: flux-CT edge field; otherwise upwind CT with that
+// reconstruction.
+template <int UCT_RECON>
 AXB_D void ct_psi_body(const RhsArgs &a, const uint3 bid) {
   const BoxDev &b = a.b;
   const int ng = b.ng;
@@ -364,21 +407,25 @@ AXB_D void ct_psi_body(const RhsArgs &a, const uint3 bid) {
   for (int e = 0; e < 3; ++e) {
     if (ijk[e] >= ng + b.n[e])
       continue;
-    const int ej = (e + 1) % 3, ek = (e + 2) % 3;
-    // fBs(j)(k): flux along k of B_j; fBs(k)(j): flux along j of B_k
-    const double *fjk, *fkj;
-    if (e == 0) {
-      fjk = a.bflux[5]; // fzBy
-      fkj = a.bflux[3]; // fyBz
-    } else if (e == 1) {
-      fjk = a.bflux[1]; // fxBz
-      fkj = a.bflux[4]; // fzBx
+    double E;
+    if constexpr (UCT_RECON >= 0) {
+      E = uct_edge_E<UCT_RECON>(a, I, e);
     } else {
-      fjk = a.bflux[2]; // fyBx
-      fkj = a.bflux[0]; // fxBy
+      const int ej = (e + 1) % 3, ek = (e + 2) % 3;
+      // fBs(j)(k): flux along k of B_j; fBs(k)(j): flux along j of B_k
+      const double *fjk, *fkj;
+      if (e == 0) {
+        fjk = a.bflux[5]; // fzBy
+        fkj = a.bflux[3]; // fyBz
+      } else if (e == 1) {
+        fjk = a.bflux[1]; // fxBz
+        fkj = a.bflux[4]; // fzBx
+      } else {
+        fjk = a.bflux[2]; // fyBx
+        fkj = a.bflux[0]; // fxBy
+      }
+      E = 0.25 * ((fjk[I] + fjk[I - b.stride(ej)]) - (fkj[I] + fkj[I - b.stride(ek)]));
     }
-    const double E = 0.25 * ((fjk[I] + fjk[I - b.stride(ej)]) -
-                             (fkj[I] + fkj[I - b.stride(ek)]));
     double r = -E;
     if (gl)
       r = -E - (G[I + b.stride(e)] - G[I]) / b.dx[e];
@@ -416,7 +463,12 @@ AXB_D void ct_psi_body(const RhsArgs &a, const uint3 bid) {
 }
 __global__ void __launch_bounds__(128)
     k_ct_psi(const RhsArgs a) {
-  ct_psi_body(a, blockIdx);
+  ct_psi_body<-1>(a, blockIdx);
+}
+template <int RECON>
+__global__ void __launch_bounds__(128)
+    k_ct_psi_uct(const RhsArgs a) {
+  ct_psi_body<RECON>(a, blockIdx);
 }
 
 } // namespace axb

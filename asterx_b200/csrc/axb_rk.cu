@@ -150,9 +150,15 @@ int centring_of(int gf, int c[3]) {
   case AXB_GF_Avec_x: case AXB_GF_Avec_x_rhs: c[1] = c[2] = 0; break;
   case AXB_GF_Avec_y: case AXB_GF_Avec_y_rhs: c[0] = c[2] = 0; break;
   case AXB_GF_Avec_z: case AXB_GF_Avec_z_rhs: c[0] = c[1] = 0; break;
-  case AXB_GF_dBx_stag: case AXB_GF_fxBy: case AXB_GF_fxBz: c[0] = 0; break;
-  case AXB_GF_dBy_stag: case AXB_GF_fyBx: case AXB_GF_fyBz: c[1] = 0; break;
-  case AXB_GF_dBz_stag: case AXB_GF_fzBx: case AXB_GF_fzBy: c[2] = 0; break;
+  case AXB_GF_dBx_stag: case AXB_GF_fxBy: case AXB_GF_fxBz:
+  case AXB_GF_vtilde_y_xface: case AXB_GF_vtilde_z_xface:
+  case AXB_GF_amax_xface: case AXB_GF_amin_xface: c[0] = 0; break;
+  case AXB_GF_dBy_stag: case AXB_GF_fyBx: case AXB_GF_fyBz:
+  case AXB_GF_vtilde_z_yface: case AXB_GF_vtilde_x_yface:
+  case AXB_GF_amax_yface: case AXB_GF_amin_yface: c[1] = 0; break;
+  case AXB_GF_dBz_stag: case AXB_GF_fzBx: case AXB_GF_fzBy:
+  case AXB_GF_vtilde_x_zface: case AXB_GF_vtilde_y_zface:
+  case AXB_GF_amax_zface: case AXB_GF_amin_zface: c[2] = 0; break;
   default:
     if ((gf >= AXB_GF_gxx && gf <= AXB_GF_kzz) || gf == AXB_GF_Psi ||
         gf == AXB_GF_Psi_rhs || (gf >= AXB_GF_Fx && gf <= AXB_GF_G))

@@ -193,6 +193,7 @@ CENTRING = {"Avec_x": (1, 0, 0), "Avec_y": (0, 1, 0), "Avec_z": (0, 0, 1), "Psi"
 for _g in ("gxx", "gxy", "gxz", "gyy", "gyz", "gzz", "alp", "betax", "betay", "betaz",
            "kxx", "kxy", "kxz", "kyy", "kyz", "kzz"):
     CENTRING[_g] = (0, 0, 0)
+CENTRING.update(abi.UCT_CENT)
 
 
 def one_d_initial(case, ng=None, ye=0.5):
@@ -256,6 +257,127 @@ def one_d_initial(case, ng=None, ye=0.5):
     for n in abi.GF_NAMES:
         f.setdefault(n, L.zeros())
     return L, f
+
+
+# The reference's 2-D regression tests (AsterX/test/<name>.par): AsterSeeds'
+# 2DTest cases (AsterSeeds/src/2D_tests.cxx:33-190) on a box two cells thick
+# in z, Neumann boundaries, RK4, dt = dtfac * the smallest spacing, and the
+# settings the hot path reads (the rest are the param.ccl defaults).
+TWO_D_TESTS = {
+    "Magnetic_rotor": dict(
+        test="magnetic rotor", recon="ppm", flux="hlle", n=(40, 40, 2), ng=3,
+        xmin=(-0.5, -0.5, -0.004), xmax=(0.5, 0.5, 0.004), bc="neumann",
+        gamma=1.66666666666667, c2p=("noble", "palenzuela"), c2p_tol=1e-8, max_iter=30,
+        rho_abs_min=1e-13, eps_min=1e-6, B_lim=100.0, vw_lim=10.0, Ye_lenient=0,
+        use_uct=0, recon_type=0, use_entropy_fix=0, dtfac=0.35, final_time=0.1,
+        method="rk4", out_every=20),
+    "Cylindrical_blast": dict(
+        test="cylindrical blast", recon="minmod", flux="hlle", n=(50, 50, 2), ng=2,
+        xmin=(-6.0, -6.0, -0.06), xmax=(6.0, 6.0, 0.06), bc="neumann",
+        gamma=1.3333333333, c2p=("noble", "palenzuela"), c2p_tol=1e-8, max_iter=1000,
+        rho_abs_min=1e-6, eps_min=1e-7, B_lim=1e8, vw_lim=1e8, Ye_lenient=1,
+        use_uct=1, recon_type=1, use_entropy_fix=1, dtfac=0.35, final_time=2.0,
+        method="rk4", out_every=20),
+}
+
+
+def two_d_layout(case, ng=None):
+    c = TWO_D_TESTS[case]
+    dx = tuple((hi - lo) / n for lo, hi, n in zip(c["xmin"], c["xmax"], c["n"]))
+    return Layout(tuple(c["n"]), c["ng"] if ng is None else ng, dx, tuple(c["xmin"]))
+
+
+def two_d_params(case):
+    c = TWO_D_TESTS[case]
+    prime, second = c["c2p"]
+    return abi.default_params(
+        reconstruction_method=c["recon"], flux_type=c["flux"], c2p_prime=prime,
+        c2p_second=second, c2p_tol=c["c2p_tol"], max_iter=c["max_iter"],
+        rho_abs_min=c["rho_abs_min"], B_lim=c["B_lim"], vw_lim=c["vw_lim"],
+        Ye_lenient=c["Ye_lenient"], poly_gamma=c["gamma"], use_uct=c["use_uct"],
+        recon_type=c["recon_type"], use_entropy_fix=c["use_entropy_fix"])
+
+
+def two_d_eos_kw(case):
+    c = TWO_D_TESTS[case]
+    return dict(gamma=c["gamma"], rho=(0.0, 1e8), eps=(c["eps_min"], 1e8), ye=(0.0, 1.0),
+                poly_gamma=c["gamma"], poly_k=100.0)
+
+
+def two_d_initial(case, ng=None, ye=0.5):
+    """Initial state of a 2-D test on the host: AsterSeeds' primitives on
+    every cell and vector potential on every edge (2D_tests.cxx:33-73 and
+    135-190: A_x = A_y = 0, A_z = a y with a = 1 for the rotor and 0.1 for
+    the blast), flat metric, then AsterX_InitialGroup as in one_d_initial."""
+    from . import workloads as W
+    c = TWO_D_TESTS[case]
+    L = two_d_layout(case, ng)
+    gamma = c["gamma"]
+    bc = (BC_NAMES[c["bc"]],) * 6
+    f: Dict[str, np.ndarray] = {}
+    W.flat_metric(L, f)
+    shape = L.view(L.zeros()).shape
+    x, y, _ = (np.broadcast_to(a, shape) for a in L.coords((1, 1, 1)))
+    r = np.sqrt(x * x + y * y)
+    zero = np.zeros(shape)
+    if c["test"] == "magnetic rotor":
+        inside = r < 0.1
+        omega = 9.95
+        rho = np.where(inside, 10.0, 1.0)
+        vx = np.where(inside, -omega * y, 0.0)
+        vy = np.where(inside, omega * x, 0.0)
+        press = np.ones(shape)
+        a_z = 1.0
+    else:
+        r_in, r_out, rho_in, rho_out, p_in, p_out = 0.8, 1.0, 1e-2, 1e-4, 1.0, 3.0e-5
+        with np.errstate(divide="ignore", invalid="ignore"):
+            rho_mid = np.exp(((r_out - r) * math.log(rho_in) + (r - r_in) * math.log(rho_out))
+                             / (r_out - r_in))
+            p_mid = np.exp(((r_out - r) * math.log(p_in) + (r - r_in) * math.log(p_out))
+                           / (r_out - r_in))
+        rho = np.where(r < r_in, rho_in, np.where(r > r_out, rho_out, rho_mid))
+        press = np.where(r < r_in, p_in, np.where(r > r_out, p_out, p_mid))
+        vx = vy = zero
+        a_z = 0.1
+    f["rho"] = rho.ravel().copy()
+    f["velx"] = np.asarray(vx).ravel().copy()
+    f["vely"] = np.asarray(vy).ravel().copy()
+    f["velz"] = zero.ravel().copy()
+    f["press"] = press.ravel().copy()
+    f["eps"] = f["press"] / ((gamma - 1.0) * f["rho"])
+    f["Ye"] = np.full(L.size, ye)
+    f["Avec_x"] = L.zeros()
+    f["Avec_y"] = L.zeros()
+    _, ye_z, _ = (np.broadcast_to(a, shape) for a in L.coords((0, 0, 1)))
+    f["Avec_z"] = (a_z * ye_z).ravel().copy()
+    f["Psi"] = L.zeros()
+    f["dBx_stag"], f["dBy_stag"], f["dBz_stag"] = W._curl_stag(L, f["Avec_x"], f["Avec_y"],
+                                                               f["Avec_z"])
+    fill_boundary_np(L, f, ["dBx_stag", "dBy_stag", "dBz_stag"], bc)
+    W._cell_B_from_stag(L, f)
+    fill_boundary_np(L, f, ["dBx", "dBy", "dBz", "Bvecx", "Bvecy", "Bvecz"], bc)
+    f["entropy"] = (gamma - 1.0) * f["eps"] * f["rho"] ** (1.0 - gamma)
+    f["temperature"] = (gamma - 1.0) * f["eps"]
+    W.saved_from_prims(f)
+    W.cons_from_prims(L, f)
+    fill_boundary_np(L, f, PRIMS + abi.SAVED + abi.CONS +
+                     ["zvec_x", "zvec_y", "zvec_z", "svec_x", "svec_y", "svec_z"], bc)
+    for n in abi.GF_NAMES:
+        f.setdefault(n, L.zeros())
+    return L, f
+
+
+def cut_at(L: Layout, f, name, axis, fixed):
+    """Values of `name` along `axis` (ghosts included) through the point whose
+    other two interior indices are `fixed` (the reference's TSV output)."""
+    v = L.view(f[name])
+    ax = "xyz".index(axis)
+    others = [d for d in range(3) if d != ax]
+    idx = [0, 0, 0]
+    for d, q in zip(others, fixed):
+        idx[d] = L.ng + int(q)
+    idx[ax] = slice(0, L.n[ax] + 2 * L.ng)
+    return np.asarray(v[idx[2], idx[1], idx[0]])
 
 
 # Runge-Kutta methods: per stage, the combination that forms the next state

@@ -86,7 +86,13 @@ typedef enum axb_status {
   X(fxBy) X(fxBz) X(fyBx) X(fyBz) X(fzBx) X(fzBy)                              \
   /* scratch: partial flux divergence of the 7 hydro variables */              \
   X(acc_dens) X(acc_momx) X(acc_momy) X(acc_momz) X(acc_tau) X(acc_DYe)        \
-  X(acc_DEnt)
+  X(acc_DEnt)                                                                  \
+  /* upwind CT face data (use_uct; AsterX/interface.ccl:135-165): the  */      \
+  /* transverse vtilde^i = alpha v^i - beta^i averaged with the bounding */    \
+  /* speeds, and those speeds amax, amin, per face direction */                \
+  X(vtilde_y_xface) X(vtilde_z_xface) X(vtilde_z_yface) X(vtilde_x_yface)      \
+  X(vtilde_x_zface) X(vtilde_y_zface) X(amax_xface) X(amin_xface)              \
+  X(amax_yface) X(amin_yface) X(amax_zface) X(amin_zface)
 
 typedef enum axb_gf {
 #define AXB_GF_ENUM_(name) AXB_GF_##name,

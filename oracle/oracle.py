@@ -134,16 +134,18 @@ class Oracle:
 
     def rhs_group(self):
         """AsterX_RHSGroup (AsterX/schedule.ccl:169-228): Fluxes, SourceTerms,
-        RHS, with the fluxes and auxiliaries widened onto ghost points."""
+        RHS, with the fluxes and auxiliaries widened onto ghost points (the
+        fluxes by three cell layers with upwind CT, whose edge
+        reconstructions reach three faces out)."""
         assert self.layout.ng >= 5
-        self.run("fluxes", ext_c=1, ext_v=2)
+        self.run("fluxes", ext_c=3 if self._params.use_uct else 1, ext_v=2)
         self.run("sources")
         self.run("rhs")
 
     def con2prim_group(self):
         """AsterX_Con2PrimGroup (AsterX/schedule.ccl:119-165): curl A on the
         interior faces widened by one transverse layer, centred dB, c2p."""
-        self.run("bstag", ext_c=1)
+        self.run("bstag", ext_c=3 if self._params.use_uct else 1)
         self.run("dB")
         self.run("c2p")
 

@@ -100,3 +100,22 @@ def test_max_char_speed_matches_reference(engine, ref, recon):
     got = engine.status()["max_speed"]
     assert want > 0.5
     assert abs(got - want) <= 1e-13 * want, (got, want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("recon,recon_type", [("ppm", 0), ("wenoz", 1), ("mp5", 1),
+                                              ("minmod", 0), ("monocentral", 1)])
+def test_rhs_upwind_ct(engine, ref, recon, recon_type):
+    """Upwind CT (use_uct, rhs.cxx:124-168): the face vtilde / amax / amin of
+    the flux passes (fluxes.cxx:776-794) and the edge field reconstructed
+    from the staggered B and vtilde of the adjacent faces, on a curved
+    magnetised box, against the reference build with its fluxes widened by
+    three layers."""
+    L, f = W.curved_box(n=12, ng=5, seed=13, wmax=3.0)
+    p = abi.default_params(reconstruction_method=recon, flux_type="hlle", use_uct=1,
+                           recon_type=recon_type)
+    host, gpu, st = run_both(engine, ref, L, f, p, 4.0 / 3.0)
+    assert st["error_word"] == 0
+    for n in RHS_OUT:
+        emax, el2 = errors(interior(L, n, gpu[n]), interior(L, n, host[n]))
+        assert emax <= TOL, (n, emax, el2)
