@@ -3,6 +3,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <vector>
 #include <limits>
 #include <new>
 
@@ -269,6 +270,82 @@ AXB_API int axb_eos_create_idealgas(double gamma, double particle_mass,
 // set up as at the end of init (:179-192), including the eps range of
 // compute_eps_range_full_table, which scans the EPS * (node count) block of
 // that interleaved array.
+namespace {
+// Unit factors of EOSX (EOSX/src/utils/eos_constants.hxx:7-14): CGS to the
+// code units (G = c = M_sun = 1) the evolution uses.
+constexpr double kLengthGF = 6.77269222552442e-06;
+constexpr double kTimeGF = 2.03040204956746e05;
+constexpr double kRhoGF = 1.61887093132742e-18;
+constexpr double kPressGF = 1.80123683248503e-39;
+constexpr double kEpsGF = 1.11265005605362e-21;
+constexpr int kNTables = 19;
+} // namespace
+
+// The conversions eos_3p_tabulated3d::init applies to a StellarCollapse
+// table once it has read it
+// (EOSX/src/eos_3p_tabulated3d/eos_3p_tabulated3d.hxx:115-177): the 19
+// datasets go from one array per variable (rho fastest) to variable-fastest
+// nodes, log10 of CGS values become natural logs of code-unit values, cs^2
+// and the derivatives get their unit factors, energy_shift becomes code
+// units.  Also the ranges init sets (:179-192): rho, temperature, Ye, eps.
+AXB_API int axb_eos_stellarcollapse_convert(int nrho, int ntemp, int nye,
+                                            const double *logrho10, const double *logtemp10,
+                                            const double *ye_in, const double *const *dsets,
+                                            double energy_shift_cgs, double *logrho,
+                                            double *logtemp, double *ye, double *table,
+                                            double *energy_shift, double ranges[8]) {
+  if (nrho < 2 || ntemp < 2 || nye < 2 || !logrho10 || !logtemp10 || !ye_in || !dsets ||
+      !logrho || !logtemp || !ye || !table || !energy_shift)
+    return AXB_ERR_ARG;
+  for (int v = 0; v < kNTables; ++v)
+    if (!dsets[v])
+      return AXB_ERR_ARG;
+  const size_t nodes = size_t(nrho) * ntemp * nye;
+  const double ln10 = std::log(10.0);
+  const double inv_time2 = 1 / (kTimeGF * kTimeGF);
+  *energy_shift = energy_shift_cgs * kEpsGF;
+  const double lrho = std::log(kRhoGF);
+  for (int q = 0; q < nrho; ++q)
+    logrho[q] = logrho10[q] * ln10 + lrho;
+  for (int q = 0; q < ntemp; ++q)
+    logtemp[q] = logtemp10[q] * ln10;
+  for (int q = 0; q < nye; ++q)
+    ye[q] = ye_in[q];
+  const double lpress = std::log(kPressGF), leps = std::log(kEpsGF);
+  for (size_t n = 0; n < nodes; ++n) {
+    double *t = table + kNTables * n;
+    for (int v = 0; v < kNTables; ++v)
+      t[v] = dsets[v][n];
+    t[0] = t[0] * ln10 + lpress;                              // ln press
+    t[1] = t[1] * ln10 + leps;                                // ln(eps + shift)
+    t[4] = t[4] * kLengthGF * kLengthGF * inv_time2;           // cs^2
+    t[5] = t[5] * kEpsGF;                                     // d eps / dT
+    t[6] = t[6] * kPressGF / kRhoGF;                          // dp/drho at eps
+    t[7] = t[7] * kPressGF / kEpsGF;                          // dp/deps at rho
+  }
+  if (ranges) {
+    ranges[0] = std::exp(logrho[0]);
+    ranges[1] = std::exp(logrho[nrho - 1]);
+    ranges[2] = std::exp(logtemp[0]);
+    ranges[3] = std::exp(logtemp[ntemp - 1]);
+    ranges[4] = ye[0];
+    ranges[5] = ye[nye - 1];
+    // compute_eps_range_full_table (eos_3p_tabulated3d.hxx:447-458): the
+    // extremes of exp(ln(eps + shift)) - shift over the table's nodes, with
+    // the table read in its variable-major order as the reference reads it
+    double emin = std::numeric_limits<double>::max();
+    double emax = std::numeric_limits<double>::lowest();
+    for (size_t n = 0; n < nodes; ++n) {
+      const double e = std::exp(table[1 * nodes + n]) - *energy_shift;
+      emin = std::fmin(emin, e);
+      emax = std::fmax(emax, e);
+    }
+    ranges[6] = std::fmax(emin, 1e-15);
+    ranges[7] = emax;
+  }
+  return AXB_OK;
+}
+
 AXB_API int axb_eos_create_tabulated3d(int nrho, int ntemp, int nye,
                                        const double *logrho, const double *logtemp,
                                        const double *ye, const double *table,
@@ -352,6 +429,34 @@ AXB_API int axb_eos_create_tabulated3d(int nrho, int ntemp, int nye,
   e->tab_dev = dptr;
   *out = e;
   return AXB_OK;
+}
+
+// A StellarCollapse table as its file holds it (the datasets' values, see
+// axb_eos_stellarcollapse_convert) to the device EOS: the conversion of
+// eos_3p_tabulated3d::init, then axb_eos_create_tabulated3d.
+AXB_API int axb_eos_create_stellarcollapse(int nrho, int ntemp, int nye,
+                                           const double *logrho10, const double *logtemp10,
+                                           const double *ye_in, const double *const *dsets,
+                                           double energy_shift_cgs, double poly_gamma,
+                                           double poly_k, axb_eos **out) {
+  if (!out || nrho < 2 || ntemp < 2 || nye < 2)
+    return AXB_ERR_ARG;
+  const size_t nodes = size_t(nrho) * ntemp * nye;
+  std::vector<double> lr(nrho), lt(ntemp), y(nye);
+  std::vector<double> table;
+  try {
+    table.resize(nodes * kNTables);
+  } catch (const std::bad_alloc &) {
+    return AXB_ERR_TOO_LARGE;
+  }
+  double shift = 0.0;
+  int rc = axb_eos_stellarcollapse_convert(nrho, ntemp, nye, logrho10, logtemp10, ye_in, dsets,
+                                           energy_shift_cgs, lr.data(), lt.data(), y.data(),
+                                           table.data(), &shift, nullptr);
+  if (rc)
+    return rc;
+  return axb_eos_create_tabulated3d(nrho, ntemp, nye, lr.data(), lt.data(), y.data(),
+                                    table.data(), shift, poly_gamma, poly_k, out);
 }
 
 AXB_API int axb_eos_destroy(axb_eos *e) {

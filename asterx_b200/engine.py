@@ -180,6 +180,20 @@ class Engine:
         self._eos.append(h)
         return h
 
+    def eos_stellarcollapse(self, datasets, poly_gamma=2.0, poly_k=100.0):
+        """Tabulated3d EOS from a StellarCollapse table's datasets as the
+        file holds them (eos_tables.read_stellarcollapse), converted as the
+        reference's reader converts them."""
+        from . import eos_tables as T
+        T.bind(self.lib)
+        (nrho, ntemp, nye), axes, sets, ptrs, shift = T._args(datasets)
+        h = _vp()
+        self._check(self.lib.axb_eos_create_stellarcollapse(
+            nrho, ntemp, nye, *[a.ctypes.data_as(_dp) for a in axes], ptrs, shift,
+            poly_gamma, poly_k, C.byref(h)), "axb_eos_create_stellarcollapse")
+        self._eos.append(h)
+        return h
+
     # -- memory ---------------------------------------------------------------
     def upload(self, layout: Layout, fields: dict, names=None):
         """Device copies (torch float64 tensors) of the given host arrays, plus

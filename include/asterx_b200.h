@@ -238,6 +238,36 @@ AXB_API int axb_eos_create_tabulated3d(int nrho, int ntemp, int nye,
                                        const double *ye, const double *table,
                                        double energy_shift, double poly_gamma,
                                        double poly_k, axb_eos **out);
+/* StellarCollapse tables (eos_3p_tabulated3d::init,
+ * EOSX/src/eos_3p_tabulated3d/eos_3p_tabulated3d.hxx:53-193), from the
+ * datasets the caller read from the HDF5 file (no HDF5 library is linked):
+ * logrho10[nrho], logtemp10[ntemp] (log10 of g/cm^3 and MeV), ye_in[nye],
+ * energy_shift_cgs (erg/g), and dsets[19] = "logpress", "logenergy",
+ * "entropy", "munu", "cs2", "dedt", "dpdrhoe", "dpderho", "muhat", "mu_e",
+ * "mu_p", "mu_n", "Xa", "Xh", "Xn", "Xp", "Abar", "Zbar", "gamma", each
+ * nrho*ntemp*nye values with rho fastest, as stored in the file.
+ *
+ * axb_eos_stellarcollapse_convert applies init's conversions
+ * (:115-177): natural logs in code units (EOSX/src/utils/
+ * eos_constants.hxx:7-14), cs^2 and the derivatives scaled, the 19
+ * variables interleaved per node -- the arguments of
+ * axb_eos_create_tabulated3d: logrho, logtemp, ye (nrho, ntemp, nye values),
+ * table (19 * nrho * ntemp * nye), energy_shift; and, if `ranges` is not
+ * NULL, the ranges init sets (:179-192): rho min/max, temperature min/max,
+ * Ye min/max, eps min/max.  Host only; allocates nothing.
+ * axb_eos_create_stellarcollapse converts and then calls
+ * axb_eos_create_tabulated3d. */
+AXB_API int axb_eos_stellarcollapse_convert(int nrho, int ntemp, int nye,
+                                            const double *logrho10, const double *logtemp10,
+                                            const double *ye_in, const double *const *dsets,
+                                            double energy_shift_cgs, double *logrho,
+                                            double *logtemp, double *ye, double *table,
+                                            double *energy_shift, double ranges[8]);
+AXB_API int axb_eos_create_stellarcollapse(int nrho, int ntemp, int nye,
+                                           const double *logrho10, const double *logtemp10,
+                                           const double *ye_in, const double *const *dsets,
+                                           double energy_shift_cgs, double poly_gamma,
+                                           double poly_k, axb_eos **out);
 AXB_API int axb_eos_destroy(axb_eos *eos);
 
 /* ------------------------------------------------------------------------ */

@@ -121,6 +121,33 @@ class Oracle:
                                                _ptr(lt), _ptr(y), _ptr(t),
                                                energy_shift, poly_gamma, poly_k))
 
+    def eos_stellarcollapse(self, datasets, poly_gamma=2.0, poly_k=100.0):
+        """The reference's own StellarCollapse reader (eos_3p_tabulated3d::init)
+        on `datasets` served by the stand-in HDF5; returns the converted
+        (logrho, logtemp, ye, table, energy_shift)."""
+        L = self.lib
+        L.ora_h5_clear()
+        L.ora_h5_put_double.argtypes = [C.c_char_p, _dp, C.c_long]
+        L.ora_h5_put_int.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.c_long]
+        L.ora_eos_stellarcollapse.argtypes = [C.c_double, C.c_double]
+        L.ora_eos_tab_export.argtypes = [_dp] * 5
+        self._h5 = []
+        for k, v in datasets.items():
+            if k.startswith("points"):
+                a = np.array([int(v)], dtype=np.int32)
+                L.ora_h5_put_int(k.encode(), a.ctypes.data_as(C.POINTER(C.c_int)), 1)
+            else:
+                a = np.ascontiguousarray(v, dtype=np.float64).reshape(-1)
+                L.ora_h5_put_double(k.encode(), _ptr(a), a.size)
+            self._h5.append(a)
+        self._check(L.ora_eos_stellarcollapse(poly_gamma, poly_k))
+        nrho, ntemp, nye = (int(datasets[k]) for k in ("pointsrho", "pointstemp", "pointsye"))
+        lr, lt, y = np.empty(nrho), np.empty(ntemp), np.empty(nye)
+        table = np.empty(19 * nrho * ntemp * nye)
+        es = np.empty(1)
+        L.ora_eos_tab_export(_ptr(lr), _ptr(lt), _ptr(y), _ptr(table), _ptr(es))
+        return lr, lt, y, table, float(es[0])
+
     def tab_ranges(self):
         out = np.zeros(8)
         self.lib.ora_eos_tab_ranges(_ptr(out))

@@ -5,6 +5,7 @@
 // compare the oracle restatement and the CUDA kernels with the reference's
 // own code on the same inputs.  Built by oracle/build_oracle.py into
 // oracle/_ref/libaxref.so.
+#include <cstring>
 #include <cctk.h>
 #include <cctk_Arguments.h>
 #include <cctk_Parameters.h>
@@ -271,6 +272,54 @@ ORA_API int ora_eos_tabulated(int nrho, int ntemp, int nye,
     global_eos_1p_poly = &poly;
     axref_params.evolution_eos = "Tabulated3d";
   });
+}
+
+// The reference's StellarCollapse reader (eos_3p_tabulated3d::init,
+// EOSX/src/eos_3p_tabulated3d/eos_3p_tabulated3d.hxx:53-193) on datasets
+// registered in memory (the stand-in HDF5 of refshim/hdf5.h): ora_h5_clear,
+// ora_h5_put_* per dataset, then ora_eos_stellarcollapse, which makes the
+// result the EOS of the following routines; ora_eos_tab_export copies its
+// converted axes, table and energy shift out.
+ORA_API void ora_h5_clear() {
+  axref_h5_store().clear();
+  axref_h5_handles().clear();
+}
+ORA_API void ora_h5_put_double(const char *name, const double *v, long n) {
+  axref_h5_dset &d = axref_h5_store()[name];
+  d.is_int = false;
+  d.d.assign(v, v + n);
+}
+ORA_API void ora_h5_put_int(const char *name, const int *v, long n) {
+  axref_h5_dset &d = axref_h5_store()[name];
+  d.is_int = true;
+  d.i.assign(v, v + n);
+}
+ORA_API int ora_eos_stellarcollapse(double poly_gamma, double poly_k) {
+  using namespace EOSX;
+  return guarded([&] {
+    static eos_3p_tabulated3d tab;
+    static eos_1p_polytropic poly;
+    new (&poly) eos_1p_polytropic;
+    poly.init(poly_gamma, poly_k, 1.0);
+    new (&tab) eos_3p_tabulated3d;
+    tab.gamma = std::numeric_limits<double>::quiet_NaN(); // never set by init
+    eos_3p::range rgeps, rgrho, rgye;
+    tab.init("in-memory", rgeps, rgrho, rgye);
+    global_eos_3p_tab3d = &tab;
+    global_eos_1p_poly = &poly;
+    axref_params.evolution_eos = "Tabulated3d";
+  });
+}
+ORA_API void ora_eos_tab_export(double *logrho, double *logtemp, double *ye, double *table,
+                                double *energy_shift) {
+  auto *t = EOSX::global_eos_3p_tab3d;
+  auto *it = t->interptable;
+  const size_t n0 = it->num_points[0], n1 = it->num_points[1], n2 = it->num_points[2];
+  std::memcpy(logrho, it->x[0], n0 * sizeof(double));
+  std::memcpy(logtemp, it->x[1], n1 * sizeof(double));
+  std::memcpy(ye, it->x[2], n2 * sizeof(double));
+  std::memcpy(table, it->y, n0 * n1 * n2 * NTABLES * sizeof(double));
+  *energy_shift = *t->energy_shift;
 }
 
 ORA_API void ora_eos_tab_ranges(double *out8) {
