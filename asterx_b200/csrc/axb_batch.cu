@@ -270,7 +270,9 @@ AXB_API int axb_batch_create(axb_ctx *c, int nbox, const axb_box *boxes,
   if (!rc)
     rc = make_table(bx, g_c2p, 1, B->tab[P_C2P]);
   if (!rc)
-    rc = make_table(bx, g_sync, 1, B->tab[P_SYNC_P]);
+    rc = make_table(bx, g_sync,
+                    p->recon_type == AXB_RECVAR_Z || p->recon_type == AXB_RECVAR_S ? 2 : 1,
+                    B->tab[P_SYNC_P]);
   if (!rc && cudaMalloc(&B->ctr, NPHASE * sizeof(unsigned long long)) != cudaSuccess)
     rc = AXB_ERR_CUDA;
   if (!rc && c2p_batch_fast_ok(nbox, boxes, p) &&

@@ -82,9 +82,7 @@ enum RepStatus {
   REP_PREP_ROOT_FAIL_BRACKET,
   REP_NOT_SET,
   // (engine only) the fast pass left the cell to the full cascade
-  REP_DEFER,
-  // (engine only) the staged solve handed its bracket over (PAL_SETUP)
-  REP_PENDING
+  REP_DEFER
 };
 struct Report {
   int status = REP_NOT_SET;
@@ -547,9 +545,7 @@ AXB_HD void noble_solve(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
 
 // Brent's method as a resumable state: brent_init handles the bracket's
 // degenerate cases (a root at an end, no sign change), brent_step does one
-// iteration of the loop.  brent_bracket runs them to completion; the pooled
-// recovery pass runs one step at a time, so a lane whose cell converged can
-// take the next cell.  Both produce the same iterates and the same bits.
+// iteration of the loop; brent_bracket runs them to completion.
 struct BrentState {
   double a, b, c, d, fa, fb, fc;
   int iters;
@@ -684,8 +680,8 @@ struct PalQRST {
 // division, and P/rho comes from the EOS without a division (last-ulp
 // differences; the bracket search converges to the same tolerance).
 template <class EOS>
-AXB_HD double pal_froot_s(const EOS &eos, int use_temp, double atmo_eps, const PalQRST &k,
-                          double x, double dens) {
+AXB_HD double pal_froot(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
+                        const PalQRST &k, double x, const Cons &cv) {
   const double xs = x + k.s;
   const double ixxs = 1.0 / (x * xs); // 1/(x (x+s)); 1/x = (x+s)/(x (x+s))
   const double ix = xs * ixxs;
@@ -693,35 +689,16 @@ AXB_HD double pal_froot_s(const EOS &eos, int use_temp, double atmo_eps, const P
   Wminus2 = fmin(fmax(Wminus2, 1e-10), 1);
   const double W_loc = rsqrt(Wminus2);
   const double iW = Wminus2 * W_loc;
-  const double rho_loc = dens * iW;
+  const double rho_loc = cv.dens * iW;
   const double Ye_loc = k.ye;
   double eps_loc = W_loc - 1.0 + (1.0 - W_loc * W_loc) * x * iW +
                    W_loc * (k.q - k.s + 0.5 * k.t * k.t * (ix * ix) + 0.5 * k.s * Wminus2);
-  if (use_temp) {
-    eps_loc = fmax(eps_loc, atmo_eps);
+  if (cp.use_temp) {
+    eps_loc = fmax(eps_loc, atmo.eps);
     eps_loc = fmin(eps_loc, eos.rgeps.max);
   }
   return (x - (1.0 + eps_loc + eos.press_over_rho(rho_loc, eps_loc, Ye_loc)) * W_loc);
 }
-template <class EOS>
-AXB_HD double pal_froot(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
-                        const PalQRST &k, double x, const Cons &cv) {
-  return pal_froot_s(eos, cp.use_temp, atmo.eps, k, x, cv.dens);
-}
-
-// The Palenzuela solve in stages (the pooled recovery pass): PAL_SETUP stops
-// once the bracket and its end values are known and hands them over
-// (status REP_PENDING); PAL_FINISH takes the finished bracket and its
-// iteration count instead of running the root finder.  PAL_ALL is the solve
-// in one piece.
-enum { PAL_ALL = 0, PAL_SETUP = 1, PAL_FINISH = 2 };
-struct PalHandoff {
-  PalQRST k;
-  double dens, atmo_eps;
-  double a, b, fa, fb; // PAL_SETUP out
-  double lo, hi;       // PAL_FINISH in
-  int iters;           // PAL_FINISH in
-};
 
 // Palenzuela 1D (c2p_1DPalenzuela::solve, c2p_1DPalenzuela.hxx:306-556).
 // `xlo`/`xhi` > 0 narrow the initial bracket (learned initial guess); the
@@ -729,13 +706,10 @@ struct PalHandoff {
 // FAST: the common path only -- every failure, and a bracket that did not
 // converge (which needs the conservative-variable check), returns REP_DEFER
 // before anything else, so the caller can hand the cell to the full cascade.
-// STAGE / `h`: see PalHandoff (the staged form is only used with FAST).
-template <class EOS, bool FAST = false, int STAGE = PAL_ALL>
+template <class EOS, bool FAST = false>
 AXB_HD void palenzuela_solve(const EOS &eos, const C2PParams &cp, const Atmo &atmo,
                              Prim &pv, Cons &cv, const sym3 &glo, Report &rep,
-                             double xlo = -1.0, double xhi = -1.0,
-                             PalHandoff *h = nullptr) {
-  static_assert(STAGE == PAL_ALL || FAST, "the staged solve is the fast path's");
+                             double xlo = -1.0, double xhi = -1.0) {
   rep.iters = 0;
   rep.adjust_cons = false;
   rep.set_atmo = false;
@@ -800,46 +774,28 @@ AXB_HD void palenzuela_solve(const EOS &eos, const C2PParams &cp, const Atmo &at
   double a = fmax(1e-10, 1.0 + qP - sP);
   double b = 2.0 + 2.0 * qP - sP;
   auto fn = [&](double x) { return pal_froot(eos, cp, atmo, k, x, cv); };
-  double r0, r1;
-  if constexpr (STAGE == PAL_FINISH) {
-    r0 = h->lo;
-    r1 = h->hi;
-    rep.iters = h->iters;
-  } else {
-    bool narrowed = false;
-    double fa = 0.0, fb = 0.0;
-    if (xlo > 0.0 && xhi > xlo) {
-      const double flo = fn(xlo), fhi = fn(xhi);
-      if (flo * fhi < 0) {
-        a = xlo;
-        b = xhi;
-        fa = flo;
-        fb = fhi;
-        narrowed = true;
-      }
-    }
-    if (!narrowed) {
-      fa = fn(a);
-      fb = fn(b);
-      if (fa * fb > 0) {
-        b = 3.0 + 3.0 * qP - 1.5 * sP;
-        fb = fn(b);
-      }
-    }
-    if constexpr (STAGE == PAL_SETUP) {
-      h->k = k;
-      h->dens = cv.dens;
-      h->atmo_eps = atmo.eps;
-      h->a = a;
-      h->b = b;
-      h->fa = fa;
-      h->fb = fb;
-      rep.status = REP_PENDING;
-      return;
-    } else {
-      brent_bracket(fn, a, b, fa, fb, cp.minbits, cp.maxIter, rep.iters, r0, r1);
+  bool narrowed = false;
+  double fa = 0.0, fb = 0.0;
+  if (xlo > 0.0 && xhi > xlo) {
+    const double flo = fn(xlo), fhi = fn(xhi);
+    if (flo * fhi < 0) {
+      a = xlo;
+      b = xhi;
+      fa = flo;
+      fb = fhi;
+      narrowed = true;
     }
   }
+  if (!narrowed) {
+    fa = fn(a);
+    fb = fn(b);
+    if (fa * fb > 0) {
+      b = 3.0 + 3.0 * qP - 1.5 * sP;
+      fb = fn(b);
+    }
+  }
+  double r0, r1;
+  brent_bracket(fn, a, b, fa, fb, cp.minbits, cp.maxIter, rep.iters, r0, r1);
   const bool converged = !(fabs(r0 - r1) > cp.tolerance_0 * fmin(fabs(r0), fabs(r1)));
   if constexpr (FAST) {
     if (!converged) {

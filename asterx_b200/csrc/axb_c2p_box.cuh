@@ -168,18 +168,12 @@ AXB_D int after_both_failed(const EOS &eos, const C2PBoxArgs &a, const Atmo &atm
 // same unmodified inputs, so every cell gets exactly the full cascade's
 // result.  The rare paths' code stays out of the fast kernel and no warp of
 // it waits on them.
-//
-// MODES C2P_SETUP and C2P_FINISH split the fast path around the Palenzuela
-// root finder for the pooled pass (k_c2p_pool): SETUP stops once the
-// bracket is known and hands it over through `h` (returns C2P_PENDING);
-// FINISH recomputes the same set-up from the same inputs, takes the finished
-// bracket from `h` and completes the cell exactly as the fast path does.
-enum { C2P_FULL = 0, C2P_FAST = 1, C2P_SETUP = 2, C2P_FINISH = 3 };
-enum { C2P_DONE = 0, C2P_DEFERRED = 1, C2P_PENDING = 2 };
+enum { C2P_FULL = 0, C2P_FAST = 1 };
+enum { C2P_DONE = 0, C2P_DEFERRED = 1 };
 template <class EOS, int MODE>
 AXB_D int c2p_cell(const C2PBoxArgs &a, const EOS &eos, const int i, const int j,
-                   const int k, int &iters_first, bool &failed, PalHandoff *h = nullptr) {
-  constexpr bool FASTLIKE = MODE != C2P_FULL;
+                   const int k, int &iters_first, bool &failed) {
+  constexpr bool FASTLIKE = MODE == C2P_FAST;
   const BoxDev &b = a.b;
   {
     const long long I = b.at(i, j, k);
@@ -289,17 +283,7 @@ AXB_D int c2p_cell(const C2PBoxArgs &a, const EOS &eos, const int i, const int j
       if (call_c2p) {
         Report r1;
         code = AXB_C2P_PRIME;
-        if constexpr (MODE == C2P_FAST) {
-          palenzuela_solve<EOS, true>(eos, a.cp, atmo, pv, cv, glo, r1);
-        } else if constexpr (MODE == C2P_SETUP) {
-          palenzuela_solve<EOS, true, PAL_SETUP>(eos, a.cp, atmo, pv, cv, glo, r1, -1.0, -1.0,
-                                                 h);
-          if (r1.status == REP_PENDING)
-            return C2P_PENDING;
-        } else {
-          palenzuela_solve<EOS, true, PAL_FINISH>(eos, a.cp, atmo, pv, cv, glo, r1, -1.0,
-                                                  -1.0, h);
-        }
+        palenzuela_solve<EOS, true>(eos, a.cp, atmo, pv, cv, glo, r1);
         if (r1.failed())
           return C2P_DEFERRED; // REP_DEFER: every failure goes to the full cascade
         iters_first = r1.iters;
@@ -448,183 +432,6 @@ AXB_D void c2p_fast_body(const C2PBoxArgs &a, const EOS &eos, const uint3 bid, i
   c2p_epilogue(a, s_hist, iters_first, failed);
 }
 
-// ---------------------------------------------------------------------------
-// Pooled fast pass (k_c2p_pool): the fast path of a tile of C2P_POOL_TILE
-// cells (one (i, j) plane, flat order) in three phases, so that no lane idles
-// while a slower cell of its warp iterates.
-//   A  every thread sets up C2P_POOL_CPT cells up to the Palenzuela bracket
-//      (C2P_SETUP) and leaves the root finder's inputs in shared memory; the
-//      atmosphere cells are finished here, deferred cells queued;
-//   B  the block's lanes draw pending cells from a shared counter and run
-//      Brent one step at a time; a lane whose cell converged stores the
-//      bracket and draws the next cell;
-//   C  every thread finishes its cells from the stored brackets (C2P_FINISH,
-//      the set-up recomputed from the same inputs) and writes them.
-// Every cell takes the same Brent iterates as in k_c2p_fast, so both give the
-// same bits.
-// ---------------------------------------------------------------------------
-#ifndef AXB_C2P_POOL_CPT
-#define AXB_C2P_POOL_CPT 4 // cells per thread of a tile
-#endif
-#ifndef AXB_C2P_POOL_MINB
-#define AXB_C2P_POOL_MINB 4 // resident CTAs per SM the register budget must allow
-#endif
-constexpr int C2P_POOL_T = 128;
-constexpr int C2P_POOL_TILE = C2P_POOL_T * AXB_C2P_POOL_CPT;
-// root-finder inputs per pending cell: bracket, end values, the invariants,
-// dens and the atmosphere's eps (slots 0, 1 receive the final bracket)
-enum { PX_A = 0, PX_B, PX_FA, PX_FB, PX_Q, PX_R, PX_S, PX_T, PX_YE, PX_DENS, PX_AEPS, PX_N };
-
-template <class EOS>
-AXB_D void c2p_pool_body(const C2PBoxArgs &a, const EOS &eos, const uint3 bid, int box,
-                         const C2PQueue &q) {
-  __shared__ unsigned int s_hist[64];
-  __shared__ double s_ctx[PX_N][C2P_POOL_TILE];
-  __shared__ unsigned short s_pend[C2P_POOL_TILE];
-  __shared__ unsigned short s_iters[C2P_POOL_TILE];
-  __shared__ unsigned char s_state[C2P_POOL_TILE];
-  __shared__ int s_npend, s_next;
-  c2p_hist_init(a, s_hist);
-  if (threadIdx.x == 0) {
-    s_npend = 0;
-    s_next = 0;
-  }
-  __syncthreads();
-  const BoxDev &b = a.b;
-  const int n0 = b.n[0];
-  const long long nplane = (long long)n0 * b.n[1];
-  const int k = b.ng + bid.z;
-  const long long base = (long long)bid.x * C2P_POOL_TILE;
-  const int lane = threadIdx.x & 31;
-  constexpr unsigned FULL = 0xffffffffu;
-
-  // phase A
-  for (int m = 0; m < AXB_C2P_POOL_CPT; ++m) {
-    const int slot = threadIdx.x + C2P_POOL_T * m;
-    const long long f = base + slot;
-    int st = C2P_DONE, i = 0, j = 0, iters = -1;
-    bool failed = false;
-    PalHandoff h;
-    if (f < nplane) {
-      i = b.ng + int(f % n0);
-      j = b.ng + int(f / n0);
-      st = c2p_cell<EOS, C2P_SETUP>(a, eos, i, j, k, iters, failed, &h);
-    }
-    s_state[slot] = (unsigned char)st;
-    if (st == C2P_PENDING) {
-      s_ctx[PX_A][slot] = h.a;
-      s_ctx[PX_B][slot] = h.b;
-      s_ctx[PX_FA][slot] = h.fa;
-      s_ctx[PX_FB][slot] = h.fb;
-      s_ctx[PX_Q][slot] = h.k.q;
-      s_ctx[PX_R][slot] = h.k.r;
-      s_ctx[PX_S][slot] = h.k.s;
-      s_ctx[PX_T][slot] = h.k.t;
-      s_ctx[PX_YE][slot] = h.k.ye;
-      s_ctx[PX_DENS][slot] = h.dens;
-      s_ctx[PX_AEPS][slot] = h.atmo_eps;
-    }
-    const unsigned mp = __ballot_sync(FULL, st == C2P_PENDING);
-    if (mp) {
-      const int leader = __ffs(mp) - 1;
-      int pb = 0;
-      if (lane == leader)
-        pb = atomicAdd(&s_npend, __popc(mp));
-      pb = __shfl_sync(FULL, pb, leader);
-      if (st == C2P_PENDING)
-        s_pend[pb + __popc(mp & ((1u << lane) - 1u))] = (unsigned short)slot;
-    }
-    queue_deferred(q, st == C2P_DEFERRED, i, j, k, box);
-  }
-  __syncthreads();
-
-  // phase B
-  {
-    const double eps = ldexp(1.0, -a.cp.minbits);
-    const int maxit = a.cp.maxIter;
-    const int use_temp = a.cp.use_temp;
-    const int npend = s_npend;
-    int slot = -1;
-    bool exhausted = false;
-    BrentState st;
-    PalQRST kk;
-    double dens = 0.0, aeps = 0.0;
-    while (true) {
-      const bool need = slot < 0 && !exhausted;
-      const unsigned mn = __ballot_sync(FULL, need);
-      if (mn) {
-        const int leader = __ffs(mn) - 1;
-        int nb = 0;
-        if (lane == leader)
-          nb = atomicAdd(&s_next, __popc(mn));
-        nb = __shfl_sync(FULL, nb, leader);
-        if (need) {
-          const int e = nb + __popc(mn & ((1u << lane) - 1u));
-          if (e < npend) {
-            slot = s_pend[e];
-            kk.q = s_ctx[PX_Q][slot];
-            kk.r = s_ctx[PX_R][slot];
-            kk.s = s_ctx[PX_S][slot];
-            kk.t = s_ctx[PX_T][slot];
-            kk.ye = s_ctx[PX_YE][slot];
-            dens = s_ctx[PX_DENS][slot];
-            aeps = s_ctx[PX_AEPS][slot];
-            double lo, hi;
-            if (brent_init(st, s_ctx[PX_A][slot], s_ctx[PX_B][slot], s_ctx[PX_FA][slot],
-                           s_ctx[PX_FB][slot], lo, hi)) {
-              s_ctx[PX_A][slot] = lo;
-              s_ctx[PX_B][slot] = hi;
-              s_iters[slot] = 0;
-              slot = -1;
-            }
-          } else {
-            exhausted = true;
-          }
-        }
-      }
-      if (slot >= 0) {
-        auto fn = [&](double x) { return pal_froot_s(eos, use_temp, aeps, kk, x, dens); };
-        double lo, hi;
-        if (brent_step(st, fn, eps, maxit, lo, hi)) {
-          s_ctx[PX_A][slot] = lo;
-          s_ctx[PX_B][slot] = hi;
-          s_iters[slot] = (unsigned short)min(st.iters, 65535);
-          slot = -1;
-        }
-      }
-      if (!__any_sync(FULL, slot >= 0 || !exhausted))
-        break;
-    }
-  }
-  __syncthreads();
-
-  // phase C
-  for (int m = 0; m < AXB_C2P_POOL_CPT; ++m) {
-    const int slot = threadIdx.x + C2P_POOL_T * m;
-    const long long f = base + slot;
-    int i = 0, j = 0, iters = -1;
-    bool failed = false, defer = false;
-    if (f < nplane && s_state[slot] == C2P_PENDING) {
-      i = b.ng + int(f % n0);
-      j = b.ng + int(f / n0);
-      PalHandoff h;
-      h.lo = s_ctx[PX_A][slot];
-      h.hi = s_ctx[PX_B][slot];
-      h.iters = s_iters[slot];
-      defer = c2p_cell<EOS, C2P_FINISH>(a, eos, i, j, k, iters, failed, &h) == C2P_DEFERRED;
-    }
-    queue_deferred(q, defer, i, j, k, box);
-    if (a.want_hist && iters >= 0)
-      atomicAdd(&s_hist[min(iters, 63)], 1u);
-  }
-  if (a.want_hist) {
-    __syncthreads();
-    for (int t = threadIdx.x; t < 64; t += blockDim.x)
-      if (s_hist[t])
-        atomicAdd(&a.status->c2p_iter_hist[t], (unsigned long long)s_hist[t]);
-  }
-}
-
 // The full cascade over the queued cells; `args_of(box)` gives the box's
 // argument block.  Every thread runs the same number of rounds, so the
 // warp-level epilogue sees full warps.
@@ -671,12 +478,6 @@ template <class EOS>
 __global__ void __launch_bounds__(128, AXB_C2P_FAST_MINB)
     k_c2p_fast(const C2PBoxArgs a, const EOS eos, const C2PQueue q) {
   c2p_fast_body<EOS>(a, eos, blockIdx, 0, q);
-}
-
-template <class EOS>
-__global__ void __launch_bounds__(C2P_POOL_T, AXB_C2P_POOL_MINB)
-    k_c2p_pool(const C2PBoxArgs a, const EOS eos, const C2PQueue q) {
-  c2p_pool_body<EOS>(a, eos, blockIdx, 0, q);
 }
 
 template <class EOS>

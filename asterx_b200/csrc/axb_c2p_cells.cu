@@ -12,7 +12,8 @@ using namespace axb;
 namespace axb {
 MlpDev mlp_device_view(const axb_mlp *m);
 int mlp_nf(const axb_mlp *m);
-int launch_mlp_guess(const axb_cells &c, const axb_mlp *m, float2 *guess, cudaStream_t s);
+int launch_mlp_guess(const axb_cells &c, const axb_mlp *m, float2 *guess, DevStatus *status,
+                     cudaStream_t s);
 
 struct C2PCellsArgs {
   axb_cells c;
@@ -286,7 +287,8 @@ AXB_API int axb_c2p_cells(axb_ctx *ctx, const axb_cells *cells, const axb_params
   cudaStream_t s = (cudaStream_t)stream;
   if (mlp) {
     axb_mark(ctx, AXB_R_MLP, s, true);
-    const int rc = launch_mlp_guess(*cells, mlp, reinterpret_cast<float2 *>(cells->guess), s);
+    const int rc = launch_mlp_guess(*cells, mlp, reinterpret_cast<float2 *>(cells->guess),
+                                   ctx->status, s);
     axb_mark(ctx, AXB_R_MLP, s, false);
     if (rc)
       return rc;

@@ -8,8 +8,8 @@
 
 namespace axb {
 
-template <int RECON, class EOS>
-int launch_flux_pass_eos(int dir, const RhsArgs &a, const EOS &eos, int seglen,
+template <int RECON, class EOS, bool UCT>
+int launch_flux_pass_uct(int dir, const RhsArgs &a, const EOS &eos, int seglen,
                          cudaStream_t s) {
   const BoxDev &b = a.b;
   if (dir == 0) {
@@ -18,7 +18,7 @@ int launch_flux_pass_eos(int dir, const RhsArgs &a, const EOS &eos, int seglen,
     const long long blocks = (warps * 32 + 127) / 128;
     if (blocks > 0x7fffffffLL)
       return AXB_ERR_TOO_LARGE;
-    k_flux_x<RECON, EOS><<<(unsigned)blocks, 128, 0, s>>>(a, eos);
+    k_flux_x<RECON, EOS, UCT><<<(unsigned)blocks, 128, 0, s>>>(a, eos);
     return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
   }
   const int T0 = 0, T1 = dir == 2 ? 1 : 2;
@@ -33,9 +33,9 @@ int launch_flux_pass_eos(int dir, const RhsArgs &a, const EOS &eos, int seglen,
     const dim3 grid((b.n[T0] + 2 * a.text + 31) / 32, (b.n[T1] + 2 * a.text + 3) / 4,
                     (b.n[dir] + seglen - 1) / seglen);
     if (dir == 1)
-      k_flux_pass<1, RECON, EOS><<<grid, block, 0, s>>>(a, eos, seglen);
+      k_flux_pass<1, RECON, EOS, UCT><<<grid, block, 0, s>>>(a, eos, seglen);
     else
-      k_flux_pass<2, RECON, EOS><<<grid, block, 0, s>>>(a, eos, seglen);
+      k_flux_pass<2, RECON, EOS, UCT><<<grid, block, 0, s>>>(a, eos, seglen);
     return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
   }
   // the threads walk the transverse plane [ng-1, ng+n]^2 row after row
@@ -46,10 +46,20 @@ int launch_flux_pass_eos(int dir, const RhsArgs &a, const EOS &eos, int seglen,
   const long long plane = (long long)(b.n[T0] + 2 * a.text) * (b.n[T1] + 2 * a.text);
   const dim3 grid(unsigned((plane + 127) / 128), 1, (b.n[dir] + seglen - 1) / seglen);
   if (dir == 1)
-    k_flux_pass<1, RECON, EOS><<<grid, block, 0, s>>>(ap, eos, seglen);
+    k_flux_pass<1, RECON, EOS, UCT><<<grid, block, 0, s>>>(ap, eos, seglen);
   else
-    k_flux_pass<2, RECON, EOS><<<grid, block, 0, s>>>(ap, eos, seglen);
+    k_flux_pass<2, RECON, EOS, UCT><<<grid, block, 0, s>>>(ap, eos, seglen);
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+}
+
+// the upwind-CT face data and the wider transverse range are a separate
+// instantiation, so the flux-CT passes carry none of it
+template <int RECON, class EOS>
+int launch_flux_pass_eos(int dir, const RhsArgs &a, const EOS &eos, int seglen,
+                         cudaStream_t s) {
+  if (a.use_uct)
+    return launch_flux_pass_uct<RECON, EOS, true>(dir, a, eos, seglen, s);
+  return launch_flux_pass_uct<RECON, EOS, false>(dir, a, eos, seglen, s);
 }
 
 template <int RECON>

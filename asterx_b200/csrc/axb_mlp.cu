@@ -73,6 +73,10 @@ struct axb_mlp {
 };
 
 namespace axb {
+int launch_mlp_forward_tc(const MlpDev &m, const float *feat, long long n, float *out,
+                          DevStatus *status, cudaStream_t s);
+int launch_mlp_guess_tc(const axb_cells &c, const MlpDev &m, float2 *guess, DevStatus *status,
+                        cudaStream_t s);
 MlpDev mlp_device_view(const axb_mlp *m) { return m->dev(); }
 int mlp_nf(const axb_mlp *m) { return m->nf; }
 } // namespace axb
@@ -541,26 +545,15 @@ AXB_API int axb_mlp_forward(axb_ctx *c, const axb_mlp *m, const float *features,
     return AXB_ERR_ARG;
   if (n == 0)
     return AXB_OK;
-  const long long blocks = (n + 255) / 256;
-  k_mlp_forward<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(m->dev(), features, n,
-                                                                     out);
-  return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+  return launch_mlp_forward_tc(m->dev(), features, n, out, c->status, (cudaStream_t)stream);
 }
 
 
 namespace axb {
-int launch_mlp_guess(const axb_cells &c, const axb_mlp *m, float2 *guess, cudaStream_t s) {
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const long long chunks = (c.n + 31) / 32;
-  long long blocks = (chunks + 7) / 8;
-  if (blocks > 4LL * sms) // persistent: a few CTAs per SM amortise the weight copy
-    blocks = 4LL * sms;
-  if (blocks < 1)
-    return AXB_OK;
-  k_mlp_guess<<<(unsigned)blocks, 256, 0, s>>>(c, m->dev(), guess);
-  return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+// the learned guess on the tensor cores (axb_mlp_tc.cu)
+int launch_mlp_guess(const axb_cells &c, const axb_mlp *m, float2 *guess, DevStatus *status,
+                     cudaStream_t s) {
+  return launch_mlp_guess_tc(c, m->dev(), guess, status, s);
 }
 } // namespace axb
 

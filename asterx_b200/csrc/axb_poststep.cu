@@ -238,15 +238,12 @@ AXB_API int axb_con2prim_group(axb_ctx *c, const axb_box *box,
       cudaMemsetAsync(q.count, 0, sizeof(unsigned long long), s);
       int sms = 148;
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-      // pooled fast pass: tiles of C2P_POOL_TILE cells of one (i, j) plane
-      const long long plane = (long long)b.n[0] * b.n[1];
-      const dim3 pgrid(unsigned((plane + C2P_POOL_TILE - 1) / C2P_POOL_TILE), 1, b.n[2]);
       if (eos->kind == 1) {
         const EosTab t = tab_for_launch(*eos, a.status);
-        k_c2p_pool<<<pgrid, C2P_POOL_T, 0, s>>>(a, t, q);
+        k_c2p_fast<<<grid, T, 0, s>>>(a, t, q);
         k_c2p_deferred<<<4 * sms, T, 0, s>>>(a, t, q);
       } else {
-        k_c2p_pool<<<pgrid, C2P_POOL_T, 0, s>>>(a, eos->ideal, q);
+        k_c2p_fast<<<grid, T, 0, s>>>(a, eos->ideal, q);
         k_c2p_deferred<<<4 * sms, T, 0, s>>>(a, eos->ideal, q);
       }
       cudaFreeAsync(buf, s);

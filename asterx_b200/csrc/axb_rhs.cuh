@@ -45,7 +45,7 @@ struct RhsArgs {
   int use_uct;
   // transverse ghost layers the flux passes cover: 1 (the edge field of
   // flux CT needs one), 3 with upwind CT (its reconstructions to the edges
-  // reach three faces out)
+  // reach three faces out); the kernels take it as a template constant
   int text;
   int recon_method; // reconstruction of the upwind-CT edge values
   double *aux[7];   // Fx Fy Fz Fbetax Fbetay Fbetaz G
@@ -90,12 +90,17 @@ AXB_HD void fast_speeds(double alp, double beta, double uinv, double vdir, doubl
 // bounding speeds cmax = max(0, speeds) and cmin = min(0, speeds):
 // HLLE with the reciprocal icpm = 1 / (cmax - cmin) (a product instead of
 // the division), LxF with ch = max(cmax, -cmin) = max |speed|.
+// Every operation is rounded on its own (no multiply-add contraction): the
+// contraction choices depend on the surrounding kernel, and the single-box
+// and batched passes must give a face the same bits.
 AXB_HD double hlle_flux(double cmax, double cmin, double icpm, double uL, double uR,
                         double fL, double fR) {
-  return (cmax * fL - cmin * fR + cmax * cmin * (uR - uL)) * icpm;
+  return mul_rn(add_rn(add_rn(mul_rn(cmax, fL), -mul_rn(cmin, fR)),
+                       mul_rn(mul_rn(cmax, cmin), add_rn(uR, -uL))),
+                icpm);
 }
 AXB_HD double laxf_flux(double ch, double uL, double uR, double fL, double fR) {
-  return 0.5 * ((fL + fR) - ch * (uR - uL));
+  return mul_rn(0.5, add_rn(add_rn(fL, fR), -mul_rn(ch, add_rn(uR, -uL))));
 }
 
 // The stage combine U_k <- alpha U_n + beta U_k + gdt RHS with an explicit
@@ -175,7 +180,8 @@ struct SideOut {
 // and only the tabulated EOS, which cannot take this route, would clamp eps).
 // r[R_VX..R_VZ] hold the reconstructed vel^i, zvec^i or svec^i (recvar):
 // W and v^i follow from them as in fluxes.cxx:396-505.
-template <int DIR, class EOS>
+// UCT: also the transverse vtilde components (upwind CT)
+template <int DIR, bool UCT, class EOS>
 AXB_D void side_physics(const FaceMetric &m, const double *r, double Bdir,
                         const EOS &eos, int rec_temp, int recvar, SideOut &o) {
   constexpr int D1 = (DIR + 1) % 3, D2 = (DIR + 2) % 3;
@@ -233,8 +239,10 @@ AXB_D void side_physics(const FaceMetric &m, const double *r, double Bdir,
   double vt[3];
   for (int i = 0; i < 3; ++i)
     vt[i] = m.alp * vel[i] - m.beta[i];
-  o.vt1 = vt[D1];
-  o.vt2 = vt[D2];
+  if constexpr (UCT) {
+    o.vt1 = vt[D1];
+    o.vt2 = vt[D2];
+  }
   const double alp_b0 = W * dot3(B, vlow);
   double Blow[3];
   lower3(m.g, B, Blow);

@@ -339,10 +339,12 @@ uint3 stage_grid(const axb_box &b) {
   const long long plane = (long long)(b.n[0] + 1) * (b.n[1] + 1);
   return make_uint3(unsigned((plane + 127) / 128), 1, b.n[2] + 1);
 }
+// set 0: the 11 evolved variables; 1: the 12 cell-centred primitives; 2: the
+// primitives and the reconstructed zvec or svec (15 cell-centred fields)
 uint3 sync_grid(const axb_box &b, int set) {
   const BoxDev bd = make_box(b);
   long long g = 0;
-  const int nf = set ? 12 : NEVOLVED;
+  const int nf = set == 0 ? NEVOLVED : set == 1 ? 12 : 15;
   for (int q = 0; q < nf; ++q) {
     int c[3] = {1, 1, 1};
     if (!set)

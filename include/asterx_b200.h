@@ -57,6 +57,7 @@ typedef enum axb_status {
 #define AXB_EW_C2P_FAIL 0x4u   /* at least one cell ended as C2P_FAIL        */
 #define AXB_EW_ROOT_CAP 0x8u   /* an EOS temperature root find hit its cap    */
 #define AXB_EW_QUEUE_TIMEOUT 0x10u /* persistent work queue gave up          */
+#define AXB_EW_MMA_TIMEOUT 0x20u /* a tensor-core wait of the learned guess gave up */
 
 /* ------------------------------------------------------------------------ */
 /* grid functions                                                            */
@@ -483,9 +484,10 @@ typedef struct axb_cells {
   double *fallback; /* output, may be NULL */
 } axb_cells;
 
-/* Learned initial guess: an MLP nf -> 64 -> 64 -> 64 -> 2 (SiLU hidden
- * activations; nf = 8, or 9 with Ye for a tabulated EOS) evaluated in BF16
- * on the tensor cores with FP32 accumulation, inside the recovery kernel.
+/* Learned initial guess: an MLP nf -> 64 -> 64 -> 64 -> 2 (SiLU or ReLU
+ * hidden activations; nf = 8, or 9 with Ye for a tabulated EOS) evaluated in
+ * BF16 on the tensor cores (tcgen05, tiles of 128 cells, FP32 accumulators in
+ * tensor memory).
  * Outputs: y0 = the position of x = h W in the Palenzuela scheme's
  * initial bracket [max(1e-10, 1 + q - s), 2 + 2 q - s]
  * (c2p_1DPalenzuela.hxx:395-398), y1 = ln W.  The Noble scheme starts from

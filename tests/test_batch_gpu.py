@@ -1,8 +1,10 @@
 """Batched level substep: one persistent launch per phase over boxes of
-different shapes gives exactly (bit for bit; MP5 within last-bit
-differences of a few faces) what one axb_substep per box
-gives, over a full SSP-RK3 step, before and after the autotuner has changed
-the flux passes' segment length and grid size."""
+different shapes gives what one axb_substep per box gives (up to the
+last-bit differences of the multiply-add contraction each kernel form
+chooses, carried by the recovery to at most its tolerance), over a full
+SSP-RK3 step, before and after the autotuner has changed the flux passes'
+segment length and grid size; and the batched level against the reference
+build box by box."""
 import numpy as np
 import pytest
 
@@ -86,16 +88,14 @@ def test_batch_matches_per_box(engine, recon):
             for k in EVOLVED + ["rho", "velx", "eps", "press", "Bvecx", "con2prim_flag"]:
                 x = da[k].cpu().numpy()
                 y = db[k].cpu().numpy()
-                if recon != "mp5":
-                    assert np.array_equal(x, y, equal_nan=True), (tune, q, k)
-                elif k == "con2prim_flag":
+                if k == "con2prim_flag":
                     # a last-bit difference may move a bracket across the
                     # iteration cap: first and second scheme may swap
                     diff = x != y
                     ps = [abi.C2P_PRIME, abi.C2P_SECOND]
                     assert (np.isin(x[diff], ps) & np.isin(y[diff], ps)).all(), (tune, q, k)
                 else:
-                    # the MP5 kernels of the two forms fuse a few products
+                    # the flux kernels of the two forms fuse a few products
                     # into multiply-adds differently (contraction is decided
                     # per kernel): last-bit differences in some faces, which
                     # the recovery's Brent bracket (c2p_tol 1e-10) carries to

@@ -112,6 +112,7 @@ def test_rhs_upwind_ct(engine, ref, recon, recon_type):
     magnetised box, against the reference build with its fluxes widened by
     three layers."""
     L, f = W.curved_box(n=12, ng=5, seed=13, wmax=3.0)
+    W.cons_from_prims(L, f)  # zvec consistent with vel (the sources read it)
     p = abi.default_params(reconstruction_method=recon, flux_type="hlle", use_uct=1,
                            recon_type=recon_type)
     host, gpu, st = run_both(engine, ref, L, f, p, 4.0 / 3.0)
