@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(128, AXB_C2P_MINB)
     cv.DEnt = c.DEnt ? c.DEnt[i] : 0.0;
     glo = sym3{c.g[0][i], c.g[1][i], c.g[2][i], c.g[3][i], c.g[4][i], c.g[5][i]};
   }
-  // learned guess (x = h W, W) from k_mlp_guess
+  // learned guess (x = h W, W) from k_mlp_guess_tc
   double zguess = -1.0, vsqguess = -1.0, xlo = -1.0, xhi = -1.0;
   if (a.use_mlp && valid) {
     const float2 gs = reinterpret_cast<const float2 *>(c.guess)[i];

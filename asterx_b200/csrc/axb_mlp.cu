@@ -160,54 +160,6 @@ __global__ void k_mlp_features(const axb_cells c, int nf, float *out) {
     out[i * nf + k] = f[k];
 }
 
-// tensor-core forward on given features (the code path of the recovery's
-// learned guess, mlp_cell_guess)
-__global__ void __launch_bounds__(256) k_mlp_forward(const MlpDev m, const float *feat,
-                                                     long long n, float *out) {
-  __shared__ MlpSmem w;
-  __shared__ uint32_t stage[8][32 * 8];
-  mlp_stage_weights(m, w);
-  __syncthreads();
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  float f[MLP_K1];
-#pragma unroll
-  for (int k = 0; k < MLP_K1; ++k)
-    f[k] = (i < n && k < m.nf) ? feat[i * m.nf + k] : 0.0f;
-  float y0, y1;
-  mlp_forward_warp(w, f, stage[threadIdx.x >> 5], y0, y1);
-  if (i < n) {
-    out[2 * i] = y0;
-    out[2 * i + 1] = y1;
-  }
-}
-
-// Learned guess of independent cells, ahead of the recovery: features from
-// the conserved variables and metric, the network, and the decoded guess
-// (x = h W, W) per cell.  A persistent grid: each CTA stages the weights
-// once and its warps walk chunks of 32 cells.  (Evaluated inside the
-// recovery kernel instead, the network's fragments and the recovery's
-// state together exceed the recovery's register budget; the separate
-// launch costs one 8-byte write and read per cell.)
-__global__ void __launch_bounds__(256) k_mlp_guess(const axb_cells c, const MlpDev m,
-                                                   float2 *guess) {
-  __shared__ MlpSmem w;
-  __shared__ uint32_t stage[8][32 * 8];
-  mlp_stage_weights(m, w);
-  __syncthreads();
-  const int lane = threadIdx.x & 31;
-  const long long warp0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  const long long nchunks = (c.n + 31) / 32;
-  for (long long ch = warp0; ch < nchunks; ch += nwarps) { // warp-uniform
-    const long long i = ch * 32 + lane;
-    const bool valid = i < c.n;
-    double x, W;
-    mlp_cell_guess(c, i, valid, m.nf, w, stage[threadIdx.x >> 5], x, W);
-    if (valid)
-      guess[i] = make_float2(float(x), float(W));
-  }
-}
-
 // ---------------------------------------------------------------------------
 // training
 // ---------------------------------------------------------------------------

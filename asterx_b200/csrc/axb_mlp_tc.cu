@@ -15,12 +15,11 @@
 // byte offset (next core matrix along K) is 128 and the stride byte offset
 // (next 8 rows) is 16K.  One K = 16 step covers two core matrices along K.
 //
-// The network and its numerics are those of the warp-level path in
-// axb_mlp.cuh (BF16 weights and activations, FP32 accumulation); the bias is
-// added after the products instead of seeding the accumulator, and the
-// products are summed in the tensor core's order, so outputs agree with it
-// to FP32 rounding.  Every wait on the mbarrier is bounded: on a timeout the
-// CTA sets AXB_EW_MMA_TIMEOUT, releases its tensor memory and returns.
+// Numerics: BF16 weights and activations, FP32 accumulation, the bias added
+// to the accumulated products, so the outputs agree with the FP32 network of
+// the training kernels (axb_mlp.cu) to the BF16 rounding of the operands.
+// Every wait on the mbarrier is bounded: on a timeout the CTA sets
+// AXB_EW_MMA_TIMEOUT, releases its tensor memory and returns.
 #include <cuda_bf16.h>
 
 #include "axb_internal.hxx"
@@ -33,6 +32,7 @@ constexpr int TC_M = 128;    // cells per tile = rows of every product
 constexpr int TC_COLS = 64;  // tensor-memory columns: one 128 x 64 FP32 accumulator
 constexpr int TC_N4 = 16;    // output layer padded to the smallest N for M = 128
 constexpr long long TC_WAIT_LIMIT = 1LL << 22; // mbarrier polls before giving up
+constexpr int TC_BIAS_COL = 14; // feature columns 14, 15 carry layer 1's bias
 
 // byte offset of element (r, k) of an R x K operand (canonical K-major)
 AXB_HD constexpr unsigned kmaj(int r, int k, int K) {
@@ -129,8 +129,18 @@ AXB_D void tc_stage(const MlpDev &m, TcSmem &S) {
   const int t = threadIdx.x, nt = blockDim.x;
   char *w1 = reinterpret_cast<char *>(S.w1), *w2 = reinterpret_cast<char *>(S.w2),
        *w3 = reinterpret_cast<char *>(S.w3), *w4 = reinterpret_cast<char *>(S.w4);
-  for (int e = t; e < MLP_H * MLP_K1; e += nt)
-    *reinterpret_cast<__nv_bfloat16 *>(w1 + kmaj(e / MLP_K1, e % MLP_K1, MLP_K1)) = m.w1[e];
+  // layer 1's bias rides in the product: feature columns 14 and 15 hold 1
+  // and the weights there the bias split into a BF16 high and low part
+  // (the features use at most 9 of the 16 columns)
+  for (int e = t; e < MLP_H * MLP_K1; e += nt) {
+    const int n = e / MLP_K1, k = e % MLP_K1;
+    __nv_bfloat16 v = m.w1[e];
+    if (k >= TC_BIAS_COL) {
+      const __nv_bfloat16 hi = __float2bfloat16(m.b1[n]);
+      v = k == TC_BIAS_COL ? hi : __float2bfloat16(m.b1[n] - __bfloat162float(hi));
+    }
+    *reinterpret_cast<__nv_bfloat16 *>(w1 + kmaj(n, k, MLP_K1)) = v;
+  }
   for (int e = t; e < MLP_H * MLP_H; e += nt) {
     *reinterpret_cast<__nv_bfloat16 *>(w2 + kmaj(e / MLP_H, e % MLP_H, MLP_H)) = m.w2[e];
     *reinterpret_cast<__nv_bfloat16 *>(w3 + kmaj(e / MLP_H, e % MLP_H, MLP_H)) = m.w3[e];
@@ -165,29 +175,45 @@ AXB_D bool tc_layer(const TcSmem &S, const void *A, const void *B, int K, int N,
            smem_desc(static_cast<const char *>(B) + kk * 256, sbo), id, kk > 0);
     umma_commit(bar);
   }
-  const bool ok = mbar_wait(bar, parity);
+  // one thread waits on the mbarrier, the others at the block barrier (so
+  // they issue nothing meanwhile)
+  const bool ok = threadIdx.x == 0 ? mbar_wait(bar, parity) : true;
   parity ^= 1u;
+  const bool all_ok = !__syncthreads_or(!ok);
   fence_after_sync();
-  return ok;
+  return all_ok;
 }
 
 // This thread's row of a 64-column accumulator + bias, activated, rounded to
 // BF16 and stored as row `r` of the hidden operand.
+// (bias == nullptr: the bias is already in the product.)  ReLU is applied
+// to the packed BF16 pair (rounding and max with 0 commute).
 AXB_D void tc_hidden_out(TcSmem &S, unsigned trow, const float *bias, int r) {
   char *ah = reinterpret_cast<char *>(S.ah);
+  const bool relu = S.act == MLP_ACT_RELU;
+  const __nv_bfloat162 zero2 = __floats2bfloat162_rn(0.0f, 0.0f);
 #pragma unroll
   for (int c16 = 0; c16 < MLP_H / 16; ++c16) {
     float v[16];
     tmem_ld16(trow + unsigned(c16 * 16), v);
+    if (bias) {
+#pragma unroll
+      for (int q = 0; q < 16; ++q)
+        v[q] += bias[c16 * 16 + q];
+    }
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
       uint4 pk;
       unsigned *p = reinterpret_cast<unsigned *>(&pk);
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const int j = c16 * 16 + h * 8 + 2 * q;
-        p[q] = pack_bf16x2(mlp_act(v[h * 8 + 2 * q] + bias[j], S.act),
-                           mlp_act(v[h * 8 + 2 * q + 1] + bias[j + 1], S.act));
+        const float a = v[h * 8 + 2 * q], b = v[h * 8 + 2 * q + 1];
+        if (relu) {
+          __nv_bfloat162 x = __hmax2(__floats2bfloat162_rn(a, b), zero2);
+          p[q] = *reinterpret_cast<const unsigned *>(&x);
+        } else {
+          p[q] = pack_bf16x2(silu(a), silu(b));
+        }
       }
       *reinterpret_cast<uint4 *>(ah + kmaj(r, c16 * 16 + h * 8, MLP_H)) = pk;
     }
@@ -202,19 +228,17 @@ AXB_D bool tc_forward(TcSmem &S, unsigned tmem, unsigned &parity, float &y0, flo
   fence_async_smem();
   fence_before_sync();
   __syncthreads();
-  bool ok = tc_layer(S, S.a1, S.w1, MLP_K1, MLP_H, tmem, parity);
-  if (__syncthreads_or(!ok))
+  if (!tc_layer(S, S.a1, S.w1, MLP_K1, MLP_H, tmem, parity))
     return false;
-  const float *bias[3] = {S.b1, S.b2, S.b3};
+  const float *bias[3] = {nullptr, S.b2, S.b3}; // layer 1's is in the product
   const __nv_bfloat16 *w[2] = {S.w2, S.w3};
   for (int l = 0; l < 3; ++l) {
     tc_hidden_out(S, trow, bias[l], r);
     fence_async_smem();
     fence_before_sync();
     __syncthreads();
-    ok = tc_layer(S, S.ah, l < 2 ? static_cast<const void *>(w[l]) : S.w4, MLP_H,
-                  l < 2 ? MLP_H : TC_N4, tmem, parity);
-    if (__syncthreads_or(!ok))
+    if (!tc_layer(S, S.ah, l < 2 ? static_cast<const void *>(w[l]) : S.w4, MLP_H,
+                  l < 2 ? MLP_H : TC_N4, tmem, parity))
       return false;
   }
   float v[16];
@@ -260,8 +284,10 @@ AXB_D void tc_teardown(unsigned tmem, bool failed, DevStatus *status) {
 }
 
 // features of this thread's row (zero beyond nf) into the A operand
-AXB_D void tc_put_features(TcSmem &S, const float (&f)[MLP_K1]) {
+AXB_D void tc_put_features(TcSmem &S, float (&f)[MLP_K1]) {
   char *a1 = reinterpret_cast<char *>(S.a1);
+  f[TC_BIAS_COL] = 1.0f;
+  f[TC_BIAS_COL + 1] = 1.0f;
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     uint4 pk;
@@ -301,8 +327,62 @@ __global__ void __launch_bounds__(TC_M) k_mlp_forward_tc(const MlpDev m, const f
   tc_teardown(tmem, failed, status);
 }
 
-// The learned guess of independent cells (x = h W and W per cell, decoded as
-// mlp_cell_guess decodes it), ahead of the recovery.
+// The invariants and features of cell_invariants / mlp_features computed in
+// FP32: the features are rounded to BF16 for the first layer and the guess
+// only narrows the root finder's bracket (which the FP64 iteration checks),
+// so FP32 is ample, and the FP64 divisions, roots and logarithms dominated
+// the kernel.  q and s (for the decoded guess) come out as well.
+struct InvF {
+  float q, s;
+};
+AXB_D InvF features_fast(double dens_d, const double (&mom_d)[3], double tau_d, double DYe_d,
+                         const double (&dB_d)[3], const sym3 &gd, int nf, float *f) {
+  const float gxx = float(gd.xx), gxy = float(gd.xy), gxz = float(gd.xz),
+              gyy = float(gd.yy), gyz = float(gd.yz), gzz = float(gd.zz);
+  const float c00 = gyy * gzz - gyz * gyz, c01 = gxz * gyz - gxy * gzz,
+              c02 = gxy * gyz - gxz * gyy;
+  const float det = gxx * c00 + gxy * c01 + gxz * c02;
+  const float idet = 1.0f / det;
+  const float isq = rsqrtf(det);
+  // the inverse metric (cofactors / det)
+  const float uxx = c00 * idet, uxy = c01 * idet, uxz = c02 * idet,
+              uyy = (gxx * gzz - gxz * gxz) * idet, uyz = (gxy * gxz - gxx * gyz) * idet,
+              uzz = (gxx * gyy - gxy * gxy) * idet;
+  const float D = float(dens_d) * isq;
+  const float S[3] = {float(mom_d[0]) * isq, float(mom_d[1]) * isq, float(mom_d[2]) * isq};
+  const float B[3] = {float(dB_d[0]) * isq, float(dB_d[1]) * isq, float(dB_d[2]) * isq};
+  const float Ssq = S[0] * (uxx * S[0] + uxy * S[1] + uxz * S[2]) +
+                    S[1] * (uxy * S[0] + uyy * S[1] + uyz * S[2]) +
+                    S[2] * (uxz * S[0] + uyz * S[1] + uzz * S[2]);
+  const float Bsq = B[0] * (gxx * B[0] + gxy * B[1] + gxz * B[2]) +
+                    B[1] * (gxy * B[0] + gyy * B[1] + gyz * B[2]) +
+                    B[2] * (gxz * B[0] + gyz * B[1] + gzz * B[2]);
+  const float BS = B[0] * S[0] + B[1] * S[1] + B[2] * S[2];
+  const float iD = 1.0f / D;
+  const float qr = float(tau_d) * isq * iD, r = Ssq * iD * iD, sv = Bsq * iD,
+              t = BS * iD * rsqrtf(D);
+  const float q = fmaxf(qr, -0.999f);
+  const float lq = log1pf(q);
+  const float lr = log1pf(fmaxf(r, 0.0f));
+  const float den = 1.0f + q + sv;
+  const float iden = 1.0f / den;
+  f[0] = __logf(fmaxf(D, 1e-37f)) * 0.1f;
+  f[1] = lq;
+  f[2] = 0.5f * lr;
+  f[3] = log1pf(fmaxf(sv, 0.0f));
+  f[4] = fminf(t * t / (r * sv + 1e-37f), 1.0f);
+  f[5] = r * iden * iden;
+  f[6] = sv * iden;
+  f[7] = lq - 0.5f * lr;
+  if (nf > 8)
+    f[8] = float(DYe_d / dens_d);
+  return InvF{qr, sv};
+}
+
+// The learned guess of independent cells, ahead of the recovery: x = h W
+// placed by y0 in the Palenzuela scheme's initial bracket
+// [max(1e-10, 1 + q - s), 2 + 2 q - s] (c2p_1DPalenzuela.hxx:395-398) and
+// W = max(exp(y1), 1).
 __global__ void __launch_bounds__(TC_M) k_mlp_guess_tc(const axb_cells c, const MlpDev m,
                                                         float2 *guess, DevStatus *status) {
   __shared__ TcSmem S;
@@ -317,13 +397,12 @@ __global__ void __launch_bounds__(TC_M) k_mlp_guess_tc(const axb_cells c, const 
 #pragma unroll
     for (int k = 0; k < MLP_K1; ++k)
       f[k] = 0.0f;
-    CellInvariants inv{1.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    InvF inv{0.0f, 0.0f};
     if (valid) {
       const sym3 glo{c.g[0][i], c.g[1][i], c.g[2][i], c.g[3][i], c.g[4][i], c.g[5][i]};
       const double mom[3] = {c.mom[0][i], c.mom[1][i], c.mom[2][i]};
       const double dB[3] = {c.dB[0][i], c.dB[1][i], c.dB[2][i]};
-      inv = cell_invariants(c.dens[i], mom, c.tau[i], c.DYe[i], dB, glo);
-      mlp_features(inv, m.nf, f);
+      inv = features_fast(c.dens[i], mom, c.tau[i], c.DYe[i], dB, glo, m.nf, f);
     }
     tc_put_features(S, f);
     float y0, y1;
@@ -332,9 +411,9 @@ __global__ void __launch_bounds__(TC_M) k_mlp_guess_tc(const axb_cells c, const 
       break;
     }
     if (valid) {
-      const double lo = fmax(1e-10, 1.0 + inv.q - inv.s), hi = 2.0 + 2.0 * inv.q - inv.s;
-      guess[i] = make_float2(float(lo + double(y0) * (hi - lo)),
-                             float(fmax(exp(double(y1)), 1.0)));
+      const double q = inv.q, sv = inv.s;
+      const double lo = fmax(1e-10, 1.0 + q - sv), hi = 2.0 + 2.0 * q - sv;
+      guess[i] = make_float2(float(lo + double(y0) * (hi - lo)), fmaxf(__expf(y1), 1.0f));
     }
   }
   tc_teardown(tmem, failed, status);

@@ -34,10 +34,13 @@ UNIT = "zone-updates/s"
 SSPRK3 = [(0.0, 1.0, 1.0), (0.75, 0.25, 0.25), (1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0)]
 GAMMA = 4.0 / 3.0
 CFL_MAX = 0.9
-# the tabulated-EOS substep: temperature reconstructed and the recovery's
-# limits applied through the temperature (use_temperature), since the
-# tabulated EOS has no eps(rho, p); atmosphere temperature inside the table
-TAB_PARAMS = dict(reconstruct_with_temperature=1, t_atmo=0.011, use_temperature=1)
+# the tabulated-EOS substep: temperature reconstructed (the tabulated EOS has
+# no eps(rho, p) for the fluxes), the recovery with the reference's default
+# use_temperature = no (with it, the recovery floors eps at the atmosphere's
+# eps, which the synthetic table's T^4 / rho makes ~1e5 at the 1e-13 density
+# floor, and nearly every cell fails in both builds), atmosphere temperature
+# inside the table
+TAB_PARAMS = dict(reconstruct_with_temperature=1, t_atmo=0.011, use_temperature=0)
 # the survey's algorithmic figure for one substep: 112 FP64 values per zone
 # (RHS reads 34, stage 33, post-step reads 23 and writes 22)
 SUBSTEP_BYTES = 112 * 8

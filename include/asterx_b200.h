@@ -287,8 +287,12 @@ AXB_API int axb_eos_destroy(axb_eos *eos);
  * Face quantities the reference obtains by SYNC (face B fluxes one cell
  * outside the interior, vertex auxiliaries two vertices outside) are computed
  * from the ghost data instead, so no synchronisation is needed inside the
- * group.  Requires ng >= 3 and recon_type v_vec, use_uct = no.  The CFL speed
- * maximum accumulates into the context status. */
+ * group.  Requires ng >= 3; recon_type v_vec, z_vec (zvec_*) or s_vec
+ * (svec_*).  With use_uct (upwind CT, rhs.cxx:124-168) the fields also hold
+ * the twelve face arrays vtilde_*face, amax_*face, amin_*face (written), the
+ * face data are computed three layers outside the interior, and dB*_stag
+ * must be valid on three ghost layers.  The CFL speed maximum accumulates
+ * into the context status. */
 AXB_API int axb_rhs_group(axb_ctx *ctx, const axb_box *box,
                           const axb_fields *fields, const axb_params *params,
                           const axb_eos *eos, void *stream);
@@ -585,7 +589,8 @@ AXB_API int axb_c2p_cells(axb_ctx *ctx, const axb_cells *cells,
  * axb_ctx.  The device error word and the CFL maximum go to a static status
  * block that this entry point clears on every call and that is not
  * reported: a caller that needs them (for instance the root-cap flag of a
- * tabulated EOS) uses axb_rhs_group.  The first call on a device looks up the
+ * tabulated EOS) uses axb_rhs_group.  use_uct is not available here (its
+ * twelve face arrays are not part of the static scratch).   The first call on a device looks up the
  * arrays' device addresses with that device current; make it before any
  * stream capture.  All calls share the arrays: calls that overlap on the GPU
  * (other streams, other threads) race; order them on one stream. */
