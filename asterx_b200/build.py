@@ -87,7 +87,9 @@ def build(force=False, verbose=False, extra=()):
                 if verbose and log:
                     print(f"== {os.path.basename(futs[fu])}\n{log}")
     if force or jobs or _stale(SO, objs):
-        cmd = [NVCC, *ARCH, "-shared", "-o", SO, *objs, "-lcudart"]
+        # (NCCL, for the halo exchange of axb_halo.cu, is looked up at run
+        # time: whichever libnccl the process has loaded, else libnccl.so.2)
+        cmd = [NVCC, *ARCH, "-shared", "-o", SO, *objs, "-lcudart", "-ldl"]
         subprocess.run(cmd, check=True)
     return SO
 

@@ -4,7 +4,9 @@
 //   interpolation  EOSX/src/utils/eos_linear_interp_ND.hxx:50-206 (uniform
 //                  axes, index clamped to [0, n-2], linear along ln rho, then
 //                  ln T, then Ye)
-//   T inversion    Brent's zero finder, EOSX/src/utils/eos_brent.hxx:7-170
+//   T inversion    the root of the interpolant, found exactly (logtemp_root);
+//                  Brent's zero finder (EOSX/src/utils/eos_brent.hxx:7-170)
+//                  where the table is not monotonic in T
 //
 // Layout: only the four variables the hot path reads are kept, interleaved
 // per node as (ln P, ln(eps + shift), s, cs^2) -- variables 0, 1, 2 and 4 of
@@ -157,15 +159,62 @@ struct EosTab {
       eps = exp(vmax) - shift;
       return xlast[1];
     }
-    bool capped;
-    const double lt = zero_brent(
-        x0[1], xlast[1], 1.e-14,
-        [&](double l) { return leps - interp(TAB_EPS, lrho, l, ye); }, capped);
+    return logtemp_root(lrho, leps, ye, vmin, vmax);
+  }
+
+  // The root in ln T of leps = interp(EPS, lrho, ln T, ye).  The
+  // interpolant is linear in ln T within each cell of the T axis (the
+  // trilinear scheme interpolates along ln T between the two T nodes of the
+  // cell), so the root is found exactly: a bisection over the nodes' values
+  // (which grow with T for a thermodynamic table) locates the cell, and the
+  // linear equation of that cell gives the root.  The reference runs Brent's
+  // method on the whole axis to 1e-14 (eos_3p_tabulated3d.hxx:219-225,
+  // eos_brent.hxx); both land on the same root of the same interpolant,
+  // here to rounding.  Where the node values are not increasing around the
+  // root, the reference's Brent search is run instead.
+  AXB_HD double logtemp_root(double lrho, double leps, double ye, double vlo, double vhi) const {
+    // vlo = interp at node 0 < leps < vhi = interp at the last node
+    int lo = 0, hi = n[1] - 1;
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      const double vm = interp(TAB_EPS, lrho, x[1][mid], ye);
+      if (vm <= leps) {
+        lo = mid;
+        vlo = vm;
+      } else {
+        hi = mid;
+        vhi = vm;
+      }
+    }
+    // the cell [x_lo, x_lo+1]: interp = c0 + c1 * lambda, lambda in [0, 1]
+    const double xa = x[1][lo], xb = x[1][lo + 1];
+    const int i = find(0, lrho), k = find(2, ye);
+    double c[2][2]; // [T end][Ye end] after the interpolation along ln rho
+#pragma unroll
+    for (int o2 = 0; o2 < 2; ++o2)
+#pragma unroll
+      for (int o1 = 0; o1 < 2; ++o1) {
+        const long long base =
+            i + (long long)n[0] * ((lo + o1) + (long long)n[1] * (k + o2));
+        c[o1][o2] = lin(y[TAB_NV * base + TAB_EPS], y[TAB_NV * (base + 1) + TAB_EPS],
+                        x[0][i], x[0][i + 1], lrho);
+      }
+    const double lamy = (ye - x[2][k]) / (x[2][k + 1] - x[2][k]);
+    const double e0 = (c[0][1] - c[0][0]) * lamy + c[0][0]; // at x_lo
+    const double e1 = (c[1][1] - c[1][0]) * lamy + c[1][0]; // at x_lo+1
+    if (!(vlo <= leps && leps <= vhi) || !(e1 > e0)) {
+      bool capped;
+      const double lt = zero_brent(
+          x0[1], xlast[1], 1.e-14,
+          [&](double l) { return leps - interp(TAB_EPS, lrho, l, ye); }, capped);
 #ifdef __CUDA_ARCH__
-    if (capped && err)
-      atomicOr(err, AXB_EW_ROOT_CAP);
+      if (capped && err)
+        atomicOr(err, AXB_EW_ROOT_CAP);
 #endif
-    return lt;
+      return lt;
+    }
+    const double lam = fmin(fmax((leps - e0) / (e1 - e0), 0.0), 1.0);
+    return xa + lam * (xb - xa);
   }
   AXB_HD double lr_clamped(double rho) const {
     return log(fmin(fmax(rho, rgrho.min), rgrho.max));

@@ -5,7 +5,8 @@ Two ways to shard (boxes are the unit of work):
 * ``balance_boxes`` -- independent boxes (the benchmark's default, and a
   level's boxes): each rank takes a set of whole boxes, balanced by zone
   count with the longest-processing-time rule; no data-path collective.
-* ``SlabHalo`` -- one periodic patch cut into z-slabs, one per rank, with
+* ``SlabHalo`` / ``NcclSlabHalo`` -- one periodic patch cut into z-slabs,
+  one per rank (NcclSlabHalo: the same exchange in the engine, over NCCL), with
   the analogue of the driver's SYNC (AsterX/schedule.ccl:110-115,157-164):
   after the local periodic ghost fill, the ng ghost k-planes of every
   listed grid function are replaced by the neighbours' planes.  A k-plane
@@ -131,6 +132,41 @@ class SlabHalo:
             rh.copy_(b_high[q * seg:(q + 1) * seg])
 
 
+class NcclSlabHalo:
+    """The same exchange as SlabHalo behind the engine's C ABI: the packed
+    ghost planes travel in one NCCL group per exchange (axb_halo_create /
+    axb_halo_exchange; the pack and unpack are kernels of the engine).  One
+    engine-side halo per list of grid functions, created on first use; rank
+    0 makes the NCCL id and the process group hands it to the others."""
+
+    def __init__(self, eng, layout: Layout, rank: int, world: int, group=None):
+        if layout.n[2] < layout.ng:
+            raise ValueError("a slab must be at least ng cells thick")
+        self.eng, self.L, self.rank, self.world, self.group = eng, layout, rank, world, group
+        self._halos = {}
+
+    def _uid(self) -> bytes:
+        uid = self.eng.halo_unique_id() if self.rank == 0 else None
+        if self.world > 1:
+            import torch.distributed as dist
+            box = [uid]
+            dist.broadcast_object_list(box, src=0, group=self.group)
+            uid = box[0]
+        return uid
+
+    def exchange(self, tensors: Dict[str, "object"], names: Iterable[str]) -> None:
+        key = tuple(names)
+        if key not in self._halos:
+            self._halos[key] = self.eng.halo_create(self.L, self.world, self.rank, self._uid(),
+                                                    list(key))
+        self.eng.halo_exchange(self._halos[key], tensors)
+
+    def close(self) -> None:
+        for h in self._halos.values():
+            self.eng.halo_destroy(h)
+        self._halos = {}
+
+
 def allreduce_max(value: float, group=None, device=None) -> float:
     """The largest `value` over the ranks of `group` (one all-reduce of a
     double; the identity without an initialised process group)."""
@@ -167,7 +203,7 @@ def prims_to_sync(params) -> List[str]:
     return PRIMS + extra.get(int(getattr(params, "recon_type", 0)), [])
 
 
-def slab_substep(eng, L, f, fn, params, eos, alpha, beta, gamma, dt, halo: SlabHalo,
+def slab_substep(eng, L, f, fn, params, eos, alpha, beta, gamma, dt, halo,
                  cfl: bool = False):
     """One RK substep of a rank's slab (axb_substep's sequence with the
     neighbours' ghost planes): RHS group, stage update, local periodic fill

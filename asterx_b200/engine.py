@@ -333,6 +333,38 @@ class Engine:
                                                len(names), self.stream_ptr(stream)),
                     "axb_sync_periodic")
 
+    # -- multi-GPU halo exchange (z-slabs over NCCL) ------------------------------
+    def _bind_halo(self):
+        L = self.lib
+        L.axb_halo_unique_id.argtypes = [C.c_char_p]
+        L.axb_halo_create.argtypes = [_vp, C.POINTER(Box), C.c_int, C.c_int, C.c_char_p,
+                                      C.POINTER(C.c_int), C.c_int, C.POINTER(_vp)]
+        L.axb_halo_exchange.argtypes = [_vp, C.POINTER(Fields), _vp]
+        L.axb_halo_destroy.argtypes = [_vp]
+
+    def halo_unique_id(self) -> bytes:
+        self._bind_halo()
+        buf = C.create_string_buffer(128)
+        self._check(self.lib.axb_halo_unique_id(buf), "axb_halo_unique_id")
+        return buf.raw
+
+    def halo_create(self, layout, nranks, rank, uid: bytes, names):
+        self._bind_halo()
+        h = _vp()
+        box = layout.box()
+        ids = (C.c_int * len(names))(*[GF[n] for n in names])
+        self._check(self.lib.axb_halo_create(self.ctx, C.byref(box), nranks, rank, uid, ids,
+                                             len(names), C.byref(h)), "axb_halo_create")
+        return h
+
+    def halo_exchange(self, halo, tensors, stream=None):
+        f = self.fields_struct(tensors)
+        self._check(self.lib.axb_halo_exchange(halo, C.byref(f), self.stream_ptr(stream)),
+                    "axb_halo_exchange")
+
+    def halo_destroy(self, halo):
+        self._check(self.lib.axb_halo_destroy(halo), "axb_halo_destroy")
+
     def substep(self, layout, tensors, tensors_n, params, eos, alpha, beta, gamma, dt,
                 periodic=True, stream=None):
         box = layout.box()

@@ -599,6 +599,33 @@ AXB_API int axb_rhs_group_noalloc(const axb_box *box, const axb_fields *fields,
                                   void *stream);
 
 /* ------------------------------------------------------------------------ */
+/* multi-GPU: halo exchange of a z-slab decomposition over NCCL              */
+/* ------------------------------------------------------------------------ */
+
+/* The analogue of the driver's SYNC (AsterX/schedule.ccl:110-115,157-164)
+ * between ranks that each hold one z-slab of a periodic patch (one process
+ * per GPU; no counterpart as a routine in the reference, where CarpetX/AMReX
+ * does it).  axb_halo_unique_id makes the NCCL id on one rank (the caller
+ * hands it to the others); axb_halo_create builds the communicator and the
+ * packed buffers for the listed grid functions of this rank's box (n[2] =
+ * its slab's cells, at least ng); axb_halo_exchange replaces the ng ghost
+ * k-planes below and above the slab by the neighbours' planes: one pack
+ * kernel, one NCCL group of two sends and two receives, one unpack kernel,
+ * all on `stream`.  Plane mapping for nz interior cells and v = 1 for a
+ * field vertex-centred in z: ghosts [0, ng) <- lower neighbour's
+ * [nz, nz + ng); ghosts [ng + nz + v, 2 ng + nz + v) <- upper neighbour's
+ * [ng + v, 2 ng + v); with one rank this is the periodic wrap in z.  The x
+ * and y ghosts are filled beforehand by axb_sync_periodic (whose z wrap the
+ * exchange then overwrites). */
+typedef struct axb_halo axb_halo;
+AXB_API int axb_halo_unique_id(unsigned char id[128]);
+AXB_API int axb_halo_create(axb_ctx *ctx, const axb_box *box, int nranks, int rank,
+                            const unsigned char id[128], const int *field_ids, int nfields,
+                            axb_halo **out);
+AXB_API int axb_halo_exchange(axb_halo *halo, const axb_fields *fields, void *stream);
+AXB_API int axb_halo_destroy(axb_halo *halo);
+
+/* ------------------------------------------------------------------------ */
 /* stress-energy tensor and regrid error                                     */
 /* ------------------------------------------------------------------------ */
 

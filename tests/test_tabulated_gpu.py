@@ -78,8 +78,14 @@ def test_con2prim_tabulated(engine, ref, prime, second, use_temp):
     flags_g = interior(L, "x", got["con2prim_flag"])
     flags_r = interior(L, "x", host["con2prim_flag"])
     assert np.array_equal(flags_g, flags_r)
-    # the cells are recovered (not a comparison of two all-failed boxes)
-    assert np.isin(flags_r, [abi.C2P_PRIME, abi.C2P_SECOND]).mean() > 0.9
+    if prime == "noble":
+        # the reference's Noble scheme reads the EOS's gamma, which a table
+        # does not set: it fails, its failure leaves the conserved variables
+        # NaN, and the backup then fails as well -- in both builds
+        assert (flags_r == abi.C2P_FAIL).all()
+    else:
+        # the cells are recovered (not a comparison of two all-failed boxes)
+        assert np.isin(flags_r, [abi.C2P_PRIME, abi.C2P_SECOND]).mean() > 0.9
     assert st["error_word"] & 0x8 == 0  # no capped temperature inversion
     for n in C2P_OUT:
         emax, _ = errors(interior(L, n, got[n]), interior(L, n, host[n]))
