@@ -237,10 +237,12 @@ struct EosTab {
   AXB_HD double eps_from_valid_rho_temp_ye(double rho, double temp, double ye) const {
     return exp(interp(TAB_EPS, lr_clamped(rho), lt_clamped(temp), ye)) - shift;
   }
-  // not available for the tabulated EOS (the reference asserts, :259-269)
-  AXB_HD double eps_from_valid_rho_press_ye(double, double, double) const {
-    return nan("");
-  }
+  // no inversion of eps(press) for the tabulated EOS: the reference prints a
+  // warning, asserts, and with assertions compiled out returns 0
+  // (eos_3p_tabulated3d.hxx:259-269); the recovery reaches it only when a
+  // limit (v_lim, the table's largest rho, the pressure atmosphere) fires
+  // with use_temperature off
+  AXB_HD double eps_from_valid_rho_press_ye(double, double, double) const { return 0.0; }
   AXB_HD double csnd_from_valid_rho_eps_ye(double rho, double &eps, double ye) const {
     const double lr = lr_clamped(rho);
     const double lt = logtemp(rho, eps, ye);
