@@ -6,8 +6,11 @@
 // instructions (BF16 operands in shared memory, FP32 accumulator in tensor
 // memory), commits it to an mbarrier, and every thread then reads its row of
 // the accumulator back with `tcgen05.ld.32x32b` (warp w owns TMEM lanes
-// 32w..32w+31), adds the bias, applies the activation, rounds to BF16 and
-// stores the row as the next layer's A operand.
+// 32w..32w+31), applies the activation, rounds to BF16 and stores the row as
+// the next layer's A operand.  The hidden layers' biases ride in the
+// products: feature columns 14 and 15 of every row hold 1, and one more K = 16
+// step per layer multiplies the tile's features by a block whose columns 14
+// and 15 hold the bias split into a BF16 high and low part (zero elsewhere).
 //
 // Operands use the canonical K-major layout without swizzle: 8 x 8 core
 // matrices of 8 rows x 16 bytes; element (r, k) of an R x K operand sits at
@@ -15,9 +18,9 @@
 // byte offset (next core matrix along K) is 128 and the stride byte offset
 // (next 8 rows) is 16K.  One K = 16 step covers two core matrices along K.
 //
-// Numerics: BF16 weights and activations, FP32 accumulation, the bias added
-// to the accumulated products, so the outputs agree with the FP32 network of
-// the training kernels (axb_mlp.cu) to the BF16 rounding of the operands.
+// Numerics: BF16 weights and activations, FP32 accumulation, biases to about
+// 16 bits (high + low BF16 part), so the outputs agree with the FP32 network
+// of the training kernels (axb_mlp.cu) to the BF16 rounding of the operands.
 // Every wait on the mbarrier is bounded: on a timeout the CTA sets
 // AXB_EW_MMA_TIMEOUT, releases its tensor memory and returns.
 #include <cuda_bf16.h>
@@ -32,7 +35,7 @@ constexpr int TC_M = 128;    // cells per tile = rows of every product
 constexpr int TC_COLS = 64;  // tensor-memory columns: one 128 x 64 FP32 accumulator
 constexpr int TC_N4 = 16;    // output layer padded to the smallest N for M = 128
 constexpr long long TC_WAIT_LIMIT = 1LL << 22; // mbarrier polls before giving up
-constexpr int TC_BIAS_COL = 14; // feature columns 14, 15 carry layer 1's bias
+constexpr int TC_BIAS_COL = 14; // feature columns 14, 15 hold 1: the biases' columns
 
 // byte offset of element (r, k) of an R x K operand (canonical K-major)
 AXB_HD constexpr unsigned kmaj(int r, int k, int K) {
@@ -44,9 +47,11 @@ struct __align__(128) TcSmem {
   __nv_bfloat16 w2[MLP_H * MLP_H];  // N = 64 x K = 64
   __nv_bfloat16 w3[MLP_H * MLP_H];
   __nv_bfloat16 w4[TC_N4 * MLP_H];  // N = 16 x K = 64, rows 2..15 zero
-  __nv_bfloat16 a1[TC_M * MLP_K1];  // features of the tile
+  __nv_bfloat16 w2b[MLP_H * MLP_K1]; // layer 2's bias block: N = 64 x K = 16
+  __nv_bfloat16 w3b[MLP_H * MLP_K1]; // layer 3's
+  __nv_bfloat16 a1[TC_M * MLP_K1];  // features of the tile (kept for the bias steps)
   __nv_bfloat16 ah[TC_M * MLP_H];   // hidden activations of the tile
-  float b1[MLP_H], b2[MLP_H], b3[MLP_H], b4[2];
+  float b4[2];
   unsigned long long bar;
   unsigned int tmem;
   int act;
@@ -123,6 +128,27 @@ AXB_D void tmem_ld16(unsigned taddr, float (&v)[16]) {
     v[q] = __uint_as_float(r[q]);
 }
 
+// 32 consecutive columns: one load, one wait
+AXB_D void tmem_ld32(unsigned taddr, float (&v)[32]) {
+  unsigned r[32];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+               "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+               "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, "
+               "%31}, [%32];\n\t"
+               "tcgen05.wait::ld.sync.aligned;"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                 "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                 "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]),
+                 "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+                 "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
+                 "=r"(r[30]), "=r"(r[31])
+               : "r"(taddr)
+               : "memory");
+#pragma unroll
+  for (int q = 0; q < 32; ++q)
+    v[q] = __uint_as_float(r[q]);
+}
+
 // Stage the network's weights in the canonical operand layout (all threads;
 // a barrier must follow).
 AXB_D void tc_stage(const MlpDev &m, TcSmem &S) {
@@ -150,10 +176,18 @@ AXB_D void tc_stage(const MlpDev &m, TcSmem &S) {
     *reinterpret_cast<__nv_bfloat16 *>(w4 + kmaj(n, k, MLP_H)) =
         n < 2 ? m.w4[n * MLP_H + k] : __float2bfloat16(0.0f);
   }
-  for (int e = t; e < MLP_H; e += nt) {
-    S.b1[e] = m.b1[e];
-    S.b2[e] = m.b2[e];
-    S.b3[e] = m.b3[e];
+  // the bias blocks of layers 2 and 3 (against the features' unit columns)
+  char *w2b = reinterpret_cast<char *>(S.w2b), *w3b = reinterpret_cast<char *>(S.w3b);
+  for (int e = t; e < MLP_H * MLP_K1; e += nt) {
+    const int n = e / MLP_K1, k = e % MLP_K1;
+    __nv_bfloat16 v2 = __float2bfloat16(0.0f), v3 = v2;
+    if (k >= TC_BIAS_COL) {
+      const __nv_bfloat16 h2 = __float2bfloat16(m.b2[n]), h3 = __float2bfloat16(m.b3[n]);
+      v2 = k == TC_BIAS_COL ? h2 : __float2bfloat16(m.b2[n] - __bfloat162float(h2));
+      v3 = k == TC_BIAS_COL ? h3 : __float2bfloat16(m.b3[n] - __bfloat162float(h3));
+    }
+    *reinterpret_cast<__nv_bfloat16 *>(w2b + kmaj(n, k, MLP_K1)) = v2;
+    *reinterpret_cast<__nv_bfloat16 *>(w3b + kmaj(n, k, MLP_K1)) = v3;
   }
   if (t < 2)
     S.b4[t] = m.b4[t];
@@ -161,10 +195,12 @@ AXB_D void tc_stage(const MlpDev &m, TcSmem &S) {
     S.act = m.act;
 }
 
-// One layer's product into tensor memory: thread 0 issues K/16 MMAs and the
-// commit; every thread waits for the result.  Returns false on a timeout.
+// One layer's product into tensor memory: thread 0 issues K/16 MMAs (and,
+// with `Bb`, one more K = 16 step of the features against the bias block)
+// and the commit; every thread waits for the result.  Returns false on a
+// timeout.
 AXB_D bool tc_layer(const TcSmem &S, const void *A, const void *B, int K, int N, unsigned tmem,
-                    unsigned &parity) {
+                    unsigned &parity, const void *Bb = nullptr) {
   const unsigned bar = smem_u32(&S.bar);
   if (threadIdx.x == 0) {
     fence_after_sync();
@@ -173,6 +209,8 @@ AXB_D bool tc_layer(const TcSmem &S, const void *A, const void *B, int K, int N,
     for (int kk = 0; kk < K / 16; ++kk)
       umma(tmem, smem_desc(static_cast<const char *>(A) + kk * 256, sbo),
            smem_desc(static_cast<const char *>(B) + kk * 256, sbo), id, kk > 0);
+    if (Bb)
+      umma(tmem, smem_desc(S.a1, MLP_K1 * 16), smem_desc(Bb, MLP_K1 * 16), id, 1u);
     umma_commit(bar);
   }
   // one thread waits on the mbarrier, the others at the block barrier (so
@@ -184,38 +222,33 @@ AXB_D bool tc_layer(const TcSmem &S, const void *A, const void *B, int K, int N,
   return all_ok;
 }
 
-// This thread's row of a 64-column accumulator + bias, activated, rounded to
-// BF16 and stored as row `r` of the hidden operand.
-// (bias == nullptr: the bias is already in the product.)  ReLU is applied
-// to the packed BF16 pair (rounding and max with 0 commute).
-AXB_D void tc_hidden_out(TcSmem &S, unsigned trow, const float *bias, int r) {
+// a and b rounded to BF16 and clamped at 0 in one conversion (a in the low
+// half); rounding and the clamp commute
+AXB_D unsigned relu_bf16x2(float a, float b) {
+  unsigned d;
+  asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(b), "f"(a));
+  return d;
+}
+
+// This thread's row of a 64-column accumulator (bias included), activated,
+// rounded to BF16 and stored as row `r` of the hidden operand.
+AXB_D void tc_hidden_out(TcSmem &S, unsigned trow, int r) {
   char *ah = reinterpret_cast<char *>(S.ah);
   const bool relu = S.act == MLP_ACT_RELU;
-  const __nv_bfloat162 zero2 = __floats2bfloat162_rn(0.0f, 0.0f);
 #pragma unroll
-  for (int c16 = 0; c16 < MLP_H / 16; ++c16) {
-    float v[16];
-    tmem_ld16(trow + unsigned(c16 * 16), v);
-    if (bias) {
+  for (int c32 = 0; c32 < MLP_H / 32; ++c32) {
+    float v[32];
+    tmem_ld32(trow + unsigned(c32 * 32), v);
 #pragma unroll
-      for (int q = 0; q < 16; ++q)
-        v[q] += bias[c16 * 16 + q];
-    }
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < 4; ++h) {
       uint4 pk;
       unsigned *p = reinterpret_cast<unsigned *>(&pk);
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const float a = v[h * 8 + 2 * q], b = v[h * 8 + 2 * q + 1];
-        if (relu) {
-          __nv_bfloat162 x = __hmax2(__floats2bfloat162_rn(a, b), zero2);
-          p[q] = *reinterpret_cast<const unsigned *>(&x);
-        } else {
-          p[q] = pack_bf16x2(silu(a), silu(b));
-        }
+        p[q] = relu ? relu_bf16x2(a, b) : pack_bf16x2(silu(a), silu(b));
       }
-      *reinterpret_cast<uint4 *>(ah + kmaj(r, c16 * 16 + h * 8, MLP_H)) = pk;
+      *reinterpret_cast<uint4 *>(ah + kmaj(r, c32 * 32 + h * 8, MLP_H)) = pk;
     }
   }
 }
@@ -230,15 +263,17 @@ AXB_D bool tc_forward(TcSmem &S, unsigned tmem, unsigned &parity, float &y0, flo
   __syncthreads();
   if (!tc_layer(S, S.a1, S.w1, MLP_K1, MLP_H, tmem, parity))
     return false;
-  const float *bias[3] = {nullptr, S.b2, S.b3}; // layer 1's is in the product
-  const __nv_bfloat16 *w[2] = {S.w2, S.w3};
+#pragma unroll
   for (int l = 0; l < 3; ++l) {
-    tc_hidden_out(S, trow, bias[l], r);
+    tc_hidden_out(S, trow, r);
     fence_async_smem();
     fence_before_sync();
     __syncthreads();
-    if (!tc_layer(S, S.ah, l < 2 ? static_cast<const void *>(w[l]) : S.w4, MLP_H,
-                  l < 2 ? MLP_H : TC_N4, tmem, parity))
+    const void *B = l == 0 ? static_cast<const void *>(S.w2)
+                           : l == 1 ? static_cast<const void *>(S.w3) : S.w4;
+    const void *Bb = l == 0 ? static_cast<const void *>(S.w2b)
+                            : l == 1 ? static_cast<const void *>(S.w3b) : nullptr;
+    if (!tc_layer(S, S.ah, B, MLP_H, l < 2 ? MLP_H : TC_N4, tmem, parity, Bb))
       return false;
   }
   float v[16];
@@ -342,7 +377,7 @@ AXB_D InvF features_fast(double dens_d, const double (&mom_d)[3], double tau_d, 
   const float c00 = gyy * gzz - gyz * gyz, c01 = gxz * gyz - gxy * gzz,
               c02 = gxy * gyz - gxz * gyy;
   const float det = gxx * c00 + gxy * c01 + gxz * c02;
-  const float idet = 1.0f / det;
+  const float idet = __frcp_rn(det);
   const float isq = rsqrtf(det);
   // the inverse metric (cofactors / det)
   const float uxx = c00 * idet, uxy = c01 * idet, uxz = c02 * idet,
@@ -358,14 +393,14 @@ AXB_D InvF features_fast(double dens_d, const double (&mom_d)[3], double tau_d, 
                     B[1] * (gxy * B[0] + gyy * B[1] + gyz * B[2]) +
                     B[2] * (gxz * B[0] + gyz * B[1] + gzz * B[2]);
   const float BS = B[0] * S[0] + B[1] * S[1] + B[2] * S[2];
-  const float iD = 1.0f / D;
+  const float iD = __frcp_rn(D);
   const float qr = float(tau_d) * isq * iD, r = Ssq * iD * iD, sv = Bsq * iD,
               t = BS * iD * rsqrtf(D);
   const float q = fmaxf(qr, -0.999f);
   const float lq = log1pf(q);
   const float lr = log1pf(fmaxf(r, 0.0f));
   const float den = 1.0f + q + sv;
-  const float iden = 1.0f / den;
+  const float iden = __frcp_rn(den);
   f[0] = __logf(fmaxf(D, 1e-37f)) * 0.1f;
   f[1] = lq;
   f[2] = 0.5f * lr;
@@ -383,6 +418,22 @@ AXB_D InvF features_fast(double dens_d, const double (&mom_d)[3], double tau_d, 
 // placed by y0 in the Palenzuela scheme's initial bracket
 // [max(1e-10, 1 + q - s), 2 + 2 q - s] (c2p_1DPalenzuela.hxx:395-398) and
 // W = max(exp(y1), 1).
+// the inputs of one cell, loaded a tile ahead
+struct CellIn {
+  double dens, tau, DYe, mom[3], dB[3];
+  sym3 g;
+};
+AXB_D void load_cell(const axb_cells &c, long long i, int nf, CellIn &x) {
+  x.dens = c.dens[i];
+  x.tau = c.tau[i];
+  x.DYe = nf > 8 ? c.DYe[i] : 0.0;
+  for (int q = 0; q < 3; ++q) {
+    x.mom[q] = c.mom[q][i];
+    x.dB[q] = c.dB[q][i];
+  }
+  x.g = sym3{c.g[0][i], c.g[1][i], c.g[2][i], c.g[3][i], c.g[4][i], c.g[5][i]};
+}
+
 __global__ void __launch_bounds__(TC_M) k_mlp_guess_tc(const axb_cells c, const MlpDev m,
                                                         float2 *guess, DevStatus *status) {
   __shared__ TcSmem S;
@@ -390,6 +441,14 @@ __global__ void __launch_bounds__(TC_M) k_mlp_guess_tc(const axb_cells c, const 
   unsigned parity = 0;
   bool failed = false;
   const long long ntiles = (c.n + TC_M - 1) / TC_M;
+  // the next tile's inputs are loaded before this tile's layers run, so
+  // their latency hides behind the tensor-core chain
+  CellIn cur{};
+  {
+    const long long i0 = (long long)blockIdx.x * TC_M + threadIdx.x;
+    if (blockIdx.x < ntiles && i0 < c.n)
+      load_cell(c, i0, m.nf, cur);
+  }
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const long long i = tile * TC_M + threadIdx.x;
     const bool valid = i < c.n;
@@ -398,12 +457,11 @@ __global__ void __launch_bounds__(TC_M) k_mlp_guess_tc(const axb_cells c, const 
     for (int k = 0; k < MLP_K1; ++k)
       f[k] = 0.0f;
     InvF inv{0.0f, 0.0f};
-    if (valid) {
-      const sym3 glo{c.g[0][i], c.g[1][i], c.g[2][i], c.g[3][i], c.g[4][i], c.g[5][i]};
-      const double mom[3] = {c.mom[0][i], c.mom[1][i], c.mom[2][i]};
-      const double dB[3] = {c.dB[0][i], c.dB[1][i], c.dB[2][i]};
-      inv = features_fast(c.dens[i], mom, c.tau[i], c.DYe[i], dB, glo, m.nf, f);
-    }
+    if (valid)
+      inv = features_fast(cur.dens, cur.mom, cur.tau, cur.DYe, cur.dB, cur.g, m.nf, f);
+    const long long inext = (tile + gridDim.x) * TC_M + threadIdx.x;
+    if (tile + gridDim.x < ntiles && inext < c.n)
+      load_cell(c, inext, m.nf, cur);
     tc_put_features(S, f);
     float y0, y1;
     if (!tc_forward(S, tmem, parity, y0, y1)) {
