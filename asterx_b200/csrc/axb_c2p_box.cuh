@@ -46,8 +46,26 @@ struct C2PBoxArgs {
   // ghost layers across each face set that curl A covers: 1 (the next RHS
   // reads one), 3 with upwind CT (its edge reconstructions reach three)
   int bext;
+  // learned guess (x = h W, W) of each interior cell, (i, j, k) at
+  // ((k - ng) n_y + j - ng) n_x + i - ng, and the half-width of the
+  // Palenzuela bracket around x; read only by the GUESS kernels
+  const float2 *guess;
+  double bracket;
   DevStatus *status;
 };
+
+template <class EOS>
+AXB_D void run_solver_guess(int which, const EOS &eos, const C2PBoxArgs &a, const Atmo &atmo,
+                            Prim &pv, Prim &seeds, Cons &cv, const sym3 &glo, Report &rep,
+                            double zguess, double vsqguess, double xlo, double xhi) {
+  if (which == AXB_C2P_NOBLE)
+    noble_solve(eos, a.cp, atmo, a.gamma_noble, a.Zmin, pv, seeds, cv, glo, rep, zguess,
+                vsqguess);
+  else if (which == AXB_C2P_PALENZUELA)
+    palenzuela_solve(eos, a.cp, atmo, pv, cv, glo, rep, xlo, xhi);
+  else if (which == AXB_C2P_ENTROPY)
+    entropy_solve(eos, a.cp, atmo, pv, cv, glo, rep);
+}
 
 // ComputeStaggeredB<dir> (AsterX/src/computeBfromA.cxx:20-56) on the faces
 // [ng, ng+n] along d and [ng-e, ng+n+e-1] across, e = bext ghost layers
@@ -168,11 +186,18 @@ AXB_D int after_both_failed(const EOS &eos, const C2PBoxArgs &a, const Atmo &atm
 // same unmodified inputs, so every cell gets exactly the full cascade's
 // result.  The rare paths' code stays out of the fast kernel and no warp of
 // it waits on them.
+//
+// GUESS (with a.guess): the first solver starts from the learned guess --
+// the Noble seeds Z = D x, v^2 = 1 - 1/W^2, or the Palenzuela bracket
+// x (1 -+ bracket).  A guessed first attempt that fails returns C2P_RETRY
+// having written nothing; the caller then runs the cell again without the
+// guess (the plain seeds, as c2p_2DNoble.hxx:374-393 and
+// c2p_1DPalenzuela.hxx:395-401 set them, and the plain cascade).
 enum { C2P_FULL = 0, C2P_FAST = 1 };
-enum { C2P_DONE = 0, C2P_DEFERRED = 1 };
-template <class EOS, int MODE>
+enum { C2P_DONE = 0, C2P_DEFERRED = 1, C2P_RETRY = 2 };
+template <class EOS, int MODE, bool GUESS = false>
 AXB_D int c2p_cell(const C2PBoxArgs &a, const EOS &eos, const int i, const int j,
-                   const int k, int &iters_first, bool &failed) {
+                   const int k, int &iters_first, bool &failed, bool use_guess = false) {
   constexpr bool FASTLIKE = MODE == C2P_FAST;
   const BoxDev &b = a.b;
   {
@@ -278,12 +303,27 @@ AXB_D int c2p_cell(const C2PBoxArgs &a, const EOS &eos, const int i, const int j
       pv = seeds;
       call_c2p = false;
     }
+    double zguess = -1.0, vsqguess = -1.0, xlo = -1.0, xhi = -1.0;
+    if constexpr (GUESS) {
+      if (use_guess && call_c2p) {
+        const long long ci =
+            ((long long)(k - b.ng) * b.n[1] + (j - b.ng)) * b.n[0] + (i - b.ng);
+        const float2 gs = a.guess[ci];
+        const double x = gs.x, W = gs.y;
+        zguess = cv.dens / sqrt_detg * x; // Z = rho h W^2 = D (h W)
+        vsqguess = 1.0 - 1.0 / (W * W);
+        xlo = x * (1.0 - a.bracket);
+        xhi = x * (1.0 + a.bracket);
+        if (!(zguess > 0.0 && zguess < 1e300 && vsqguess >= 0.0 && vsqguess < 1.0))
+          zguess = vsqguess = xlo = xhi = -1.0;
+      }
+    }
     cons_floors(cv, glo);
     if constexpr (FASTLIKE) {
       if (call_c2p) {
         Report r1;
         code = AXB_C2P_PRIME;
-        palenzuela_solve<EOS, true>(eos, a.cp, atmo, pv, cv, glo, r1);
+        palenzuela_solve<EOS, true>(eos, a.cp, atmo, pv, cv, glo, r1, xlo, xhi);
         if (r1.failed())
           return C2P_DEFERRED; // REP_DEFER: every failure goes to the full cascade
         iters_first = r1.iters;
@@ -291,7 +331,16 @@ AXB_D int c2p_cell(const C2PBoxArgs &a, const EOS &eos, const int i, const int j
     } else if (call_c2p) {
       Report r1, r2;
       code = AXB_C2P_PRIME;
-      run_solver(a.c2p_prime, eos, a, atmo, pv, seeds, cv, glo, r1);
+      if (GUESS && zguess >= 0.0) {
+        run_solver_guess(a.c2p_prime, eos, a, atmo, pv, seeds, cv, glo, r1, zguess, vsqguess,
+                         xlo, xhi);
+        if (r1.failed()) {
+          iters_first = r1.iters;
+          return C2P_RETRY;
+        }
+      } else {
+        run_solver(a.c2p_prime, eos, a, atmo, pv, seeds, cv, glo, r1);
+      }
       iters_first = r1.iters;
       if (r1.failed()) {
         code = AXB_C2P_SECOND;
@@ -367,7 +416,30 @@ AXB_D void c2p_epilogue(const C2PBoxArgs &a, unsigned int *s_hist, int iters_fir
   }
 }
 
-template <class EOS>
+// The full cascade on one cell; with GUESS a failed guessed attempt is
+// followed by the plain one, and the cell's first-solver iterations count
+// both attempts.
+template <class EOS, bool GUESS>
+AXB_D void c2p_cell_full(const C2PBoxArgs &a, const EOS &eos, int i, int j, int k,
+                         int &iters_first, bool &failed) {
+  if constexpr (GUESS) {
+    int it0 = 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      const int rc =
+          c2p_cell<EOS, C2P_FULL, true>(a, eos, i, j, k, iters_first, failed, attempt == 0);
+      if (rc != C2P_RETRY) {
+        if (attempt == 1 && iters_first >= 0)
+          iters_first += it0;
+        return;
+      }
+      it0 = iters_first;
+    }
+  } else {
+    c2p_cell<EOS, C2P_FULL>(a, eos, i, j, k, iters_first, failed);
+  }
+}
+
+template <class EOS, bool GUESS = false>
 AXB_D void c2p_box_body(const C2PBoxArgs &a, const EOS &eos, const uint3 bid) {
   __shared__ unsigned int s_hist[64];
   c2p_hist_init(a, s_hist);
@@ -377,13 +449,13 @@ AXB_D void c2p_box_body(const C2PBoxArgs &a, const EOS &eos, const uint3 bid) {
   int iters_first = -1;
   bool failed = false;
   if (in_range)
-    c2p_cell<EOS, C2P_FULL>(a, eos, i, j, k, iters_first, failed);
+    c2p_cell_full<EOS, GUESS>(a, eos, i, j, k, iters_first, failed);
   c2p_epilogue(a, s_hist, iters_first, failed);
 }
-template <class EOS>
+template <class EOS, bool GUESS = false>
 __global__ void __launch_bounds__(128, AXB_C2P_MINB)
     k_c2p_box(const C2PBoxArgs a, const EOS eos) {
-  c2p_box_body<EOS>(a, eos, blockIdx);
+  c2p_box_body<EOS, GUESS>(a, eos, blockIdx);
 }
 
 // Deferred cells of a fast pass: the count, then one entry per cell,
@@ -415,7 +487,7 @@ AXB_D void queue_deferred(const C2PQueue &q, bool defer, int i, int j, int k, in
 
 // Fast pass over one tile: the common path, deferred cells appended to the
 // queue (warp-aggregated).
-template <class EOS>
+template <class EOS, bool GUESS = false>
 AXB_D void c2p_fast_body(const C2PBoxArgs &a, const EOS &eos, const uint3 bid, int box,
                          const C2PQueue &q) {
   __shared__ unsigned int s_hist[64];
@@ -427,7 +499,8 @@ AXB_D void c2p_fast_body(const C2PBoxArgs &a, const EOS &eos, const uint3 bid, i
   bool failed = false;
   bool defer = false;
   if (in_range)
-    defer = c2p_cell<EOS, C2P_FAST>(a, eos, i, j, k, iters_first, failed) == C2P_DEFERRED;
+    defer = c2p_cell<EOS, C2P_FAST, GUESS>(a, eos, i, j, k, iters_first, failed, GUESS) ==
+            C2P_DEFERRED;
   queue_deferred(q, defer, i, j, k, box);
   c2p_epilogue(a, s_hist, iters_first, failed);
 }
@@ -435,7 +508,7 @@ AXB_D void c2p_fast_body(const C2PBoxArgs &a, const EOS &eos, const uint3 bid, i
 // The full cascade over the queued cells; `args_of(box)` gives the box's
 // argument block.  Every thread runs the same number of rounds, so the
 // warp-level epilogue sees full warps.
-template <class EOS, class ArgsOf>
+template <class EOS, class ArgsOf, bool GUESS = false>
 AXB_D void c2p_deferred_body(const ArgsOf &args_of, const EOS &eos, const C2PQueue &q) {
   __shared__ unsigned int s_hist[64];
   const C2PBoxArgs &a0 = args_of(0);
@@ -456,7 +529,7 @@ AXB_D void c2p_deferred_body(const ArgsOf &args_of, const EOS &eos, const C2PQue
     if (e < n) {
       const unsigned long long v = q.cell[e];
       const int i = int(v & 0x7fff), j = int((v >> 15) & 0x7fff), k = int((v >> 30) & 0x7fff);
-      c2p_cell<EOS, C2P_FULL>(args_of(int(v >> 45)), eos, i, j, k, iters_first, failed);
+      c2p_cell_full<EOS, GUESS>(args_of(int(v >> 45)), eos, i, j, k, iters_first, failed);
     }
     const unsigned nfail = __popc(__ballot_sync(0xffffffffu, failed));
     if (nfail && (threadIdx.x % 32) == 0) {
@@ -474,16 +547,17 @@ AXB_D void c2p_deferred_body(const ArgsOf &args_of, const EOS &eos, const C2PQue
   }
 }
 
-template <class EOS>
+template <class EOS, bool GUESS = false>
 __global__ void __launch_bounds__(128, AXB_C2P_FAST_MINB)
     k_c2p_fast(const C2PBoxArgs a, const EOS eos, const C2PQueue q) {
-  c2p_fast_body<EOS>(a, eos, blockIdx, 0, q);
+  c2p_fast_body<EOS, GUESS>(a, eos, blockIdx, 0, q);
 }
 
-template <class EOS>
+template <class EOS, bool GUESS = false>
 __global__ void __launch_bounds__(128, AXB_C2P_MINB)
     k_c2p_deferred(const C2PBoxArgs a, const EOS eos, const C2PQueue q) {
-  c2p_deferred_body([&](int) -> const C2PBoxArgs & { return a; }, eos, q);
+  auto args_of = [&](int) -> const C2PBoxArgs & { return a; };
+  c2p_deferred_body<EOS, decltype(args_of), GUESS>(args_of, eos, q);
 }
 
 // whether a box's extent fits the queue's packing

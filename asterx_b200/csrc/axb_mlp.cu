@@ -77,6 +77,8 @@ int launch_mlp_forward_tc(const MlpDev &m, const float *feat, long long n, float
                           DevStatus *status, cudaStream_t s);
 int launch_mlp_guess_tc(const axb_cells &c, const MlpDev &m, float2 *guess, DevStatus *status,
                         cudaStream_t s);
+int launch_mlp_guess_box_tc(const MlpBoxIn &in, const MlpDev &m, float2 *guess,
+                            DevStatus *status, cudaStream_t s);
 MlpDev mlp_device_view(const axb_mlp *m) { return m->dev(); }
 int mlp_nf(const axb_mlp *m) { return m->nf; }
 } // namespace axb
@@ -506,6 +508,10 @@ namespace axb {
 int launch_mlp_guess(const axb_cells &c, const axb_mlp *m, float2 *guess, DevStatus *status,
                      cudaStream_t s) {
   return launch_mlp_guess_tc(c, m->dev(), guess, status, s);
+}
+int launch_mlp_guess_box(const MlpBoxIn &in, const axb_mlp *m, float2 *guess,
+                         DevStatus *status, cudaStream_t s) {
+  return launch_mlp_guess_box_tc(in, m->dev(), guess, status, s);
 }
 } // namespace axb
 

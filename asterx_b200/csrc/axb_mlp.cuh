@@ -32,6 +32,16 @@ struct MlpDev {
   double bracket;
 };
 
+// The interior cells of a box as the learned guess reads them: cell ci =
+// ((k - ng) n_y + j - ng) n_x + i - ng, the cell-centred B the average of the
+// two dB_stag faces and the cell-centred metric the average of the eight
+// vertices (as the box recovery forms them, computeBfromA.cxx:67-85,
+// aster_interp.hxx:23-36).
+struct MlpBoxIn {
+  BoxDev b;
+  const double *dens, *mom[3], *tau, *DYe, *dBstag[3], *g[6];
+};
+
 // ---------------------------------------------------------------------------
 // features (double arithmetic, FP32 result); must match axb_mlp_features
 // ---------------------------------------------------------------------------

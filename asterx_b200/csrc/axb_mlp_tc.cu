@@ -423,35 +423,73 @@ struct CellIn {
   double dens, tau, DYe, mom[3], dB[3];
   sym3 g;
 };
-AXB_D void load_cell(const axb_cells &c, long long i, int nf, CellIn &x) {
-  x.dens = c.dens[i];
-  x.tau = c.tau[i];
-  x.DYe = nf > 8 ? c.DYe[i] : 0.0;
-  for (int q = 0; q < 3; ++q) {
-    x.mom[q] = c.mom[q][i];
-    x.dB[q] = c.dB[q][i];
-  }
-  x.g = sym3{c.g[0][i], c.g[1][i], c.g[2][i], c.g[3][i], c.g[4][i], c.g[5][i]};
-}
 
-__global__ void __launch_bounds__(TC_M) k_mlp_guess_tc(const axb_cells c, const MlpDev m,
+// independent cells: the arrays of axb_cells
+struct CellsSrc {
+  axb_cells c;
+  long long n;
+  AXB_D void load(long long i, int nf, CellIn &x) const {
+    x.dens = c.dens[i];
+    x.tau = c.tau[i];
+    x.DYe = nf > 8 ? c.DYe[i] : 0.0;
+    for (int q = 0; q < 3; ++q) {
+      x.mom[q] = c.mom[q][i];
+      x.dB[q] = c.dB[q][i];
+    }
+    x.g = sym3{c.g[0][i], c.g[1][i], c.g[2][i], c.g[3][i], c.g[4][i], c.g[5][i]};
+  }
+};
+
+// the interior cells of a box (MlpBoxIn)
+struct BoxSrc {
+  MlpBoxIn in;
+  long long n;
+  AXB_D void load(long long ci, int nf, CellIn &x) const {
+    const BoxDev &b = in.b;
+    const long long nxy = (long long)b.n[0] * b.n[1];
+    const int k = int(ci / nxy);
+    const long long r = ci - k * nxy;
+    const int j = int(r / b.n[0]);
+    const int i = int(r - (long long)j * b.n[0]);
+    const long long I = b.at(i + b.ng, j + b.ng, k + b.ng);
+    x.dens = in.dens[I];
+    x.tau = in.tau[I];
+    x.DYe = nf > 8 ? in.DYe[I] : 0.0;
+    for (int q = 0; q < 3; ++q)
+      x.mom[q] = in.mom[q][I];
+    x.dB[0] = 0.5 * (in.dBstag[0][I] + in.dBstag[0][I + 1]);
+    x.dB[1] = 0.5 * (in.dBstag[1][I] + in.dBstag[1][I + b.sy]);
+    x.dB[2] = 0.5 * (in.dBstag[2][I] + in.dBstag[2][I + b.sz]);
+    double gv[6];
+    for (int q = 0; q < 6; ++q) {
+      const double *f = in.g[q];
+      gv[q] = (f[I] + f[I + 1] + f[I + b.sy] + f[I + 1 + b.sy] + f[I + b.sz] +
+               f[I + 1 + b.sz] + f[I + b.sy + b.sz] + f[I + 1 + b.sy + b.sz]) *
+              0.125;
+    }
+    x.g = sym3{gv[0], gv[1], gv[2], gv[3], gv[4], gv[5]};
+  }
+};
+
+template <class Src>
+__global__ void __launch_bounds__(TC_M) k_mlp_guess_tc(const Src src, const MlpDev m,
                                                         float2 *guess, DevStatus *status) {
   __shared__ TcSmem S;
   const unsigned tmem = tc_setup(m, S);
   unsigned parity = 0;
   bool failed = false;
-  const long long ntiles = (c.n + TC_M - 1) / TC_M;
+  const long long ntiles = (src.n + TC_M - 1) / TC_M;
   // the next tile's inputs are loaded before this tile's layers run, so
   // their latency hides behind the tensor-core chain
   CellIn cur{};
   {
     const long long i0 = (long long)blockIdx.x * TC_M + threadIdx.x;
-    if (blockIdx.x < ntiles && i0 < c.n)
-      load_cell(c, i0, m.nf, cur);
+    if (blockIdx.x < ntiles && i0 < src.n)
+      src.load(i0, m.nf, cur);
   }
   for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const long long i = tile * TC_M + threadIdx.x;
-    const bool valid = i < c.n;
+    const bool valid = i < src.n;
     float f[MLP_K1];
 #pragma unroll
     for (int k = 0; k < MLP_K1; ++k)
@@ -460,8 +498,8 @@ __global__ void __launch_bounds__(TC_M) k_mlp_guess_tc(const axb_cells c, const 
     if (valid)
       inv = features_fast(cur.dens, cur.mom, cur.tau, cur.DYe, cur.dB, cur.g, m.nf, f);
     const long long inext = (tile + gridDim.x) * TC_M + threadIdx.x;
-    if (tile + gridDim.x < ntiles && inext < c.n)
-      load_cell(c, inext, m.nf, cur);
+    if (tile + gridDim.x < ntiles && inext < src.n)
+      src.load(inext, m.nf, cur);
     tc_put_features(S, f);
     float y0, y1;
     if (!tc_forward(S, tmem, parity, y0, y1)) {
@@ -503,7 +541,17 @@ int launch_mlp_guess_tc(const axb_cells &c, const MlpDev &m, float2 *guess, DevS
   const int blocks = tc_blocks(c.n);
   if (blocks < 1)
     return AXB_OK;
-  k_mlp_guess_tc<<<blocks, TC_M, 0, s>>>(c, m, guess, status);
+  k_mlp_guess_tc<<<blocks, TC_M, 0, s>>>(CellsSrc{c, c.n}, m, guess, status);
+  return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+}
+
+int launch_mlp_guess_box_tc(const MlpBoxIn &in, const MlpDev &m, float2 *guess,
+                            DevStatus *status, cudaStream_t s) {
+  const long long n = (long long)in.b.n[0] * in.b.n[1] * in.b.n[2];
+  const int blocks = tc_blocks(n);
+  if (blocks < 1)
+    return AXB_OK;
+  k_mlp_guess_tc<<<blocks, TC_M, 0, s>>>(BoxSrc{in, n}, m, guess, status);
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
 }
 

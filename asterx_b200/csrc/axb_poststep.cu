@@ -3,6 +3,7 @@
 // its Noble -> Palenzuela -> atmosphere cascade (AsterX/src/con2prim.cxx:
 // 73-454); the device code is in axb_c2p_box.cuh.
 #include "axb_c2p_box.cuh"
+#include "axb_mlp.cuh"
 
 using namespace axb;
 
@@ -125,6 +126,8 @@ int fill_c2p_args(axb_ctx *c, const axb_box *box, const axb_fields *f,
   a.svec[1] = GFP(svec_y);
   a.svec[2] = GFP(svec_z);
   a.flag = GFP(con2prim_flag);
+  a.guess = nullptr;
+  a.bracket = 0.0;
   const void *req[] = {a.Avec[0], a.Avec[1], a.Avec[2], a.dBstag[0], a.dBstag[1],
                        a.dBstag[2], a.alp, a.dens, a.mom[0], a.mom[1], a.mom[2],
                        a.tau, a.DYe, a.DEnt, a.rho, a.vel[0], a.vel[1], a.vel[2],
@@ -194,19 +197,43 @@ int fill_c2p_args(axb_ctx *c, const axb_box *box, const axb_fields *f,
 
 } // namespace axb
 
-// AsterX_Con2PrimGroup on one box (AsterX/schedule.ccl:119-165): replaces
-// AsterX_ComputedBstagFromA (computeBfromA.cxx:58-65),
-// AsterX_ComputedBFromdBstag (computeBfromA.cxx:67-85) and AsterX_Con2Prim
-// (con2prim.cxx:457-502).
-AXB_API int axb_con2prim_group(axb_ctx *c, const axb_box *box,
-                               const axb_fields *f, const axb_params *p,
-                               const axb_eos *eos, void *stream) {
+namespace axb {
+MlpDev mlp_device_view(const axb_mlp *m);
+int mlp_nf(const axb_mlp *m);
+int launch_mlp_guess_box(const MlpBoxIn &in, const axb_mlp *m, float2 *guess,
+                         DevStatus *status, cudaStream_t s);
+
+// the recovery kernels of one box, with or without the learned guess
+template <bool GUESS>
+void launch_box_recovery(const C2PBoxArgs &a, const axb_eos *eos, const dim3 grid, int T,
+                         bool fast, const C2PQueue &q, int sms, cudaStream_t s) {
+  if (fast) {
+    if (eos->kind == 1) {
+      const EosTab t = tab_for_launch(*eos, a.status);
+      k_c2p_fast<EosTab, GUESS><<<grid, T, 0, s>>>(a, t, q);
+      k_c2p_deferred<EosTab, GUESS><<<4 * sms, T, 0, s>>>(a, t, q);
+    } else {
+      k_c2p_fast<EosIdeal, GUESS><<<grid, T, 0, s>>>(a, eos->ideal, q);
+      k_c2p_deferred<EosIdeal, GUESS><<<4 * sms, T, 0, s>>>(a, eos->ideal, q);
+    }
+  } else if (eos->kind == 1) {
+    k_c2p_box<EosTab, GUESS><<<grid, T, 0, s>>>(a, tab_for_launch(*eos, a.status));
+  } else {
+    k_c2p_box<EosIdeal, GUESS><<<grid, T, 0, s>>>(a, eos->ideal);
+  }
+}
+
+int con2prim_group_run(axb_ctx *c, const axb_box *box, const axb_fields *f,
+                       const axb_params *p, const axb_eos *eos, const axb_mlp *mlp,
+                       void *stream) {
   if (!c)
     return AXB_ERR_ARG;
   C2PBoxArgs a;
   int rc = fill_c2p_args(c, box, f, p, eos, a);
   if (rc)
     return rc;
+  if (mlp && eos->kind == 1 && mlp_nf(mlp) != 9)
+    return AXB_ERR_ARG; // the tabulated guess takes Ye as a ninth input
   cudaStream_t s = (cudaStream_t)stream;
   const BoxDev &b = a.b;
   const int T = 128;
@@ -221,38 +248,86 @@ AXB_API int axb_con2prim_group(axb_ctx *c, const axb_box *box,
     k_bstag<<<grid, T, 0, s>>>(ap);
     axb_mark(c, AXB_R_BSTAG, s, false);
   }
+  const unsigned long long ncell = (unsigned long long)b.n[0] * b.n[1] * b.n[2];
+  void *gbuf = nullptr;
+  if (mlp) {
+    // the guess of every interior cell from its conserved variables, the
+    // dB_stag just computed and the metric, ahead of the recovery
+    if (axb_scratch_alloc(c, &gbuf, ncell * sizeof(float2), s) != cudaSuccess)
+      return AXB_ERR_CUDA;
+    MlpBoxIn in;
+    in.b = a.b;
+    in.dens = a.dens;
+    in.tau = a.tau;
+    in.DYe = a.DYe;
+    for (int q = 0; q < 3; ++q) {
+      in.mom[q] = a.mom[q];
+      in.dBstag[q] = a.dBstag[q];
+    }
+    for (int q = 0; q < 6; ++q)
+      in.g[q] = a.g[q];
+    axb_mark(c, AXB_R_MLP, s, true);
+    rc = launch_mlp_guess_box(in, mlp, static_cast<float2 *>(gbuf), a.status, s);
+    axb_mark(c, AXB_R_MLP, s, false);
+    if (rc) {
+      cudaFreeAsync(gbuf, s);
+      return rc;
+    }
+    a.guess = static_cast<const float2 *>(gbuf);
+    a.bracket = mlp_device_view(mlp).bracket;
+  }
   {
     const dim3 grid((b.n[0] + T - 1) / T, b.n[1], b.n[2]);
     axb_mark(c, AXB_R_C2P, s, true);
-    if (a.c2p_prime == AXB_C2P_PALENZUELA && c2p_queue_fits(*box)) {
+    const bool fast = a.c2p_prime == AXB_C2P_PALENZUELA && c2p_queue_fits(*box);
+    void *buf = nullptr;
+    C2PQueue q{nullptr, nullptr};
+    int sms = 148;
+    if (fast) {
       // fast pass + the full cascade on the deferred cells; the queue (all
       // interior cells at most) comes from the stream-ordered allocator
-      const unsigned long long ncell = (unsigned long long)b.n[0] * b.n[1] * b.n[2];
-      void *buf = nullptr;
       if (axb_scratch_alloc(c, &buf, (ncell + 1) * sizeof(unsigned long long), s) !=
-          cudaSuccess)
+          cudaSuccess) {
+        if (gbuf)
+          cudaFreeAsync(gbuf, s);
         return AXB_ERR_CUDA;
-      C2PQueue q;
+      }
       q.count = static_cast<unsigned long long *>(buf);
       q.cell = q.count + 1;
       cudaMemsetAsync(q.count, 0, sizeof(unsigned long long), s);
-      int sms = 148;
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-      if (eos->kind == 1) {
-        const EosTab t = tab_for_launch(*eos, a.status);
-        k_c2p_fast<<<grid, T, 0, s>>>(a, t, q);
-        k_c2p_deferred<<<4 * sms, T, 0, s>>>(a, t, q);
-      } else {
-        k_c2p_fast<<<grid, T, 0, s>>>(a, eos->ideal, q);
-        k_c2p_deferred<<<4 * sms, T, 0, s>>>(a, eos->ideal, q);
-      }
-      cudaFreeAsync(buf, s);
-    } else if (eos->kind == 1) {
-      k_c2p_box<<<grid, T, 0, s>>>(a, tab_for_launch(*eos, a.status));
-    } else {
-      k_c2p_box<<<grid, T, 0, s>>>(a, eos->ideal);
     }
+    if (mlp)
+      launch_box_recovery<true>(a, eos, grid, T, fast, q, sms, s);
+    else
+      launch_box_recovery<false>(a, eos, grid, T, fast, q, sms, s);
+    if (buf)
+      cudaFreeAsync(buf, s);
+    if (gbuf)
+      cudaFreeAsync(gbuf, s);
     axb_mark(c, AXB_R_C2P, s, false);
   }
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
+}
+} // namespace axb
+
+// AsterX_Con2PrimGroup on one box (AsterX/schedule.ccl:119-165): replaces
+// AsterX_ComputedBstagFromA (computeBfromA.cxx:58-65),
+// AsterX_ComputedBFromdBstag (computeBfromA.cxx:67-85) and AsterX_Con2Prim
+// (con2prim.cxx:457-502).
+AXB_API int axb_con2prim_group(axb_ctx *c, const axb_box *box,
+                               const axb_fields *f, const axb_params *p,
+                               const axb_eos *eos, void *stream) {
+  return con2prim_group_run(c, box, f, p, eos, nullptr, stream);
+}
+
+// The same with the learned initial guess of the first solver (no
+// counterpart in the reference): Noble's seeds or Palenzuela's bracket from
+// the network, a failed guessed attempt retried from the plain seeds.
+AXB_API int axb_con2prim_group_guess(axb_ctx *c, const axb_box *box, const axb_fields *f,
+                                     const axb_params *p, const axb_eos *eos,
+                                     const axb_mlp *mlp, void *stream) {
+  if (!mlp)
+    return AXB_ERR_ARG;
+  return con2prim_group_run(c, box, f, p, eos, mlp, stream);
 }

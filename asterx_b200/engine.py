@@ -57,6 +57,8 @@ def load_library(path=LIB_PATH):
                                   C.POINTER(Params), _vp, _vp]
     lib.axb_con2prim_group.argtypes = [_vp, C.POINTER(Box), C.POINTER(Fields),
                                        C.POINTER(Params), _vp, _vp]
+    lib.axb_con2prim_group_guess.argtypes = [_vp, C.POINTER(Box), C.POINTER(Fields),
+                                             C.POINTER(Params), _vp, _vp, _vp]
     lib.axb_rk_stage.argtypes = [_vp, C.POINTER(Box)] + [C.POINTER(Fields)] * 4 + \
         [C.c_double] * 4 + [_vp]
     lib.axb_sync_periodic.argtypes = [_vp, C.POINTER(Box), C.POINTER(Fields),
@@ -224,13 +226,20 @@ class Engine:
                                            self.stream_ptr(stream)), "axb_rhs_group")
 
     def con2prim_group(self, layout: Layout, tensors: dict, params: Params, eos,
-                       stream=None):
+                       stream=None, mlp=None):
+        """axb_con2prim_group, or axb_con2prim_group_guess with a network."""
         box = layout.box()
         f = self.fields_struct(tensors)
-        self._check(self.lib.axb_con2prim_group(self.ctx, C.byref(box), C.byref(f),
-                                                C.byref(params), eos,
-                                                self.stream_ptr(stream)),
-                    "axb_con2prim_group")
+        if mlp is None:
+            self._check(self.lib.axb_con2prim_group(self.ctx, C.byref(box), C.byref(f),
+                                                    C.byref(params), eos,
+                                                    self.stream_ptr(stream)),
+                        "axb_con2prim_group")
+        else:
+            self._check(self.lib.axb_con2prim_group_guess(self.ctx, C.byref(box), C.byref(f),
+                                                          C.byref(params), eos, mlp,
+                                                          self.stream_ptr(stream)),
+                        "axb_con2prim_group_guess")
 
     @staticmethod
     def strided_struct(arrays: dict):

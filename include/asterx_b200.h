@@ -572,6 +572,20 @@ AXB_API int axb_c2p_cells(axb_ctx *ctx, const axb_cells *cells,
                           const axb_params *params, const axb_eos *eos,
                           const axb_mlp *mlp, void *stream);
 
+/* axb_con2prim_group with the learned guess of the first solver: after
+ * curl A, the network evaluates every interior cell (its conserved variables,
+ * the cell average of dB_stag, the metric averaged from the eight vertices),
+ * and the first solver starts from that guess (Noble's seeds or the
+ * Palenzuela bracket, as above); a cell whose guessed first attempt fails is
+ * recovered again from the plain seeds (saved_*) through the plain cascade.
+ * The tabulated EOS needs a 9-input network (Ye).  The first solver's
+ * iterations of both attempts count in the context's histogram.  Uses a
+ * scratch float2 per interior cell from the stream-ordered allocator.
+ * `mlp` must be non-NULL (AXB_ERR_ARG).  No counterpart in the reference. */
+AXB_API int axb_con2prim_group_guess(axb_ctx *ctx, const axb_box *box,
+                                     const axb_fields *fields, const axb_params *params,
+                                     const axb_eos *eos, const axb_mlp *mlp, void *stream);
+
 /* axb_rhs_group for callers that cannot allocate device memory (a host
  * framework that owns every device allocation, a tool that may not call
  * cudaMalloc on a shared device, a driver whose footprint is fixed after
