@@ -203,6 +203,30 @@ AXB_HD double add_rn(double a, double b) {
 #endif
 }
 
+// x / 60, correctly rounded, without a division: q = RN(x r) with
+// r = RN(1/60) lies within an ulp of x / 60, so x - 60 q is exact (one FMA),
+// and q + (x - 60 q) r (one FMA) is off x / 60 by at most about 2^-53 ulp
+// before its rounding.  x / 60 = (x / 4) / 15 is either representable or at
+// least 1/30 ulp from the nearest midpoint (15 is odd), so that rounding
+// gives the correctly rounded quotient (Markstein's correction step,
+// IBM J. Res. Dev. 34(1), 1990; for divisors known in advance, Brisebarre,
+// Muller and Raina, IEEE Trans. Comput. 53(8), 2004).  The bounds need x
+// and q in the normal range; zeros, subnormals, infinities and NaN take the
+// division.
+AXB_HD double div60(double x) {
+#ifdef __CUDA_ARCH__
+  constexpr double r = 1.0 / 60.0;
+  const double q = __dmul_rn(x, r);
+  const double aq = fabs(q);
+  if (!(aq >= 0x1p-960 && aq <= 0x1p1000))
+    return x / 60.0;
+  const double rem = fma(-q, 60.0, x);
+  return fma(rem, r, q);
+#else
+  return x / 60.0;
+#endif
+}
+
 #ifndef AXB_MP5_SELECT
 #define AXB_MP5_SELECT 1
 #endif
@@ -210,13 +234,12 @@ AXB_HD double add_rn(double a, double b) {
 // MP5 interface value of the middle cell towards u_p1's side.
 AXB_HD double mp5_one(double gf_Imm, double gf_Im, double gf_I, double gf_Ip,
                       double gf_Ipp, double alpha) {
-  // ul feeds the early-accept test: the reference's division, and its
-  // products and sums rounded one by one, left to right
-  const double ul =
+  // ul feeds the early-accept test: the reference's correctly rounded
+  // quotient, and its products and sums rounded one by one, left to right
+  const double ul = div60(
       add_rn(add_rn(add_rn(add_rn(mul_rn(2, gf_Imm), -mul_rn(13, gf_Im)), mul_rn(47, gf_I)),
                     mul_rn(27, gf_Ip)),
-             -mul_rn(3, gf_Ipp)) /
-      60.0;
+             -mul_rn(3, gf_Ipp)));
   const double deltam = gf_I - gf_Im;
   const double deltap = gf_Ip - gf_I;
   const double ump = gf_I + minmod2(deltap, alpha * deltam);
