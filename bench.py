@@ -135,9 +135,12 @@ def traffic_table():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle-reason samples during the timed region."""
+    """nvidia-smi clock / throttle-reason samples during the timed region:
+    sampled every 50 ms from before the region (the first sample is awaited,
+    so the sampler is running when the region starts), kept when their
+    timestamp falls inside [begin(), stop()]."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -145,6 +148,7 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.t0 = None
 
     def start(self):
         try:
@@ -153,14 +157,30 @@ class ClockSampler:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            deadline = time.time() + 5.0
+            while time.time() < deadline and os.path.getsize(self.path) == 0:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
 
+    def begin(self):
+        self.t0 = time.time()
+
+    @staticmethod
+    def _when(stamp):
+        import datetime
+        try:
+            return datetime.datetime.strptime(stamp, "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except Exception:
+            return None
+
     def stop(self):
+        t1 = time.time()
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        time.sleep(0.06)  # the sample that covers the region's end
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -170,17 +190,21 @@ class ClockSampler:
         with open(self.path) as fh:
             for line in fh:
                 parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                if len(parts) >= 10 and parts[2].replace(".", "").isdigit():
                     rows.append(parts)
         os.unlink(self.path)
+        inside = [r for r in rows if self.t0 is not None and self._when(r[0]) is not None
+                  and self.t0 - 0.05 <= self._when(r[0]) <= t1 + 0.05]
+        rows = inside or rows[-1:]
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows]
+        sm = [float(r[2]) for r in rows]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]),
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[6 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][3]),
                 "reasons": reasons, "samples": len(rows),
-                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+                "power_w_max": max((float(r[4]) for r in rows
+                                    if r[4].replace(".", "").isdigit()), default=None)}
 
 
 # ---------------------------------------------------------------------------
@@ -416,6 +440,7 @@ def ours(args):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     eng.timing_begin()
+    sampler.begin()
     e0.record(stream)
     for s in range(args.steps):
         substep(s)
@@ -917,6 +942,7 @@ def amr_bench(args):
     eng.status_reset()
     sampler = ClockSampler(0)
     sampler.start()
+    sampler.begin()
     ms_b = timed(graph.replay, nrk)
     clocks = sampler.stop()
     st = eng.status()
