@@ -109,6 +109,37 @@ AXB_API const char *axb_gf_name(int id) {
   return (id >= 0 && id < AXB_NUM_GF) ? names[id] : nullptr;
 }
 
+namespace axb {
+// the context's second stream and its events (created once, on the
+// context's device); false when they cannot be had
+bool side_stream(axb_ctx *c) {
+  if (c->side)
+    return true;
+  if (!c->allow_side)
+    return false;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev != c->device)
+    return false;
+  if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess) {
+    c->side = nullptr;
+    return false;
+  }
+  cudaEvent_t *evs[3] = {&c->ev_fork, &c->ev_sources, &c->ev_aux};
+  for (cudaEvent_t *e : evs)
+    if (cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) {
+      for (cudaEvent_t *f : evs)
+        if (*f)
+          cudaEventDestroy(*f);
+      c->ev_fork = c->ev_sources = c->ev_aux = nullptr;
+      cudaStreamDestroy(c->side);
+      c->side = nullptr;
+      return false;
+    }
+  return true;
+}
+
+} // namespace axb
+
 AXB_API int axb_ctx_create(int device, axb_ctx **out) {
   if (!out)
     return AXB_ERR_ARG;
@@ -131,6 +162,11 @@ AXB_API int axb_ctx_create(int device, axb_ctx **out) {
     return AXB_ERR_CUDA;
   }
   AXB_CUDA_TRY(cudaMemset(c->status, 0, sizeof(DevStatus)));
+  // the second stream of the RHS group, made here so that no call made
+  // during a stream capture has to create it
+  c->allow_side = 1;
+  if (!side_stream(c))
+    c->allow_side = 0;
   *out = c;
   return AXB_OK;
 }
@@ -143,6 +179,13 @@ AXB_API int axb_ctx_destroy(axb_ctx *c) {
       cudaEventDestroy(c->ev[q]);
     delete[] c->ev;
     delete[] c->ev_region;
+  }
+  if (c->side) {
+    cudaStreamSynchronize(c->side);
+    cudaStreamDestroy(c->side);
+    cudaEventDestroy(c->ev_fork);
+    cudaEventDestroy(c->ev_sources);
+    cudaEventDestroy(c->ev_aux);
   }
   cudaFree(c->status);
   cudaFreeHost(c->status_host_pinned);
@@ -650,6 +693,42 @@ int rhs_group_run(axb_ctx *c, const axb_box *box, const axb_fields *f,
 #define AXB_FLUX_SEGLEN 16 // cells per y/z pencil segment (one thread each)
 #endif
   const int seglen = AXB_FLUX_SEGLEN;
+  if (!bc && side_stream(c)) {
+    // the sources and the vertex auxiliaries read neither the partial
+    // divergences nor the face B fluxes, and the flux passes read neither
+    // the sources' RHS nor the auxiliaries: they run on the second stream
+    // beside the x and y passes; the z pass waits for the sources' RHS, the
+    // CT kernel for the auxiliaries (which read A and Psi before it
+    // updates them)
+    cudaEventRecord(c->ev_fork, s);
+    cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+    axb_mark(c, AXB_R_SOURCES, c->side, true);
+    rc = launch_rhs_misc(p->local_spatial_order == 4 ? 1 : 0, a, c->side);
+    axb_mark(c, AXB_R_SOURCES, c->side, false);
+    cudaEventRecord(c->ev_sources, c->side);
+    int rc_aux = AXB_OK;
+    if (!rc) {
+      axb_mark(c, AXB_R_AUX, c->side, true);
+      rc_aux = launch_rhs_misc(2, a, c->side);
+      axb_mark(c, AXB_R_AUX, c->side, false);
+    }
+    cudaEventRecord(c->ev_aux, c->side);
+    for (int dir = 0; dir < 3 && !rc && !rc_aux; ++dir) {
+      if (dir == 2)
+        cudaStreamWaitEvent(s, c->ev_sources, 0);
+      axb_mark(c, AXB_R_FLUX_X + dir, s, true);
+      rc = launch_flux_pass(dir, p->reconstruction_method, a, *eos, seglen, s);
+      axb_mark(c, AXB_R_FLUX_X + dir, s, false);
+    }
+    // always joined back, on success or not
+    cudaStreamWaitEvent(s, c->ev_aux, 0);
+    if (rc || rc_aux)
+      return rc ? rc : rc_aux;
+    axb_mark(c, AXB_R_CT, s, true);
+    rc = launch_rhs_misc(3, a, s);
+    axb_mark(c, AXB_R_CT, s, false);
+    return rc;
+  }
   axb_mark(c, AXB_R_SOURCES, s, true);
   rc = launch_rhs_misc(p->local_spatial_order == 4 ? 1 : 0, a, s);
   axb_mark(c, AXB_R_SOURCES, s, false);

@@ -40,6 +40,13 @@ struct axb_ctx {
   // stream-ordered pool of per-call scratch (the recovery's deferred-cell
   // queue); keeps its memory between calls
   cudaMemPool_t pool = nullptr;
+  // a second stream for the RHS group's kernels that do not depend on the
+  // flux passes (sources, vertex auxiliaries), forked from and joined back
+  // into the caller's stream with events; created on first use, in
+  // contexts from axb_ctx_create only (which destroys them)
+  int allow_side = 0;
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_sources = nullptr, ev_aux = nullptr;
 };
 
 // Stream-ordered scratch: from the context's pool, or (during a stream

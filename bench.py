@@ -550,6 +550,9 @@ def ours(args):
                                      "achieved": substep_gbs, "frac": substep_gbs / peak}},
             "kernels_ms_per_step": {REGIONS[i]: region_ms[i] / args.steps
                                     for i in range(len(REGIONS)) if region_n[i]},
+            "kernels_note": "sources and aux run on a second stream beside flux_x and "
+                            "flux_y, so their region times overlap those passes' (the "
+                            "per-kernel shares are in the committed ncu launch list)",
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": ne,
                     "copies": f"{len(inputs)} fields in, {len(outputs)} out per step from/to "
