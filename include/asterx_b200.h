@@ -187,8 +187,12 @@ AXB_API const char *axb_gf_name(int id);
 typedef struct axb_ctx axb_ctx;
 
 /* Bind to CUDA device `device` (must be sm_100) and allocate the small
- * device status block (error word, CFL maximum, c2p counters).  No
- * counterpart in the reference, whose device errors are asserts. */
+ * device status block (error word, CFL maximum, c2p counters) and a second
+ * stream with three events, onto which the RHS group forks the kernels that
+ * do not depend on the flux passes (joined back into the caller's stream
+ * before the call's last kernel).  A context serves one host thread at a
+ * time; give each thread its own.  No counterpart in the reference, whose
+ * device errors are asserts. */
 AXB_API int axb_ctx_create(int device, axb_ctx **out);
 AXB_API int axb_ctx_destroy(axb_ctx *ctx);
 
