@@ -209,12 +209,15 @@ AXB_API int axb_halo_exchange(axb_halo *h, const axb_fields *f, void *stream) {
   // the upper planes go up and arrive as the upper neighbour's lower ghosts;
   // the lower planes go down
   const Nccl &N = nccl();
-  if (N.GroupStart() != ncclSuccess ||
-      N.Send(k.send_up, n, ncclDouble, h->up, h->comm, s) != ncclSuccess ||
-      N.Recv(k.recv_low, n, ncclDouble, h->down, h->comm, s) != ncclSuccess ||
-      N.Send(k.send_down, n, ncclDouble, h->down, h->comm, s) != ncclSuccess ||
-      N.Recv(k.recv_high, n, ncclDouble, h->up, h->comm, s) != ncclSuccess ||
-      N.GroupEnd() != ncclSuccess)
+  if (N.GroupStart() != ncclSuccess)
+    return AXB_ERR_CUDA;
+  // a group once opened is always closed, whatever failed inside it
+  const bool queued =
+      N.Send(k.send_up, n, ncclDouble, h->up, h->comm, s) == ncclSuccess &&
+      N.Recv(k.recv_low, n, ncclDouble, h->down, h->comm, s) == ncclSuccess &&
+      N.Send(k.send_down, n, ncclDouble, h->down, h->comm, s) == ncclSuccess &&
+      N.Recv(k.recv_high, n, ncclDouble, h->up, h->comm, s) == ncclSuccess;
+  if (N.GroupEnd() != ncclSuccess || !queued)
     return AXB_ERR_CUDA;
   k_halo_unpack<<<blocks, 256, 0, s>>>(k);
   return cudaGetLastError() == cudaSuccess ? AXB_OK : AXB_ERR_CUDA;
