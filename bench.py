@@ -45,6 +45,8 @@ TAB_PARAMS = dict(reconstruct_with_temperature=1, t_atmo=0.011, use_temperature=
 # (RHS reads 34, stage 33, post-step reads 23 and writes 22)
 SUBSTEP_BYTES = 112 * 8
 EOS_KW = dict(rho=(1e-40, 1e10), eps=(0.0, 1e10))
+# regions that run concurrently on two streams in the single-box substep
+OVERLAPPED = {"sources", "aux", "flux_x", "flux_y"}
 REGIONS = ["sources", "flux_x", "flux_y", "flux_z", "aux", "ct_psi", "rk_stage",
            "sync", "bstag", "c2p", "c2p_cells", "mlp"]
 # Algorithmic FP64 values moved per interior zone by each kernel (each field
@@ -463,9 +465,13 @@ def ours(args):
         print(f"bench: the timed substeps raised error word {st['error_word']:#x} "
               "(non-finite face fluxes or RHS)", file=sys.stderr)
 
-    # dominant kernel and its roofline
+    # dominant kernel and its roofline: the kernel with the largest time of
+    # its own; the sources and the vertex auxiliaries run on a second stream
+    # beside the x and y flux passes, so those four regions' event times
+    # include each other's and are no kernel's own time
     shares = {REGIONS[i]: region_ms[i] for i in range(len(REGIONS))
-              if region_n[i] and REGIONS[i] in ALG_DOUBLES}
+              if region_n[i] and REGIONS[i] in ALG_DOUBLES
+              and REGIONS[i] not in OVERLAPPED}
     dom = max(shares, key=shares.get)
     idom = REGIONS.index(dom)
     avg_launch_s = region_ms[idom] / region_n[idom] / 1e3
