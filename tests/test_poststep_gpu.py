@@ -2,7 +2,7 @@
 the Noble / Palenzuela cascade) and of full SSP-RK3 substeps on the GPU
 against the reference sources compiled on the host, same seeded inputs.
 Tolerance for recovered primitives and conserved variables: normalised max
-error <= 1e-10 (north-star primitive tolerance); c2p cell flags identical."""
+error <= 1e-10 (the primitive tolerance); c2p cell flags identical."""
 import numpy as np
 import pytest
 

@@ -1,7 +1,7 @@
 """Parity of the RHS group (AsterX_Fluxes + AsterX_SourceTerms + AsterX_RHS)
 on the GPU against the reference sources compiled on the host, on the same
-seeded boxes.  Tolerance: normalised max error <= 1e-12 per field (north-star
-RHS tolerance per substep)."""
+seeded boxes.  Tolerance: normalised max error <= 1e-12 per field (the RHS
+tolerance per substep)."""
 import numpy as np
 import pytest
 
