@@ -173,11 +173,29 @@ struct EosTab {
   // here to rounding.  Where the node values are not increasing around the
   // root, the reference's Brent search is run instead.
   AXB_HD double logtemp_root(double lrho, double leps, double ye, double vlo, double vhi) const {
-    // vlo = interp at node 0 < leps < vhi = interp at the last node
+    // vlo = interp at node 0 < leps < vhi = interp at the last node.
+    // The bisection evaluates the interpolant at temperature nodes, where it
+    // is the bilinear interpolant in (ln rho, Ye) of that node's four
+    // values: the rho and Ye cells and weights are found once, and each step
+    // reads four values (interp's own arithmetic with the temperature weight
+    // zero)
+    const int i = find(0, lrho), k = find(2, ye);
+    const double lam_r = (lrho - x[0][i]) / (x[0][i + 1] - x[0][i]);
+    const double lam_y = (ye - x[2][k]) / (x[2][k + 1] - x[2][k]);
+    auto at_node = [&](int jn) {
+      double A[2];
+#pragma unroll
+      for (int o2 = 0; o2 < 2; ++o2) {
+        const long long base = i + (long long)n[0] * (jn + (long long)n[1] * (k + o2));
+        const double y0 = y[TAB_NV * base + TAB_EPS], y1 = y[TAB_NV * (base + 1) + TAB_EPS];
+        A[o2] = (y1 - y0) * lam_r + y0;
+      }
+      return (A[1] - A[0]) * lam_y + A[0];
+    };
     int lo = 0, hi = n[1] - 1;
     while (hi - lo > 1) {
       const int mid = (lo + hi) >> 1;
-      const double vm = interp(TAB_EPS, lrho, x[1][mid], ye);
+      const double vm = at_node(mid);
       if (vm <= leps) {
         lo = mid;
         vlo = vm;
@@ -188,7 +206,6 @@ struct EosTab {
     }
     // the cell [x_lo, x_lo+1]: interp = c0 + c1 * lambda, lambda in [0, 1]
     const double xa = x[1][lo], xb = x[1][lo + 1];
-    const int i = find(0, lrho), k = find(2, ye);
     double c[2][2]; // [T end][Ye end] after the interpolation along ln rho
 #pragma unroll
     for (int o2 = 0; o2 < 2; ++o2)
@@ -196,12 +213,11 @@ struct EosTab {
       for (int o1 = 0; o1 < 2; ++o1) {
         const long long base =
             i + (long long)n[0] * ((lo + o1) + (long long)n[1] * (k + o2));
-        c[o1][o2] = lin(y[TAB_NV * base + TAB_EPS], y[TAB_NV * (base + 1) + TAB_EPS],
-                        x[0][i], x[0][i + 1], lrho);
+        const double y0 = y[TAB_NV * base + TAB_EPS], y1 = y[TAB_NV * (base + 1) + TAB_EPS];
+        c[o1][o2] = (y1 - y0) * lam_r + y0; // lin along ln rho, its weight found once
       }
-    const double lamy = (ye - x[2][k]) / (x[2][k + 1] - x[2][k]);
-    const double e0 = (c[0][1] - c[0][0]) * lamy + c[0][0]; // at x_lo
-    const double e1 = (c[1][1] - c[1][0]) * lamy + c[1][0]; // at x_lo+1
+    const double e0 = (c[0][1] - c[0][0]) * lam_y + c[0][0]; // at x_lo
+    const double e1 = (c[1][1] - c[1][0]) * lam_y + c[1][0]; // at x_lo+1
     if (!(vlo <= leps && leps <= vhi) || !(e1 > e0)) {
       bool capped;
       const double lt = zero_brent(
